@@ -1,0 +1,462 @@
+// extern "C" boundary: status codes instead of exceptions, thread-local
+// error messages, caller-owned device pointers.
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "gb_internal.cuh"
+#include "gb_ops.hpp"
+
+namespace gb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+struct Failure {
+    gb_status st;
+    std::string msg;
+};
+
+void fail(gb_status st, const std::string &msg) { throw Failure{st, msg}; }
+
+void check_cuda(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(e == cudaErrorMemoryAllocation ? GB_ERR_OUT_OF_MEMORY : GB_ERR_CUDA,
+             std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+void check_cufft(cufftResult r, const char *what) {
+    if (r != CUFFT_SUCCESS)
+        fail(r == CUFFT_ALLOC_FAILED ? GB_ERR_OUT_OF_MEMORY : GB_ERR_CUFFT,
+             std::string(what) + ": cuFFT error " + std::to_string((int)r));
+}
+
+template <class F>
+static gb_status guarded(F &&f) {
+    try {
+        f();
+        return GB_OK;
+    } catch (const Failure &e) {
+        set_error(e.msg);
+        return e.st;
+    } catch (const std::bad_alloc &) {
+        set_error("host allocation failed");
+        return GB_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception &e) {
+        set_error(e.what());
+        return GB_ERR_INTERNAL;
+    } catch (...) {
+        set_error("unknown error");
+        return GB_ERR_INTERNAL;
+    }
+}
+
+static cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Switches to the object's device for the duration of a call.
+struct DeviceGuard {
+    int old = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&old);
+        if (old != dev) check_cuda(cudaSetDevice(dev), "cudaSetDevice");
+    }
+    ~DeviceGuard() {
+        int cur;
+        if (cudaGetDevice(&cur) == cudaSuccess && cur != old && old >= 0) cudaSetDevice(old);
+    }
+};
+
+static void set_tiling(NufftPlan &p, const int *tile, int cg) {
+    const KParams &k = p.kp;
+    int t[kMaxD] = {1, 1, 1};
+    for (int d = 0; d < p.D; d++) t[d] = tile[d];
+    int cells = t[0] * t[1] * t[2];
+    for (int d = 0; d < p.D; d++)
+        if (t[d] <= 0 || k.mos[d] % t[d]) fail(GB_ERR_INVALID_ARGUMENT, "tile size must divide the oversampled size");
+    if (p.D == 1) {
+        if (t[0] % 32) fail(GB_ERR_INVALID_ARGUMENT, "1D tile must be a multiple of 32");
+    } else if (t[0] % 8 || t[1] % 4) {
+        fail(GB_ERR_INVALID_ARGUMENT, "tile x must be a multiple of 8 and y a multiple of 4");
+    }
+    if (cells > 4 * kThreads || (cells > kThreads && cells % kThreads) || (cells < kThreads && kThreads % cells))
+        fail(GB_ERR_INVALID_ARGUMENT, "tile must hold a divisor of 256 cells, or 512 or 1024 cells");
+    if (2 * k.hw + 1 > kWMax) fail(GB_ERR_INVALID_ARGUMENT, "kernel width too large");
+    // A footprint of at most 2*hw+1 cells must span at most 3 tiles per
+    // dimension (the binning records up to 3 tiles per dimension).
+    for (int d = 0; d < p.D; d++)
+        if (t[d] < 2 * k.hw && t[d] != k.mos[d])
+            fail(GB_ERR_INVALID_ARGUMENT, "tile must be at least W cells wide in every dimension");
+    if (cg != 1 && cg != 2 && cg != 4 && cg != 8 && cg != 16)
+        fail(GB_ERR_INVALID_ARGUMENT, "coil group must be 1, 2, 4, 8 or 16");
+    p.tiling.cg = cg;
+    for (int d = 0; d < kMaxD; d++) {
+        p.tiling.tile[d] = t[d];
+        p.kp.tile[d] = t[d];
+        p.kp.ntiles[d] = p.kp.mos[d] / t[d];
+    }
+    p.kp.ntiles_total = p.kp.ntiles[0] * p.kp.ntiles[1] * p.kp.ntiles[2];
+}
+
+}  // namespace gb
+
+using namespace gb;
+
+struct gb_nufft_plan_s {
+    std::unique_ptr<NufftPlan> owned;   // null for a view of an operator's plan
+    NufftPlan *p = nullptr;
+};
+struct gb_sense_op_s {
+    SenseOp s;
+    gb_nufft_plan_s view;
+};
+struct gb_cg_solver_s {
+    CgSolver c;
+};
+
+extern "C" {
+
+GB_API const char *gb_last_error_message(void) { return g_last_error.c_str(); }
+
+GB_API const char *gb_version(void) { return "gadgetron_b200 0.1 (sm_100a)"; }
+
+static void default_tiling(NufftPlan &p) {
+    int t[3] = {16, 16, 1};
+    if (p.D == 1) { t[0] = 256; }
+    if (p.D == 3) { t[0] = 8; t[1] = 8; t[2] = 8; }
+    // shrink for small grids while keeping >= 256 cells per tile
+    for (int d = 0; d < p.D; d++)
+        if (t[d] > p.kp.mos[d]) t[d] = (int)p.kp.mos[d];
+    set_tiling(p, t, 8);
+}
+
+GB_API gb_status gb_nufft_plan_create(int D, const uint64_t *matrix_size, const uint64_t *matrix_size_os,
+                                      float W, uint32_t flags, gb_nufft_plan *plan) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan pointer");
+        *plan = nullptr;
+        auto *h = new gb_nufft_plan_s();
+        h->owned.reset(new NufftPlan());
+        h->p = h->owned.get();
+        try {
+            plan_init(*h->p, D, matrix_size, matrix_size_os, W, flags);
+            default_tiling(*h->p);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *plan = h;
+    });
+}
+
+GB_API gb_status gb_nufft_plan_destroy(gb_nufft_plan plan) {
+    return guarded([&] {
+        if (!plan) return;
+        if (!plan->owned) fail(GB_ERR_INVALID_ARGUMENT, "this plan belongs to a SENSE operator");
+        DeviceGuard g((*plan->p).device);
+        delete plan;
+    });
+}
+
+GB_API gb_status gb_nufft_preprocess(gb_nufft_plan plan, const float *trajectory, uint64_t num_samples_total,
+                                     uint32_t num_frames, const uint64_t *frame_offsets, gb_prep_mode mode,
+                                     void *stream) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
+        DeviceGuard g((*plan->p).device);
+        plan_preprocess((*plan->p), trajectory, num_samples_total, num_frames, frame_offsets, mode, S(stream));
+    });
+}
+
+GB_API gb_status gb_nufft_compute(gb_nufft_plan plan, const void *in, void *out, const float *dcw,
+                                  gb_comp_mode mode, uint32_t num_batches, int image_oversampled, void *stream) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
+        DeviceGuard g((*plan->p).device);
+        nufft_compute((*plan->p), in, out, dcw, mode, (int)num_batches, image_oversampled != 0, S(stream));
+    });
+}
+
+GB_API gb_status gb_nufft_mult_MH_M(gb_nufft_plan plan, const void *in, void *out, const float *dcw,
+                                    uint32_t num_batches, void *stream) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
+        if (num_batches == 0) fail(GB_ERR_INVALID_ARGUMENT, "number of batches must be positive");
+        DeviceGuard g((*plan->p).device);
+        nufft_mult_MH_M((*plan->p), in, out, dcw, (int)num_batches, S(stream));
+    });
+}
+
+GB_API gb_status gb_nufft_convolve(gb_nufft_plan plan, const void *in, void *out, gb_conv_mode mode,
+                                   int accumulate, uint32_t num_batches, void *stream) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
+        if (num_batches == 0) fail(GB_ERR_INVALID_ARGUMENT, "number of batches must be positive");
+        DeviceGuard g((*plan->p).device);
+        nufft_convolve((*plan->p), in, out, mode, accumulate != 0, (int)num_batches, S(stream));
+    });
+}
+
+GB_API gb_status gb_nufft_fft(gb_nufft_plan plan, void *data, gb_fft_mode mode, int do_scale,
+                              uint32_t num_frames_x_batches, void *stream) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
+        DeviceGuard g((*plan->p).device);
+        nufft_fft((*plan->p), data, mode, do_scale != 0, (int)num_frames_x_batches, S(stream));
+    });
+}
+
+GB_API gb_status gb_nufft_deapodize(gb_nufft_plan plan, void *image, int fourier_domain,
+                                    uint32_t num_frames_x_batches, void *stream) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
+        (void)fourier_domain;   // both filters carry the same real values
+        DeviceGuard g((*plan->p).device);
+        nufft_deapodize((*plan->p), image, (int)num_frames_x_batches, S(stream));
+    });
+}
+
+GB_API gb_status gb_nufft_traj_grad(gb_nufft_plan plan, const void *image, const void *weights, const float *dcw,
+                                    float *grad_traj, uint32_t num_batches, void *stream) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
+        if (!image || !weights || !grad_traj) fail(GB_ERR_INVALID_ARGUMENT, "NULL argument");
+        if (num_batches == 0) fail(GB_ERR_INVALID_ARGUMENT, "number of batches must be positive");
+        DeviceGuard g((*plan->p).device);
+        nufft_traj_grad((*plan->p), static_cast<const float2 *>(image), static_cast<const float2 *>(weights), dcw,
+                        grad_traj, (int)num_batches, S(stream));
+    });
+}
+
+GB_API gb_status gb_nufft_traj_grad_from_grid(gb_nufft_plan plan, const void *grid, const void *weights,
+                                              float *grad_traj, uint32_t num_batches, void *stream) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
+        if (!grid || !weights || !grad_traj) fail(GB_ERR_INVALID_ARGUMENT, "NULL argument");
+        if (num_batches == 0) fail(GB_ERR_INVALID_ARGUMENT, "number of batches must be positive");
+        DeviceGuard g((*plan->p).device);
+        nufft_traj_grad_from_grid((*plan->p), static_cast<const float2 *>(grid), static_cast<const float2 *>(weights),
+                                  grad_traj, (int)num_batches, S(stream));
+    });
+}
+
+GB_API gb_status gb_nufft_get_info(gb_nufft_plan plan, int *D, uint64_t *matrix_size, uint64_t *matrix_size_os,
+                                   float *W, uint64_t *num_samples_total, uint32_t *num_frames) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
+        const NufftPlan &p = (*plan->p);
+        if (D) *D = p.D;
+        for (int d = 0; d < p.D; d++) {
+            if (matrix_size) matrix_size[d] = (uint64_t)p.N[d];
+            if (matrix_size_os) matrix_size_os[d] = (uint64_t)p.mos[d];
+        }
+        if (W) *W = p.W;
+        if (num_samples_total) *num_samples_total = (uint64_t)p.Mtot;
+        if (num_frames) *num_frames = p.F;
+    });
+}
+
+GB_API gb_status gb_nufft_get_tiling(gb_nufft_plan plan, int *tile, int *coil_group) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
+        for (int d = 0; d < kMaxD; d++)
+            if (tile) tile[d] = (*plan->p).tiling.tile[d];
+        if (coil_group) *coil_group = (*plan->p).tiling.cg;
+    });
+}
+
+GB_API gb_status gb_nufft_set_tiling(gb_nufft_plan plan, const int *tile, int coil_group) {
+    return guarded([&] {
+        if (!plan || !tile) fail(GB_ERR_INVALID_ARGUMENT, "NULL argument");
+        DeviceGuard g((*plan->p).device);
+        NufftPlan &p = (*plan->p);
+        set_tiling(p, tile, coil_group);
+        if (p.prepped) {
+            // Re-bin with the new tiles: rebuild from the stored sorted data.
+            fail(GB_ERR_INVALID_ARGUMENT, "set the tiling before preprocess");
+        }
+    });
+}
+
+// ---------------------------------------------------------------- SENSE ---
+
+GB_API gb_status gb_sense_create(int D, const uint64_t *matrix_size, const uint64_t *matrix_size_os, float W,
+                                 uint32_t flags, gb_sense_op *op) {
+    return guarded([&] {
+        if (!op) fail(GB_ERR_INVALID_ARGUMENT, "NULL operator pointer");
+        *op = nullptr;
+        auto *h = new gb_sense_op_s();
+        try {
+            plan_init(h->s.plan, D, matrix_size, matrix_size_os, W, flags);
+            default_tiling(h->s.plan);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *op = h;
+    });
+}
+
+GB_API gb_status gb_sense_destroy(gb_sense_op op) {
+    return guarded([&] {
+        if (!op) return;
+        DeviceGuard g(op->s.plan.device);
+        delete op;
+    });
+}
+
+GB_API gb_status gb_sense_preprocess(gb_sense_op op, const float *trajectory, uint64_t num_samples_total,
+                                     uint32_t num_frames, const uint64_t *frame_offsets, void *stream) {
+    return guarded([&] {
+        if (!op) fail(GB_ERR_INVALID_ARGUMENT, "NULL operator");
+        if (!trajectory) fail(GB_ERR_INVALID_ARGUMENT, "cuNonCartesianSenseOperator: cannot preprocess 0x0 trajectory.");
+        DeviceGuard g(op->s.plan.device);
+        plan_preprocess(op->s.plan, trajectory, num_samples_total, num_frames, frame_offsets, GB_PREP_ALL,
+                        S(stream));
+    });
+}
+
+GB_API gb_status gb_sense_set_csm(gb_sense_op op, const void *csm, uint32_t num_coils) {
+    return guarded([&] {
+        if (!op) fail(GB_ERR_INVALID_ARGUMENT, "NULL operator");
+        if (!csm || num_coils == 0)
+            fail(GB_ERR_INVALID_ARGUMENT, "Error: senseOperator::set_csm : unexpected csm dimensionality");
+        op->s.csm = static_cast<const float2 *>(csm);
+        op->s.ncoils = (int)num_coils;
+    });
+}
+
+GB_API gb_status gb_sense_set_dcw(gb_sense_op op, const float *dcw) {
+    return guarded([&] {
+        if (!op) fail(GB_ERR_INVALID_ARGUMENT, "NULL operator");
+        op->s.dcw = dcw;
+    });
+}
+
+GB_API gb_status gb_sense_mult_M(gb_sense_op op, const void *in, void *out, int accumulate, void *stream) {
+    return guarded([&] {
+        if (!op) fail(GB_ERR_INVALID_ARGUMENT, "NULL operator");
+        DeviceGuard g(op->s.plan.device);
+        sense_mult_M(op->s, in, out, accumulate != 0, S(stream));
+    });
+}
+
+GB_API gb_status gb_sense_mult_MH(gb_sense_op op, const void *in, void *out, int accumulate, void *stream) {
+    return guarded([&] {
+        if (!op) fail(GB_ERR_INVALID_ARGUMENT, "NULL operator");
+        DeviceGuard g(op->s.plan.device);
+        sense_mult_MH(op->s, in, out, accumulate != 0, S(stream));
+    });
+}
+
+GB_API gb_status gb_sense_mult_MH_M(gb_sense_op op, const void *in, void *out, int accumulate, void *stream) {
+    return guarded([&] {
+        if (!op) fail(GB_ERR_INVALID_ARGUMENT, "NULL operator");
+        DeviceGuard g(op->s.plan.device);
+        sense_mult_MH_M(op->s, in, out, accumulate != 0, S(stream));
+    });
+}
+
+GB_API gb_status gb_sense_get_nufft_plan(gb_sense_op op, gb_nufft_plan *plan) {
+    return guarded([&] {
+        if (!op || !plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL argument");
+        // A non-owning view of the operator's plan.
+        op->view.p = &op->s.plan;
+        *plan = &op->view;
+    });
+}
+
+// ------------------------------------------------------------------- CG ---
+
+GB_API gb_status gb_cg_create(gb_cg_solver *solver) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver pointer");
+        *solver = new gb_cg_solver_s();
+    });
+}
+
+GB_API gb_status gb_cg_destroy(gb_cg_solver solver) {
+    return guarded([&] {
+        if (!solver) return;
+        if (solver->c.E) {
+            DeviceGuard g(solver->c.E->plan.device);
+            delete solver;
+        } else {
+            delete solver;
+        }
+    });
+}
+
+GB_API gb_status gb_cg_set_encoding_operator(gb_cg_solver solver, gb_sense_op op, float weight) {
+    return guarded([&] {
+        if (!solver || !op) fail(GB_ERR_INVALID_ARGUMENT, "NULL argument");
+        solver->c.E = &op->s;
+        solver->c.weight = weight;
+    });
+}
+
+GB_API gb_status gb_cg_set_max_iterations(gb_cg_solver solver, uint32_t iterations) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
+        solver->c.iterations = iterations;
+    });
+}
+
+GB_API gb_status gb_cg_set_tc_tolerance(gb_cg_solver solver, float tolerance) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
+        solver->c.tol = tolerance;
+    });
+}
+
+GB_API gb_status gb_cg_set_x0(gb_cg_solver solver, const void *x0) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
+        solver->c.x0 = static_cast<const float2 *>(x0);
+    });
+}
+
+GB_API gb_status gb_cg_set_preconditioner(gb_cg_solver solver, const float *weights) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
+        solver->c.precond = weights;
+    });
+}
+
+GB_API gb_status gb_cg_set_identity_regularization(gb_cg_solver solver, float kappa) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
+        solver->c.kappa = kappa;
+    });
+}
+
+GB_API gb_status gb_cg_set_refinements(gb_cg_solver solver, uint32_t refinements) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
+        if (refinements == 0) fail(GB_ERR_INVALID_ARGUMENT, "refinements must be >= 1");
+        solver->c.refinements = refinements;
+    });
+}
+
+GB_API gb_status gb_cg_set_use_graph(gb_cg_solver solver, int use_graph) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
+        solver->c.use_graph = use_graph != 0;
+    });
+}
+
+GB_API gb_status gb_cg_solve(gb_cg_solver solver, const void *d, void *x_out, double *residual_history,
+                             uint32_t *iterations_run, void *stream) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
+        if (!solver->c.E) fail(GB_ERR_INVALID_ARGUMENT, "Error: cgSolver::compute_rhs : no encoding operator is set");
+        DeviceGuard g(solver->c.E->plan.device);
+        cg_solve(solver->c, d, x_out, residual_history, iterations_run, S(stream));
+    });
+}
+
+}  // extern "C"

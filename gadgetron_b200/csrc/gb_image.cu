@@ -1,0 +1,260 @@
+// Image-side kernels around the oversampled FFT.
+//
+// The reference runs, for the forward NUFFT inside the SENSE operator:
+// mult_csm (sense_utilities.cu:7-18) -> pad (cuNDArray_utils.cu:273-337) ->
+// deapodize (cuNFFT.cu:74-92) -> timeswitch -> cuFFT -> timeswitch -> scale
+// (cuNDFFT.cpp:184-217, cuNDFFT.cu:6-36), and the mirror image for the
+// adjoint ending in crop (cuNDArray_utils.cu:213-262) and
+// mult_csm_conj_sum (sense_utilities.cu:66-78).  Each is a separate pass
+// over the full oversampled array.
+//
+// Here one kernel does coil multiply + deapodization + checkerboard + 1/sqrt(G)
+// and writes only the N^D interior of a padded buffer whose exterior stays
+// zero (the FFT runs out of place, so the zeros are never overwritten); the
+// checkerboard after the FFT is folded into the convolution weights.  On the
+// way back one kernel does checkerboard + scale + deapodization + crop +
+// conjugate-coil sum.
+#include "gb_internal.cuh"
+
+namespace gb {
+
+struct ImgArgs {
+    KParams k;
+    const float *deap;     // [D][stride] per-dim reciprocal transforms
+    int deap_stride;
+    float scale;
+};
+
+__device__ __forceinline__ void unflatten(int64_t n, const int *sz, int &x, int &y, int &z) {
+    x = (int)(n % sz[0]);
+    int64_t r = n / sz[0];
+    y = (int)(r % sz[1]);
+    z = (int)(r / sz[1]);
+}
+
+// Interior factor deap(n) * (-1)^(sum g) * scale for image pixel (x,y,z).
+__device__ __forceinline__ float interior_factor(const ImgArgs &a, int x, int y, int z, int64_t &g) {
+    const KParams &k = a.k;
+    const int ox = (k.mos[0] - k.N[0]) >> 1, oy = (k.mos[1] - k.N[1]) >> 1, oz = (k.mos[2] - k.N[2]) >> 1;
+    const int gx = x + ox, gy = y + oy, gz = z + oz;
+    g = ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + gx;
+    float f = a.deap[x];
+    if (k.D > 1) f *= a.deap[a.deap_stride + y];
+    if (k.D > 2) f *= a.deap[2 * a.deap_stride + z];
+    if ((gx + gy + gz) & 1) f = -f;
+    return f * a.scale;
+}
+
+__device__ __forceinline__ float os_factor(const ImgArgs &a, int gx, int gy, int gz) {
+    const KParams &k = a.k;
+    float f = a.deap[gx];
+    if (k.D > 1) f *= a.deap[a.deap_stride + gy];
+    if (k.D > 2) f *= a.deap[2 * a.deap_stride + gz];
+    if ((gx + gy + gz) & 1) f = -f;
+    return f * a.scale;
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {   // a * conj(b)
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// Forward, interior only.  csm == null: src [nb][F][NN]; else src [F][NN].
+__global__ void k_pad_forward(ImgArgs a, const float2 *__restrict__ src, const float2 *__restrict__ csm,
+                              float2 *__restrict__ dst, int nb, int F) {
+    const KParams &k = a.k;
+    const int64_t total = (int64_t)F * k.NN;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int f = (int)(e / k.NN);
+        const int64_t n = e - (int64_t)f * k.NN;
+        int x, y, z;
+        unflatten(n, k.N, x, y, z);
+        int64_t g;
+        const float fac = interior_factor(a, x, y, z, g);
+        if (csm) {
+            const float2 v = src[e];
+            for (int b = 0; b < nb; b++) {
+                const float2 c = cmul(v, csm[(int64_t)b * k.NN + n]);
+                dst[((int64_t)b * F + f) * k.G + g] = make_float2(c.x * fac, c.y * fac);
+            }
+        } else {
+            for (int b = 0; b < nb; b++) {
+                const float2 v = src[((int64_t)b * F + f) * k.NN + n];
+                dst[((int64_t)b * F + f) * k.G + g] = make_float2(v.x * fac, v.y * fac);
+            }
+        }
+    }
+}
+
+// Forward from an already oversampled image (full grid written).
+__global__ void k_pad_forward_os(ImgArgs a, const float2 *__restrict__ src, float2 *__restrict__ dst,
+                                 int64_t nbf) {
+    const KParams &k = a.k;
+    const int64_t total = nbf * k.G;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = e % k.G;
+        int x, y, z;
+        unflatten(g, k.mos, x, y, z);
+        const float fac = os_factor(a, x, y, z);
+        const float2 v = src[e];
+        dst[e] = make_float2(v.x * fac, v.y * fac);
+    }
+}
+
+// Adjoint: crop + deapodize + checkerboard + scale (+ conjugate coil sum).
+__global__ void k_crop_adjoint(ImgArgs a, const float2 *__restrict__ grid, const float2 *__restrict__ csm,
+                               float2 *__restrict__ dst, int nb, int F, int accumulate, float weight) {
+    const KParams &k = a.k;
+    const int64_t total = (int64_t)F * k.NN;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int f = (int)(e / k.NN);
+        const int64_t n = e - (int64_t)f * k.NN;
+        int x, y, z;
+        unflatten(n, k.N, x, y, z);
+        int64_t g;
+        const float fac = interior_factor(a, x, y, z, g) * weight;
+        if (csm) {
+            float2 s = make_float2(0.f, 0.f);
+            for (int b = 0; b < nb; b++) {
+                float2 v = grid[((int64_t)b * F + f) * k.G + g];
+                v = make_float2(v.x * fac, v.y * fac);
+                const float2 c = cmulc(v, csm[(int64_t)b * k.NN + n]);
+                s.x += c.x;
+                s.y += c.y;
+            }
+            if (accumulate) { const float2 o = dst[e]; s.x += o.x; s.y += o.y; }
+            dst[e] = s;
+        } else {
+            for (int b = 0; b < nb; b++) {
+                const float2 v = grid[((int64_t)b * F + f) * k.G + g];
+                float2 r = make_float2(v.x * fac, v.y * fac);
+                float2 *o = dst + ((int64_t)b * F + f) * k.NN + n;
+                if (accumulate) { const float2 ov = *o; r.x += ov.x; r.y += ov.y; }
+                *o = r;
+            }
+        }
+    }
+}
+
+__global__ void k_crop_adjoint_os(ImgArgs a, const float2 *__restrict__ grid, float2 *__restrict__ dst,
+                                  int64_t nbf, int accumulate) {
+    const KParams &k = a.k;
+    const int64_t total = nbf * k.G;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = e % k.G;
+        int x, y, z;
+        unflatten(g, k.mos, x, y, z);
+        const float fac = os_factor(a, x, y, z);
+        const float2 v = grid[e];
+        float2 r = make_float2(v.x * fac, v.y * fac);
+        if (accumulate) { const float2 o = dst[e]; r.x += o.x; r.y += o.y; }
+        dst[e] = r;
+    }
+}
+
+__global__ void k_timeswitch_scale(KParams k, float2 *__restrict__ data, int64_t nbf, float scale) {
+    const int64_t total = nbf * k.G;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = e % k.G;
+        int x, y, z;
+        unflatten(g, k.mos, x, y, z);
+        const float s = ((x + y + z) & 1) ? -scale : scale;
+        float2 v = data[e];
+        data[e] = make_float2(v.x * s, v.y * s);
+    }
+}
+
+__global__ void k_deapodize_os(ImgArgs a, float2 *__restrict__ data, int64_t nbf) {
+    const KParams &k = a.k;
+    const int64_t total = nbf * k.G;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = e % k.G;
+        int x, y, z;
+        unflatten(g, k.mos, x, y, z);
+        float f = a.deap[x];
+        if (k.D > 1) f *= a.deap[a.deap_stride + y];
+        if (k.D > 2) f *= a.deap[2 * a.deap_stride + z];
+        float2 v = data[e];
+        data[e] = make_float2(v.x * f, v.y * f);
+    }
+}
+
+__global__ void k_multiply_dcw(const float *__restrict__ dcw, float2 *__restrict__ data, int64_t M, int nb) {
+    const int64_t total = M * nb;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const float w = dcw[e % M];
+        float2 v = data[e];
+        data[e] = make_float2(v.x * w, v.y * w);
+    }
+}
+
+static unsigned grid_for(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16));
+}
+
+static ImgArgs img_args(NufftPlan &p, bool oversampled) {
+    ImgArgs a{};
+    a.k = p.kp;
+    a.deap = oversampled ? p.deap_os.get() : p.deap_img.get();
+    a.deap_stride = oversampled ? p.maxmos : p.maxN;
+    a.scale = (float)(1.0 / std::sqrt((double)p.kp.G));
+    return a;
+}
+
+void launch_pad_forward(NufftPlan &p, const float2 *src, const float2 *csm, float2 *dst, int nb,
+                        bool src_oversampled, cudaStream_t st) {
+    if (src_oversampled) {
+        ImgArgs a = img_args(p, true);
+        const int64_t nbf = (int64_t)nb * p.F;
+        k_pad_forward_os<<<grid_for(nbf * p.kp.G), 256, 0, st>>>(a, src, dst, nbf);
+    } else {
+        ImgArgs a = img_args(p, false);
+        k_pad_forward<<<grid_for((int64_t)p.F * p.kp.NN), 256, 0, st>>>(a, src, csm, dst, nb, (int)p.F);
+    }
+    GB_CUDA(cudaGetLastError());
+}
+
+void launch_crop_adjoint(NufftPlan &p, const float2 *grid, const float2 *csm, float2 *dst, int nb,
+                         bool dst_oversampled, bool accumulate, float weight, bool fourier_deapod,
+                         cudaStream_t st) {
+    (void)fourier_deapod;   // both deapodization filters have the same (real) values
+    if (dst_oversampled) {
+        ImgArgs a = img_args(p, true);
+        a.scale *= weight;
+        const int64_t nbf = (int64_t)nb * p.F;
+        k_crop_adjoint_os<<<grid_for(nbf * p.kp.G), 256, 0, st>>>(a, grid, dst, nbf, accumulate ? 1 : 0);
+    } else {
+        ImgArgs a = img_args(p, false);
+        k_crop_adjoint<<<grid_for((int64_t)p.F * p.kp.NN), 256, 0, st>>>(a, grid, csm, dst, nb, (int)p.F,
+                                                                         accumulate ? 1 : 0, weight);
+    }
+    GB_CUDA(cudaGetLastError());
+}
+
+void launch_timeswitch_scale(NufftPlan &p, float2 *data, int nbf, float scale, cudaStream_t st) {
+    k_timeswitch_scale<<<grid_for((int64_t)nbf * p.kp.G), 256, 0, st>>>(p.kp, data, nbf, scale);
+    GB_CUDA(cudaGetLastError());
+}
+
+void launch_deapodize_os(NufftPlan &p, float2 *data, int nbf, cudaStream_t st) {
+    ImgArgs a = img_args(p, true);
+    k_deapodize_os<<<grid_for((int64_t)nbf * p.kp.G), 256, 0, st>>>(a, data, nbf);
+    GB_CUDA(cudaGetLastError());
+}
+
+void launch_multiply_dcw(const float *dcw, float2 *data, int64_t M, int nb, cudaStream_t st) {
+    k_multiply_dcw<<<grid_for(M * nb), 256, 0, st>>>(dcw, data, M, nb);
+    GB_CUDA(cudaGetLastError());
+}
+
+}  // namespace gb

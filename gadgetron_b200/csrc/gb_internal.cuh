@@ -1,0 +1,301 @@
+// Internal declarations shared by the gadgetron_b200 CUDA sources.
+//
+// Data layout in HBM (x fastest everywhere, as in the reference arrays):
+//   image     [batches][frames][prod(N)]      complex64 (float2)
+//   grid      [batches][frames][prod(mos)]    complex64  (oversampled, k-space)
+//   samples   [batches][M_total]              complex64  (frame f owns
+//                                                         [off[f], off[f+1]))
+//   positions [D][M_total] float, sorted by tile ("home" order)
+//
+// The oversampled grid is cut into tiles of T_x x T_y x T_z cells.  Every
+// sample has one home tile (the tile holding floor(s) - pad/2); the degridding
+// kernel stages a home tile plus a halo of pad/2 cells and serves all its home
+// samples.  The gridding kernel owns a tile exclusively (no atomics): its
+// sample list holds every sample whose footprint touches the tile.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/gadgetron_b200.h"
+
+namespace gb {
+
+constexpr int kMaxD = 3;
+constexpr int kWMax = 8;          // max taps per dimension (W <= 7)
+constexpr int kThreads = 256;     // threads per CTA for the tile kernels
+constexpr int kChunk = 32;        // samples staged per pass
+
+// ------------------------------------------------------------ errors -----
+
+struct Error {
+    gb_status status;
+    std::string msg;
+};
+
+void set_error(const std::string &msg);
+[[noreturn]] void fail(gb_status st, const std::string &msg);
+void check_cuda(cudaError_t e, const char *what);
+void check_cufft(cufftResult r, const char *what);
+
+#define GB_CUDA(x) ::gb::check_cuda((x), #x)
+#define GB_CUFFT(x) ::gb::check_cufft((x), #x)
+
+// ------------------------------------------------- device buffer (RAII) ---
+
+template <class T>
+struct DevBuf {
+    T *ptr = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        n = 0;
+    }
+    // Grows to at least `count` elements; returns true if reallocated.
+    bool ensure(size_t count) {
+        if (count <= n && ptr) return false;
+        release();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc((void **)&ptr, count * sizeof(T));
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            cudaGetLastError();
+            fail(GB_ERR_OUT_OF_MEMORY, "device allocation of " +
+                 std::to_string(count * sizeof(T)) + " bytes failed");
+        }
+        n = count;
+        return true;
+    }
+    T *get() const { return ptr; }
+};
+
+// --------------------------------------------------------- kernel params ---
+
+// Plan constants passed by value to every kernel.
+struct KParams {
+    int D;
+    int mos[kMaxD];        // oversampled size per dim (1 for unused dims)
+    int N[kMaxD];          // matrix size per dim
+    int tile[kMaxD];       // tile size per dim
+    int ntiles[kMaxD];     // tiles per dim
+    int hw;                // pad/2 = ceil(W/2)
+    float radius;          // W/2
+    float one_over_W;
+    float beta[kMaxD];
+    float mos_f[kMaxD];
+    long long G;           // prod(mos)
+    long long NN;          // prod(N)
+    int ntiles_total;
+};
+
+// One unit of tile work: frame*ntiles + tile, a range of a sample list and,
+// for gridding tiles split across CTAs, the split bookkeeping.
+struct WorkItem {
+    int ft;        // frame * ntiles_total + tile
+    int begin;     // range in the list
+    int end;
+    int split;     // -1: not split; else index into split table
+    int chunk;     // chunk index within the split
+    int pad0, pad1, pad2;
+};
+
+struct SplitInfo {
+    int first_slot;  // first partial slot
+    int nchunks;
+};
+
+// ----------------------------------------------------------- the plan -----
+
+struct Tiling {
+    int tile[kMaxD] = {16, 16, 1};
+    int cg = 8;                 // coils per CTA (coil group)
+    int split_len = 0;          // gridding list length above which a tile is split (0 = auto)
+};
+
+struct NufftPlan {
+    int D = 0;
+    int64_t N[kMaxD] = {1, 1, 1};
+    int64_t mos[kMaxD] = {1, 1, 1};
+    float W = 0.f;
+    uint32_t flags = 0;
+    int device = 0;
+    KParams kp{};
+    Tiling tiling;
+
+    // preprocess state
+    bool prepped = false;
+    bool prepped_c2nc = false, prepped_nc2c = false;
+    uint32_t F = 0;
+    int64_t Mtot = 0;
+    std::vector<int64_t> frame_off;
+    DevBuf<float> pos_sorted;      // [D][Mtot]
+    DevBuf<uint32_t> perm;         // sorted pos -> original sample index
+    DevBuf<uint32_t> home_off;     // [F*ntiles + 1]
+    DevBuf<uint32_t> grid_list;    // gridding pair list (sorted positions)
+    DevBuf<uint32_t> grid_off;     // [F*ntiles + 1]
+    DevBuf<WorkItem> deg_items;
+    int n_deg_items = 0;
+    DevBuf<WorkItem> grd_items;
+    int n_grd_items = 0;
+    DevBuf<SplitInfo> splits;
+    int n_splits = 0, n_slots = 0;
+    DevBuf<unsigned int> split_counters;   // [n_splits * max coil groups]
+    int split_counter_groups = 0;
+    DevBuf<float2> partials;               // [n_slots][cg_groups][cells*cg]
+    int64_t total_pairs = 0;
+    std::vector<uint32_t> h_home_counts;   // per (frame, tile), for tuning
+
+    // deapodization: per-dim reciprocal of the 1D kernel transform
+    DevBuf<float> deap_img;   // [D][maxN]    1/psi_d(n + (mos-N)/2)
+    DevBuf<float> deap_os;    // [D][maxmos]  1/psi_d(g)
+    int maxN = 0, maxmos = 0;
+
+    // workspaces
+    DevBuf<float2> img_os;    // padded image, zero outside the interior
+    size_t img_os_batches_zeroed = 0;
+    bool img_os_dirty = true;
+    DevBuf<float2> kgrid;     // k-space grid
+    DevBuf<float2> samp_ws;   // samples in tile order [batches][Mtot]
+    std::map<int, cufftHandle> fft_plans;   // batch -> plan
+
+    ~NufftPlan();
+};
+
+// ------------------------------------------------ host-side operations ----
+
+void plan_init(NufftPlan &p, int D, const uint64_t *N, const uint64_t *mos, float W,
+               uint32_t flags);
+void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
+                     const uint64_t *frame_offsets, gb_prep_mode mode, cudaStream_t st);
+void plan_build_work(NufftPlan &p, cudaStream_t st);
+cufftHandle plan_fft(NufftPlan &p, int batches, cudaStream_t st);
+
+// Sample-array layout flags for the convolution kernels.
+enum SampleLayout { LAYOUT_ORIGINAL = 0, LAYOUT_SORTED = 1 };
+
+// Degridding: grid [nb][F][G] -> samples.  sign_fold multiplies the weight of
+// grid cell g by (-1)^(sum g) (the centring checkerboard after the FFT).
+// dcw (original sample order, may be null) multiplies the output, dcw_pow
+// times (1 or 2).
+void launch_degrid(NufftPlan &p, const float2 *grid, float2 *samples, int nb,
+                   SampleLayout layout, const float *dcw, int dcw_pow, bool sign_fold,
+                   bool accumulate, cudaStream_t st);
+
+// Gridding: samples -> grid [nb][F][G] (overwritten unless accumulate).
+// dcw multiplies the input samples (may be null).
+void launch_grid(NufftPlan &p, const float2 *samples, float2 *grid, int nb,
+                 SampleLayout layout, const float *dcw, bool sign_fold, bool accumulate,
+                 cudaStream_t st);
+
+// Trajectory gradient from a k-space grid (sign folded like the degridder).
+void launch_traj_grad(NufftPlan &p, const float2 *grid, const float2 *weights, int nb,
+                      const float *dcw, float *grad, bool sign_fold, cudaStream_t st);
+
+// Image-side fused kernels.
+// Forward: dst_os[b][f][interior] = src[...] * (csm) * deap * sign * scale.
+//   csm == null: src [nb][F][NN] -> dst [nb][F][G]
+//   csm != null: src [F][NN], csm [C][NN] -> dst [C][F][G] (nb = C)
+void launch_pad_forward(NufftPlan &p, const float2 *src, const float2 *csm, float2 *dst,
+                        int nb, bool src_oversampled, cudaStream_t st);
+// Adjoint: dst[...] (+)= crop(grid) * deap * sign * scale (* conj(csm) summed over coils)
+//   csm == null: grid [nb][F][G] -> dst [nb][F][NN] (or [nb][F][G] when dst_oversampled)
+//   csm != null: grid [C][F][G] -> dst [F][NN]
+void launch_crop_adjoint(NufftPlan &p, const float2 *grid, const float2 *csm, float2 *dst,
+                         int nb, bool dst_oversampled, bool accumulate, float weight,
+                         bool fourier_deapod, cudaStream_t st);
+
+// Reference-form utilities (NFFT_plan::fft / deapodize on oversampled arrays).
+void launch_timeswitch_scale(NufftPlan &p, float2 *data, int nbf, float scale, cudaStream_t st);
+void launch_deapodize_os(NufftPlan &p, float2 *data, int nbf, cudaStream_t st);
+void launch_multiply_dcw(const float *dcw, float2 *data, int64_t M, int nb, cudaStream_t st);
+
+// ------------------------------------------------------- device helpers ---
+
+__host__ __device__ __forceinline__ float bessi0f_ref(float x) {
+    // Rational approximation of I0 used by the reference kernel
+    // (toolboxes/nfft/ConvolutionKernel.hpp:39-68), same coefficients and
+    // evaluation order.
+    if (x == 0.0f) return 1.0f;
+    float z = x * x;
+    float numerator = (z * (z * (z * (z * (z * (z * (z * (z * (z * (z * (z * (z * (z *
+                       (z * 0.210580722890567e-22f + 0.380715242345326e-19f) +
+                       0.479440257548300e-16f) + 0.435125971262668e-13f) +
+                       0.300931127112960e-10f) + 0.160224679395361e-7f) +
+                       0.654858370096785e-5f) + 0.202591084143397e-2f) +
+                       0.463076284721000e0f) + 0.754337328948189e2f) +
+                       0.830792541809429e4f) + 0.571661130563785e6f) +
+                       0.216415572361227e8f) + 0.356644482244025e9f) +
+                       0.144048298227235e10f);
+    float denominator = (z * (z * (z - 0.307646912682801e4f) + 0.347626332405882e7f) -
+                         0.144048298227235e10f);
+    return -numerator / denominator;
+}
+
+// d/dz of the rational function R(z) = -num(z)/den(z) that bessi0f_ref
+// evaluates at z = x^2 (derivative of the same approximation, so finite
+// differences of the forward operator agree with it).
+__host__ __device__ __forceinline__ float bessi0_dRdz(float z) {
+    const float a[15] = {0.144048298227235e10f, 0.356644482244025e9f, 0.216415572361227e8f,
+                         0.571661130563785e6f,  0.830792541809429e4f, 0.754337328948189e2f,
+                         0.463076284721000e0f,  0.202591084143397e-2f, 0.654858370096785e-5f,
+                         0.160224679395361e-7f, 0.300931127112960e-10f, 0.435125971262668e-13f,
+                         0.479440257548300e-16f, 0.380715242345326e-19f, 0.210580722890567e-22f};
+    float num = a[14], dnum = 0.f;
+    for (int i = 13; i >= 0; --i) {
+        dnum = dnum * z + num;
+        num = num * z + a[i];
+    }
+    // den(z) = z^3 - 3076.46912682801 z^2 + 3476263.32405882 z - 1.44048298227235e9
+    const float b2 = -0.307646912682801e4f, b1 = 0.347626332405882e7f, b0 = -0.144048298227235e10f;
+    float den = ((z + b2) * z + b1) * z + b0;
+    float dden = (3.f * z + 2.f * b2) * z + b1;
+    // R = -num/den ; R' = -(num' den - num den') / den^2
+    return -(dnum * den - num * dden) / (den * den);
+}
+
+// One-dimensional Kaiser-Bessel value in the reference's arithmetic
+// (toolboxes/nfft/ConvolutionKernel.hpp:85-94), zero beyond the radius
+// (ConvolutionKernel.hpp:164-170).  Non-finite values are returned as 0: the
+// reference drops a tap whose product weight is not finite
+// (ConvolverC2NC.cuh:96-97, ConvolverNC2C_standard.cuh:266-268).
+__device__ __forceinline__ float kb_weight_1d(float delta, float mos_f, float one_over_W,
+                                              float beta, float radius) {
+    if (delta > radius) return 0.f;
+    float _tmp = 2.0f * delta * one_over_W;
+    float tmp = _tmp * _tmp;
+    float arg = beta * sqrtf(1.0f - tmp);
+    float bessi = bessi0f_ref(arg);
+    float w = mos_f * bessi * one_over_W;
+    return isfinite(w) ? w : 0.f;
+}
+
+// d/d(delta) of the 1D kernel for delta in [0, radius]:
+//   phi(u) = mos/W * R(beta^2 (1 - (2u/W)^2))
+//   phi'(u) = -(8 mos beta^2 u / W^3) * R'(z)
+__device__ __forceinline__ float kb_deriv_1d(float delta, float mos_f, float one_over_W,
+                                             float beta, float radius) {
+    if (delta > radius) return 0.f;
+    float t = 2.0f * delta * one_over_W;
+    float z = beta * beta * (1.0f - t * t);
+    if (!(z >= 0.f)) return 0.f;
+    float ow3 = one_over_W * one_over_W * one_over_W;
+    float d = -8.0f * mos_f * beta * beta * delta * ow3 * bessi0_dRdz(z);
+    return isfinite(d) ? d : 0.f;
+}
+
+__host__ __device__ __forceinline__ int wrapmod(int x, int m) {
+    int r = x % m;
+    return r < 0 ? r + m : r;
+}
+
+}  // namespace gb

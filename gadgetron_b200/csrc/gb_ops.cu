@@ -1,0 +1,566 @@
+// NUFFT plan operations (compute / mult_MH_M / convolve / fft / deapodize /
+// trajectory gradient), the non-Cartesian SENSE operator and the CG solver.
+//
+// Reference call sequences restated (paths relative to the Gadgetron tree):
+//   NFFT_plan::compute          toolboxes/nfft/NFFT.hpp:105-240
+//   NFFT_plan::mult_MH_M        toolboxes/nfft/NFFT.hpp:90-102
+//   cuNonCartesianSenseOperator toolboxes/mri/pmri/gpu/cuNonCartesianSenseOperator.cu:14-90
+//   cgSolver                    toolboxes/solvers/cgSolver.h:105-390
+//   relativeResidualTCB         toolboxes/solvers/cgCallback.h:56-104
+//   cgPreconditioner            toolboxes/solvers/cgPreconditioner.h:24-39
+//
+// The CG solver keeps every scalar on the device: dot products and norms are
+// accumulated in FP64 (per-block partials summed in a fixed order by the last
+// block, so results are reproducible), alpha/beta are computed on the device,
+// and no host synchronisation happens between iterations.  The whole solve
+// can be captured into one CUDA graph and replayed.
+#include <cmath>
+#include <cstring>
+
+#include "gb_internal.cuh"
+#include "gb_ops.hpp"
+
+namespace gb {
+
+// ----------------------------------------------------------- workspaces ---
+
+float2 *ensure_img_os(NufftPlan &p, int64_t nbf, cudaStream_t st) {
+    const size_t need = (size_t)nbf * p.kp.G;
+    const bool re = p.img_os.ensure(need);
+    if (re || p.img_os_dirty || p.img_os_batches_zeroed < (size_t)nbf) {
+        GB_CUDA(cudaMemsetAsync(p.img_os.get(), 0, p.img_os.n * sizeof(float2), st));
+        p.img_os_batches_zeroed = p.img_os.n / p.kp.G;
+        p.img_os_dirty = false;
+    }
+    return p.img_os.get();
+}
+
+float2 *ensure_kgrid(NufftPlan &p, int64_t nbf) {
+    p.kgrid.ensure((size_t)nbf * p.kp.G);
+    return p.kgrid.get();
+}
+
+float2 *ensure_samp(NufftPlan &p, int nb) {
+    p.samp_ws.ensure((size_t)nb * p.Mtot);
+    return p.samp_ws.get();
+}
+
+static void exec_fft(NufftPlan &p, float2 *in, float2 *out, int nbf, int dir, cudaStream_t st) {
+    cufftHandle h = plan_fft(p, nbf, st);
+    GB_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex *>(in), reinterpret_cast<cufftComplex *>(out), dir));
+}
+
+// Forward NUFFT into device sample buffer (layout chosen by caller).
+// csm != null: image [F][NN] and nb = coils.
+void nufft_forward(NufftPlan &p, const float2 *img, const float2 *csm, int nb, bool img_os,
+                   float2 *samples, SampleLayout layout, const float *dcw, int dcw_pow,
+                   bool accumulate, cudaStream_t st) {
+    const int64_t nbf = (int64_t)nb * p.F;
+    float2 *pad = ensure_img_os(p, nbf, st);
+    float2 *kg = ensure_kgrid(p, nbf);
+    launch_pad_forward(p, img, csm, pad, nb, img_os, st);
+    if (img_os) p.img_os_dirty = true;
+    exec_fft(p, pad, kg, (int)nbf, CUFFT_FORWARD, st);
+    launch_degrid(p, kg, samples, nb, layout, dcw, dcw_pow, true, accumulate, st);
+}
+
+// Adjoint NUFFT from samples.  csm != null: out image [F][NN], nb = coils.
+void nufft_adjoint(NufftPlan &p, const float2 *samples, SampleLayout layout, const float *dcw,
+                   const float2 *csm, int nb, float2 *img, bool img_os, bool accumulate, float weight,
+                   int fft_dir, cudaStream_t st) {
+    const int64_t nbf = (int64_t)nb * p.F;
+    float2 *kg = ensure_kgrid(p, nbf);
+    launch_grid(p, samples, kg, nb, layout, dcw, true, false, st);
+    exec_fft(p, kg, kg, (int)nbf, fft_dir, st);
+    launch_crop_adjoint(p, kg, csm, img, nb, img_os, accumulate, weight, fft_dir == CUFFT_FORWARD, st);
+}
+
+// Normal operator A^H W^2 A on images (csm optional), samples stay in tile order.
+void nufft_normal(NufftPlan &p, const float2 *img, const float2 *csm, int nb, const float *dcw,
+                  float2 *out, bool accumulate, float weight, cudaStream_t st) {
+    float2 *samp = ensure_samp(p, nb);
+    nufft_forward(p, img, csm, nb, false, samp, LAYOUT_SORTED, dcw, 2, false, st);
+    nufft_adjoint(p, samp, LAYOUT_SORTED, nullptr, csm, nb, out, false, accumulate, weight, CUFFT_INVERSE, st);
+}
+
+void nufft_compute(NufftPlan &p, const void *in, void *out, const float *dcw, gb_comp_mode mode,
+                   int nb, bool image_os, cudaStream_t st) {
+    if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "NFFT_plan::compute: preprocess has not been called");
+    if (!in || !out) fail(GB_ERR_INVALID_ARGUMENT, "NULL input/output");
+    if (nb <= 0) fail(GB_ERR_INVALID_ARGUMENT, "number of batches must be positive");
+    const float2 *ci = static_cast<const float2 *>(in);
+    float2 *co = static_cast<float2 *>(out);
+    switch (mode) {
+        case GB_FORWARDS_C2NC:
+            nufft_forward(p, ci, nullptr, nb, image_os, co, LAYOUT_ORIGINAL, dcw, 1, false, st);
+            break;
+        case GB_BACKWARDS_NC2C:
+            nufft_adjoint(p, ci, LAYOUT_ORIGINAL, dcw, nullptr, nb, co, image_os, false, 1.f, CUFFT_INVERSE, st);
+            break;
+        case GB_FORWARDS_NC2C:
+            nufft_adjoint(p, ci, LAYOUT_ORIGINAL, dcw, nullptr, nb, co, image_os, false, 1.f, CUFFT_FORWARD, st);
+            break;
+        default:
+            fail(GB_ERR_INVALID_ARGUMENT, "BACKWARDS_C2NC is not supported (the reference form passes swapped arguments)");
+    }
+}
+
+void nufft_mult_MH_M(NufftPlan &p, const void *in, void *out, const float *dcw, int nb, cudaStream_t st) {
+    if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "NFFT_plan::mult_MH_M: preprocess has not been called");
+    if (!in || !out) fail(GB_ERR_INVALID_ARGUMENT, "NULL input/output");
+    nufft_normal(p, static_cast<const float2 *>(in), nullptr, nb, dcw, static_cast<float2 *>(out), false, 1.f, st);
+}
+
+void nufft_convolve(NufftPlan &p, const void *in, void *out, gb_conv_mode mode, bool accumulate, int nb,
+                    cudaStream_t st) {
+    if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "NFFT_plan::convolve: preprocess has not been called");
+    if (!in || !out) fail(GB_ERR_INVALID_ARGUMENT, "NULL input/output");
+    if (mode == GB_CONV_C2NC)
+        launch_degrid(p, static_cast<const float2 *>(in), static_cast<float2 *>(out), nb, LAYOUT_ORIGINAL,
+                      nullptr, 1, false, accumulate, st);
+    else
+        launch_grid(p, static_cast<const float2 *>(in), static_cast<float2 *>(out), nb, LAYOUT_ORIGINAL,
+                    nullptr, false, accumulate, st);
+}
+
+void nufft_fft(NufftPlan &p, void *data, gb_fft_mode mode, bool do_scale, int nbf, cudaStream_t st) {
+    if (!data || nbf <= 0) fail(GB_ERR_INVALID_ARGUMENT, "invalid fft arguments");
+    float2 *d = static_cast<float2 *>(data);
+    launch_timeswitch_scale(p, d, nbf, 1.f, st);
+    exec_fft(p, d, d, nbf, mode == GB_FFT_FORWARDS ? CUFFT_FORWARD : CUFFT_INVERSE, st);
+    launch_timeswitch_scale(p, d, nbf, do_scale ? (float)(1.0 / std::sqrt((double)p.kp.G)) : 1.f, st);
+}
+
+void nufft_deapodize(NufftPlan &p, void *data, int nbf, cudaStream_t st) {
+    if (!data || nbf <= 0) fail(GB_ERR_INVALID_ARGUMENT, "invalid deapodize arguments");
+    launch_deapodize_os(p, static_cast<float2 *>(data), nbf, st);
+}
+
+void nufft_traj_grad(NufftPlan &p, const float2 *img, const float2 *weights, const float *dcw, float *grad,
+                     int nb, cudaStream_t st) {
+    if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
+    const int64_t nbf = (int64_t)nb * p.F;
+    float2 *pad = ensure_img_os(p, nbf, st);
+    float2 *kg = ensure_kgrid(p, nbf);
+    launch_pad_forward(p, img, nullptr, pad, nb, false, st);
+    exec_fft(p, pad, kg, (int)nbf, CUFFT_FORWARD, st);
+    launch_traj_grad(p, kg, weights, nb, dcw, grad, true, st);
+}
+
+void nufft_traj_grad_from_grid(NufftPlan &p, const float2 *grid, const float2 *weights, float *grad, int nb,
+                               cudaStream_t st) {
+    if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
+    launch_traj_grad(p, grid, weights, nb, nullptr, grad, false, st);
+}
+
+// ---------------------------------------------------------------- SENSE ---
+
+void sense_mult_M(SenseOp &s, const void *in, void *out, bool accumulate, cudaStream_t st) {
+    if (!in || !out) fail(GB_ERR_INVALID_ARGUMENT, "cuNonCartesianSenseOperator::mult_M : 0x0 input/output not accepted");
+    if (!s.csm) fail(GB_ERR_INVALID_ARGUMENT, "csm not set");
+    if (!s.plan.prepped) fail(GB_ERR_NOT_PREPROCESSED, "operator not preprocessed");
+    nufft_forward(s.plan, static_cast<const float2 *>(in), s.csm, s.ncoils, false, static_cast<float2 *>(out),
+                  LAYOUT_ORIGINAL, s.dcw, 1, accumulate, st);
+}
+
+void sense_mult_MH(SenseOp &s, const void *in, void *out, bool accumulate, cudaStream_t st) {
+    if (!in || !out) fail(GB_ERR_INVALID_ARGUMENT, "cuNonCartesianSenseOperator::mult_MH : 0x0 input/output not accepted");
+    if (!s.csm) fail(GB_ERR_INVALID_ARGUMENT, "csm not set");
+    if (!s.plan.prepped) fail(GB_ERR_NOT_PREPROCESSED, "operator not preprocessed");
+    nufft_adjoint(s.plan, static_cast<const float2 *>(in), LAYOUT_ORIGINAL, s.dcw, s.csm, s.ncoils,
+                  static_cast<float2 *>(out), false, accumulate, 1.f, CUFFT_INVERSE, st);
+}
+
+void sense_mult_MH_M(SenseOp &s, const void *in, void *out, bool accumulate, cudaStream_t st) {
+    if (!in || !out) fail(GB_ERR_INVALID_ARGUMENT, "NULL input/output");
+    if (!s.csm) fail(GB_ERR_INVALID_ARGUMENT, "csm not set");
+    if (!s.plan.prepped) fail(GB_ERR_NOT_PREPROCESSED, "operator not preprocessed");
+    nufft_normal(s.plan, static_cast<const float2 *>(in), s.csm, s.ncoils, s.dcw, static_cast<float2 *>(out),
+                 accumulate, 1.f, st);
+}
+
+// ------------------------------------------------------------------- CG ---
+
+// Device scalar block.
+struct CgScalars {
+    double rq, rq0, alpha_re, alpha_im, beta, pq_re, pq_im, tol;
+    int done, iters, hist_base, pad;
+    unsigned int ctr_dot, ctr_upd, ctr_init, ctr_pad;
+};
+
+constexpr int kDotBlocks = 296;
+
+__device__ __forceinline__ double2 block_reduce_d2(double2 v, double2 *sh) {
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : make_double2(0.0, 0.0);
+        for (int o = 16; o > 0; o >>= 1) {
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+        }
+    }
+    return v;
+}
+
+// Returns true in every thread of the last block to finish; that block then
+// holds the ordered sum of all block partials in `total`.
+__device__ bool last_block_sum(double2 mine, double2 *partials, unsigned int *ctr, double2 *total) {
+    __shared__ double2 sh[32];
+    __shared__ int s_last;
+    double2 v = block_reduce_d2(mine, sh);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = v;
+        __threadfence();
+        const unsigned int old = atomicAdd(ctr, 1u);
+        s_last = (old == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+    double2 acc = make_double2(0.0, 0.0);
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+        const double2 q = __ldcg(&partials[b]);
+        acc.x += q.x;
+        acc.y += q.y;
+    }
+    __syncthreads();
+    acc = block_reduce_d2(acc, sh);
+    if (threadIdx.x == 0) *ctr = 0u;
+    *total = acc;
+    return true;
+}
+
+// q = weight * crop(...) + kappa * p, then <p, q> -> alpha = rq / <p, q>.
+__global__ void k_cg_crop_dot(KParams k, const float *deap, int deap_stride, float scale,
+                              const float2 *__restrict__ grid, const float2 *__restrict__ csm, int nb, int F,
+                              const float2 *__restrict__ p, float2 *__restrict__ q, float weight, float kappa,
+                              CgScalars *S, double2 *partials) {
+    if (S->done) return;
+    const int64_t total = (int64_t)F * k.NN;
+    const int ox = (k.mos[0] - k.N[0]) >> 1, oy = (k.mos[1] - k.N[1]) >> 1, oz = (k.mos[2] - k.N[2]) >> 1;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int f = (int)(e / k.NN);
+        const int64_t n = e - (int64_t)f * k.NN;
+        const int x = (int)(n % k.N[0]);
+        const int y = (int)((n / k.N[0]) % k.N[1]);
+        const int z = (int)(n / ((int64_t)k.N[0] * k.N[1]));
+        const int gx = x + ox, gy = y + oy, gz = z + oz;
+        const int64_t g = ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + gx;
+        float fac = deap[x];
+        if (k.D > 1) fac *= deap[deap_stride + y];
+        if (k.D > 2) fac *= deap[2 * deap_stride + z];
+        if ((gx + gy + gz) & 1) fac = -fac;
+        fac *= scale * weight;
+        float2 s = make_float2(0.f, 0.f);
+        for (int b = 0; b < nb; b++) {
+            const float2 v = grid[((int64_t)b * F + f) * k.G + g];
+            const float2 c = csm[(int64_t)b * k.NN + n];
+            const float vr = v.x * fac, vi = v.y * fac;
+            s.x += vr * c.x + vi * c.y;
+            s.y += vi * c.x - vr * c.y;
+        }
+        const float2 pv = p[e];
+        s.x += kappa * pv.x;
+        s.y += kappa * pv.y;
+        q[e] = s;
+        // conj(p) * q
+        acc.x += (double)pv.x * s.x + (double)pv.y * s.y;
+        acc.y += (double)pv.x * s.y - (double)pv.y * s.x;
+    }
+    double2 tot;
+    if (last_block_sum(acc, partials, &S->ctr_dot, &tot) && threadIdx.x == 0) {
+        S->pq_re = tot.x;
+        S->pq_im = tot.y;
+        const double den = tot.x * tot.x + tot.y * tot.y;
+        // alpha = rq / pq  (rq real)
+        S->alpha_re = S->rq * tot.x / den;
+        S->alpha_im = -S->rq * tot.y / den;
+    }
+}
+
+// x += alpha p ; r -= alpha q ; rq' = Re<r, P^2 r> ; beta = rq'/rq ; stop rule.
+__global__ void k_cg_update(int64_t n, float2 *__restrict__ x, float2 *__restrict__ r,
+                            const float2 *__restrict__ p, const float2 *__restrict__ q,
+                            const float *__restrict__ P, int64_t Pn, CgScalars *S, double2 *partials,
+                            double *hist) {
+    if (S->done) return;
+    const float ar = (float)S->alpha_re, ai = (float)S->alpha_im;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const float2 pv = p[e], qv = q[e];
+        float2 xv = x[e], rv = r[e];
+        xv.x += ar * pv.x - ai * pv.y;
+        xv.y += ar * pv.y + ai * pv.x;
+        rv.x -= ar * qv.x - ai * qv.y;
+        rv.y -= ar * qv.y + ai * qv.x;
+        x[e] = xv;
+        r[e] = rv;
+        float w2 = 1.f;
+        if (P) { const float w = P[e % Pn]; w2 = w * w; }
+        acc.x += (double)rv.x * (double)(rv.x * w2) + (double)rv.y * (double)(rv.y * w2);
+    }
+    double2 tot;
+    if (last_block_sum(acc, partials, &S->ctr_upd, &tot) && threadIdx.x == 0) {
+        const double rq_new = tot.x;
+        S->beta = rq_new / S->rq;
+        S->rq = rq_new;
+        const double metric = rq_new / S->rq0;
+        if (hist) hist[S->hist_base + S->iters] = metric;
+        S->iters += 1;
+        if (metric < S->tol) S->done = 1;
+    }
+}
+
+// p = beta p + P^2 r
+__global__ void k_cg_pupdate(int64_t n, float2 *__restrict__ p, const float2 *__restrict__ r,
+                             const float *__restrict__ P, int64_t Pn, const CgScalars *S) {
+    const float b = (float)S->beta;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        float2 rv = r[e];
+        if (P) { const float w = P[e % Pn]; const float w2 = w * w; rv.x *= w2; rv.y *= w2; }
+        float2 pv = p[e];
+        p[e] = make_float2(b * pv.x + rv.x, b * pv.y + rv.y);
+    }
+}
+
+// Initialisation: r = rhs - q (q optional), p = P^2 r, rq = Re<r, p>;
+// set_rq0 also records rq0 and clears the iteration state.
+__global__ void k_cg_init(int64_t n, const float2 *__restrict__ rhs, const float2 *__restrict__ q,
+                          float2 *__restrict__ x, const float2 *__restrict__ x0, float2 *__restrict__ r,
+                          float2 *__restrict__ p, const float *__restrict__ P, int64_t Pn, CgScalars *S,
+                          double2 *partials, int set_rq0, double tol, int hist_base) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        float2 rv = rhs[e];
+        if (q) { const float2 qv = q[e]; rv.x -= qv.x; rv.y -= qv.y; }
+        r[e] = rv;
+        float w2 = 1.f;
+        if (P) { const float w = P[e % Pn]; w2 = w * w; }
+        const float2 pv = make_float2(rv.x * w2, rv.y * w2);
+        p[e] = pv;
+        if (set_rq0) x[e] = x0 ? x0[e] : make_float2(0.f, 0.f);
+        acc.x += (double)rv.x * pv.x + (double)rv.y * pv.y;
+    }
+    double2 tot;
+    if (last_block_sum(acc, partials, &S->ctr_init, &tot) && threadIdx.x == 0) {
+        S->rq = tot.x;
+        if (set_rq0) {
+            S->rq0 = tot.x;
+            S->done = 0;
+            S->iters = 0;
+            S->tol = tol;
+            S->hist_base = hist_base;
+        }
+    }
+}
+
+// Refinement bookkeeping in FP64: x64 += x (delta); rhs = rhs0 - q in double.
+__global__ void k_refine_accumulate(int64_t n, double2 *__restrict__ x64, const float2 *__restrict__ dx,
+                                    float2 *__restrict__ xf) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        double2 v = x64[e];
+        const float2 d = dx[e];
+        v.x += d.x;
+        v.y += d.y;
+        x64[e] = v;
+        xf[e] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
+__global__ void k_refine_residual(int64_t n, const float2 *__restrict__ rhs0, const float2 *__restrict__ q,
+                                  float2 *__restrict__ rhs) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const float2 a = rhs0[e], b = q[e];
+        rhs[e] = make_float2((float)((double)a.x - (double)b.x), (float)((double)a.y - (double)b.y));
+    }
+}
+
+__global__ void k_copy_f2(int64_t n, const float2 *__restrict__ a, float2 *__restrict__ b) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        b[e] = a[e];
+}
+
+static unsigned blocks_for(int64_t n) {
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, kDotBlocks));
+}
+
+CgSolver::~CgSolver() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+}
+
+// E^H E p -> q with the fused crop/dot kernel (used inside the iteration).
+static void cg_normal_dot(CgSolver &cg, cudaStream_t st) {
+    SenseOp &s = *cg.E;
+    NufftPlan &p = s.plan;
+    const int nb = s.ncoils;
+    const int64_t nbf = (int64_t)nb * p.F;
+    float2 *samp = ensure_samp(p, nb);
+    nufft_forward(p, cg.p.get(), s.csm, nb, false, samp, LAYOUT_SORTED, s.dcw, 2, false, st);
+    float2 *kg = ensure_kgrid(p, nbf);
+    launch_grid(p, samp, kg, nb, LAYOUT_SORTED, nullptr, true, false, st);
+    exec_fft(p, kg, kg, (int)nbf, CUFFT_INVERSE, st);
+    const int64_t n = (int64_t)p.F * p.kp.NN;
+    k_cg_crop_dot<<<blocks_for(n), 256, 0, st>>>(p.kp, p.deap_img.get(), p.maxN,
+                                                 (float)(1.0 / std::sqrt((double)p.kp.G)), kg, s.csm, nb,
+                                                 (int)p.F, cg.p.get(), cg.q.get(), cg.weight, cg.kappa, cg.S.get(),
+                                                 cg.partials.get());
+    GB_CUDA(cudaGetLastError());
+}
+
+static void cg_iteration(CgSolver &cg, cudaStream_t st, double *hist) {
+    NufftPlan &p = cg.E->plan;
+    const int64_t n = (int64_t)p.F * p.kp.NN;
+    cg_normal_dot(cg, st);
+    k_cg_update<<<blocks_for(n), 256, 0, st>>>(n, cg.x.get(), cg.r.get(), cg.p.get(), cg.q.get(), cg.precond, n,
+                                                cg.S.get(), cg.partials.get(), hist);
+    GB_CUDA(cudaGetLastError());
+    k_cg_pupdate<<<blocks_for(n), 256, 0, st>>>(n, cg.p.get(), cg.r.get(), cg.precond, n, cg.S.get());
+    GB_CUDA(cudaGetLastError());
+}
+
+// Applies E^H E (with weight and kappa) to `in` into `out` without the dot.
+static void cg_apply_normal(CgSolver &cg, const float2 *in, float2 *out, cudaStream_t st) {
+    SenseOp &s = *cg.E;
+    nufft_normal(s.plan, in, s.csm, s.ncoils, s.dcw, out, false, cg.weight, st);
+}
+
+// One full solve of E^H E x = rhs (device rhs) from x0 (optional) into cg.x.
+static void cg_solve_once(CgSolver &cg, const float2 *rhs, const float2 *x0, double *hist, int hist_base,
+                          cudaStream_t st) {
+    NufftPlan &p = cg.E->plan;
+    const int64_t n = (int64_t)p.F * p.kp.NN;
+    k_cg_init<<<blocks_for(n), 256, 0, st>>>(n, rhs, nullptr, cg.x.get(), x0, cg.r.get(), cg.p.get(), cg.precond,
+                                              n, cg.S.get(), cg.partials.get(), 1, (double)cg.tol, hist_base);
+    GB_CUDA(cudaGetLastError());
+    if (x0) {
+        cg_apply_normal(cg, x0, cg.q.get(), st);
+        k_cg_init<<<blocks_for(n), 256, 0, st>>>(n, cg.r.get(), cg.q.get(), cg.x.get(), x0, cg.r.get(), cg.p.get(),
+                                                  cg.precond, n, cg.S.get(), cg.partials.get(), 0, (double)cg.tol,
+                                                  hist_base);
+        GB_CUDA(cudaGetLastError());
+    }
+    for (uint32_t it = 0; it < cg.iterations; it++) cg_iteration(cg, st, hist);
+}
+
+static void cg_prepare(CgSolver &cg, cudaStream_t st) {
+    SenseOp &s = *cg.E;
+    NufftPlan &p = s.plan;
+    const int64_t n = (int64_t)p.F * p.kp.NN;
+    const int nb = s.ncoils;
+    cg.x.ensure(n);
+    cg.r.ensure(n);
+    cg.p.ensure(n);
+    cg.q.ensure(n);
+    cg.rhs0.ensure(n);
+    cg.rhs.ensure(n);
+    cg.partials.ensure(kDotBlocks);
+    if (cg.S.ensure(1)) GB_CUDA(cudaMemsetAsync(cg.S.get(), 0, sizeof(CgScalars), st));
+    if (cg.refinements > 1) cg.x64.ensure(n);
+    // Workspaces and FFT plans must exist before any graph capture.
+    ensure_img_os(p, (int64_t)nb * p.F, st);
+    ensure_kgrid(p, (int64_t)nb * p.F);
+    ensure_samp(p, nb);
+    plan_fft(p, nb * (int)p.F, st);
+    // Split-tile counters/partials for the gridding kernel.
+    launch_grid_prepare(p, nb, st);
+}
+
+static void cg_record(CgSolver &cg, const float2 *d, float2 *x_out, double *hist, cudaStream_t st) {
+    SenseOp &s = *cg.E;
+    NufftPlan &p = s.plan;
+    const int64_t n = (int64_t)p.F * p.kp.NN;
+    // rhs0 = weight * E^H d
+    nufft_adjoint(p, d, LAYOUT_ORIGINAL, s.dcw, s.csm, s.ncoils, cg.rhs0.get(), false, false, cg.weight,
+                  CUFFT_INVERSE, st);
+    if (cg.refinements <= 1) {
+        cg_solve_once(cg, cg.rhs0.get(), cg.x0, hist, 0, st);
+        k_copy_f2<<<blocks_for(n), 256, 0, st>>>(n, cg.x.get(), x_out);
+        GB_CUDA(cudaGetLastError());
+        return;
+    }
+    GB_CUDA(cudaMemsetAsync(cg.x64.get(), 0, n * sizeof(double2), st));
+    for (uint32_t k = 0; k < cg.refinements; k++) {
+        const float2 *rhs = cg.rhs0.get();
+        if (k > 0) {
+            cg_apply_normal(cg, x_out, cg.q.get(), st);
+            k_refine_residual<<<blocks_for(n), 256, 0, st>>>(n, cg.rhs0.get(), cg.q.get(), cg.rhs.get());
+            GB_CUDA(cudaGetLastError());
+            rhs = cg.rhs.get();
+        }
+        cg_solve_once(cg, rhs, (k == 0) ? cg.x0 : nullptr, hist, (int)(k * cg.iterations), st);
+        k_refine_accumulate<<<blocks_for(n), 256, 0, st>>>(n, cg.x64.get(), cg.x.get(), x_out);
+        GB_CUDA(cudaGetLastError());
+    }
+}
+
+void cg_solve(CgSolver &cg, const void *d, void *x_out, double *hist, uint32_t *iters_run, cudaStream_t st) {
+    if (!cg.E) fail(GB_ERR_INVALID_ARGUMENT, "Error: cgSolver::compute_rhs : no encoding operator is set");
+    if (!d || !x_out) fail(GB_ERR_INVALID_ARGUMENT, "NULL data or result");
+    SenseOp &s = *cg.E;
+    if (!s.csm) fail(GB_ERR_INVALID_ARGUMENT, "csm not set");
+    if (!s.plan.prepped) fail(GB_ERR_NOT_PREPROCESSED, "operator not preprocessed");
+    if (cg.kappa != 0.f && (cg.refinements > 1 || cg.x0))
+        fail(GB_ERR_INVALID_ARGUMENT, "identity regularisation cannot be combined with x0 or refinement");
+    NufftPlan &p = s.plan;
+    const int64_t n = (int64_t)p.F * p.kp.NN;
+    const float2 *dd = static_cast<const float2 *>(d);
+    float2 *xo = static_cast<float2 *>(x_out);
+    if (cg.iterations == 0) {
+        nufft_adjoint(p, dd, LAYOUT_ORIGINAL, s.dcw, s.csm, s.ncoils, xo, false, false, cg.weight, CUFFT_INVERSE, st);
+        if (iters_run) *iters_run = 0;
+        return;
+    }
+    cg_prepare(cg, st);
+    if (cg.use_graph) {
+        GraphKey key{d, x_out, hist, cg.iterations, cg.refinements, cg.x0, cg.precond, cg.kappa, cg.weight,
+                     cg.tol, s.csm, s.dcw, s.ncoils};
+        if (!cg.graph_exec || !(key == cg.graph_key)) {
+            cudaStream_t cs;
+            GB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+            GB_CUDA(cudaStreamSynchronize(st));
+            cudaGraph_t g;
+            GB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+            try {
+                cg_record(cg, dd, xo, hist, cs);
+            } catch (...) {
+                cudaGraph_t tmp;
+                cudaStreamEndCapture(cs, &tmp);
+                if (tmp) cudaGraphDestroy(tmp);
+                cudaStreamDestroy(cs);
+                throw;
+            }
+            GB_CUDA(cudaStreamEndCapture(cs, &g));
+            if (cg.graph_exec) {
+                cudaGraphExecUpdateResultInfo info;
+                if (cudaGraphExecUpdate(cg.graph_exec, g, &info) != cudaSuccess) {
+                    cudaGetLastError();
+                    cudaGraphExecDestroy(cg.graph_exec);
+                    cg.graph_exec = nullptr;
+                }
+            }
+            if (!cg.graph_exec) GB_CUDA(cudaGraphInstantiate(&cg.graph_exec, g, 0));
+            cudaGraphDestroy(g);
+            GB_CUDA(cudaStreamDestroy(cs));
+            // cuFFT plans were bound to the capture stream; rebind lazily.
+            cg.graph_key = key;
+        }
+        GB_CUDA(cudaGraphLaunch(cg.graph_exec, st));
+    } else {
+        cg_record(cg, dd, xo, hist, st);
+    }
+    CgScalars hs;
+    GB_CUDA(cudaMemcpyAsync(&hs, cg.S.get(), sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaStreamSynchronize(st));
+    if (iters_run) *iters_run = (uint32_t)(hs.hist_base + hs.iters);
+    (void)n;
+}
+
+}  // namespace gb

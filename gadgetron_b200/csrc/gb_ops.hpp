@@ -1,0 +1,85 @@
+// Host-side objects behind the C ABI: the SENSE operator and the CG solver,
+// plus the NUFFT operation entry points used by the ABI layer.
+#pragma once
+
+#include "gb_internal.cuh"
+
+namespace gb {
+
+struct SenseOp {
+    NufftPlan plan;
+    const float2 *csm = nullptr;
+    int ncoils = 0;
+    const float *dcw = nullptr;
+};
+
+struct GraphKey {
+    const void *d, *x;
+    const double *hist;
+    uint32_t iterations, refinements;
+    const float2 *x0;
+    const float *precond;
+    float kappa, weight, tol;
+    const float2 *csm;
+    const float *dcw;
+    int ncoils;
+    bool operator==(const GraphKey &o) const {
+        return d == o.d && x == o.x && hist == o.hist && iterations == o.iterations &&
+               refinements == o.refinements && x0 == o.x0 && precond == o.precond && kappa == o.kappa &&
+               weight == o.weight && tol == o.tol && csm == o.csm && dcw == o.dcw && ncoils == o.ncoils;
+    }
+};
+
+struct CgScalars;
+
+struct CgSolver {
+    SenseOp *E = nullptr;
+    float weight = 1.f;
+    uint32_t iterations = 10;      // cgSolver.h:51
+    float tol = 1e-3f;             // cgSolver.h:52
+    const float2 *x0 = nullptr;
+    const float *precond = nullptr;
+    float kappa = 0.f;
+    uint32_t refinements = 1;
+    bool use_graph = false;
+
+    DevBuf<float2> x, r, p, q, rhs0, rhs;
+    DevBuf<double2> x64, partials;
+    DevBuf<CgScalars> S;
+    cudaGraphExec_t graph_exec = nullptr;
+    GraphKey graph_key{};
+    ~CgSolver();
+};
+
+// NUFFT operations
+float2 *ensure_img_os(NufftPlan &p, int64_t nbf, cudaStream_t st);
+float2 *ensure_kgrid(NufftPlan &p, int64_t nbf);
+float2 *ensure_samp(NufftPlan &p, int nb);
+void launch_grid_prepare(NufftPlan &p, int nb, cudaStream_t st);
+void nufft_forward(NufftPlan &p, const float2 *img, const float2 *csm, int nb, bool img_os, float2 *samples,
+                   SampleLayout layout, const float *dcw, int dcw_pow, bool accumulate, cudaStream_t st);
+void nufft_adjoint(NufftPlan &p, const float2 *samples, SampleLayout layout, const float *dcw, const float2 *csm,
+                   int nb, float2 *img, bool img_os, bool accumulate, float weight, int fft_dir, cudaStream_t st);
+void nufft_normal(NufftPlan &p, const float2 *img, const float2 *csm, int nb, const float *dcw, float2 *out,
+                  bool accumulate, float weight, cudaStream_t st);
+void nufft_compute(NufftPlan &p, const void *in, void *out, const float *dcw, gb_comp_mode mode, int nb,
+                   bool image_os, cudaStream_t st);
+void nufft_mult_MH_M(NufftPlan &p, const void *in, void *out, const float *dcw, int nb, cudaStream_t st);
+void nufft_convolve(NufftPlan &p, const void *in, void *out, gb_conv_mode mode, bool accumulate, int nb,
+                    cudaStream_t st);
+void nufft_fft(NufftPlan &p, void *data, gb_fft_mode mode, bool do_scale, int nbf, cudaStream_t st);
+void nufft_deapodize(NufftPlan &p, void *data, int nbf, cudaStream_t st);
+void nufft_traj_grad(NufftPlan &p, const float2 *img, const float2 *weights, const float *dcw, float *grad,
+                     int nb, cudaStream_t st);
+void nufft_traj_grad_from_grid(NufftPlan &p, const float2 *grid, const float2 *weights, float *grad, int nb,
+                               cudaStream_t st);
+
+// SENSE
+void sense_mult_M(SenseOp &s, const void *in, void *out, bool accumulate, cudaStream_t st);
+void sense_mult_MH(SenseOp &s, const void *in, void *out, bool accumulate, cudaStream_t st);
+void sense_mult_MH_M(SenseOp &s, const void *in, void *out, bool accumulate, cudaStream_t st);
+
+// CG
+void cg_solve(CgSolver &cg, const void *d, void *x_out, double *hist, uint32_t *iters_run, cudaStream_t st);
+
+}  // namespace gb

@@ -1,0 +1,496 @@
+// Plan creation, trajectory preprocessing (scaling, tile binning, sorting),
+// deapodization tables and the cuFFT plan cache.
+//
+// Reference behaviour restated here:
+//   - size/width checks: toolboxes/nfft/gpu/cuGriddingConvolution.cu:56-85
+//   - trajectory range check and scaling k*mos + (mos+pad)/2:
+//     toolboxes/nfft/gpu/cuGriddingConvolution.cu:128-172,
+//     toolboxes/nfft/gpu/ConvolverNC2C_standard.cuh:25-39
+//   - deapodization filter = 1 / (unscaled centred FFT of the kernel sampled
+//     around mos/2): toolboxes/nfft/gpu/cuNFFT.cu:136-202.  The kernel is
+//     separable, so the transform is the product of 1D transforms; each is
+//     evaluated here in double on the host from the same float kernel values.
+//
+// What is new: instead of the reference's sort of (cell, sample) pairs
+// (M * W^D keys, ConvolverNC2C_standard.cuh:162-190 and
+// cuGriddingConvolution.cu:361-422) samples are binned by tile: one key per
+// sample for its home tile, plus one (tile, sample) pair per tile touched
+// (at most 2^D per sample) for the gridding lists.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "gb_internal.cuh"
+
+namespace gb {
+
+NufftPlan::~NufftPlan() {
+    for (auto &kv : fft_plans) cufftDestroy(kv.second);
+}
+
+static double host_kb1(float delta, const NufftPlan &p, int d) {
+    // Same float arithmetic as the device helper (host: no contraction).
+    const KParams &k = p.kp;
+    if (delta > k.radius) return 0.0;
+    float _tmp = 2.0f * delta * k.one_over_W;
+    float tmp = _tmp * _tmp;
+    float arg = k.beta[d] * std::sqrt(1.0f - tmp);
+    float bessi = bessi0f_ref(arg);
+    float w = k.mos_f[d] * bessi * k.one_over_W;
+    return std::isfinite(w) ? (double)w : 0.0;
+}
+
+void plan_init(NufftPlan &p, int D, const uint64_t *N, const uint64_t *mos, float W,
+               uint32_t flags) {
+    if (D < 1 || D > kMaxD) fail(GB_ERR_INVALID_ARGUMENT, "D must be 1, 2 or 3");
+    if (!N || !mos) fail(GB_ERR_INVALID_ARGUMENT, "NULL matrix size");
+    if (!(W >= 1.8f)) fail(GB_ERR_INVALID_ARGUMENT, "Kernel width must be equal to or larger than 1.8.");
+    if (W > 7.0f) fail(GB_ERR_INVALID_ARGUMENT, "Kernel width above 7 is not supported");
+    for (int d = 0; d < D; d++) {
+        if (N[d] == 0 || mos[d] == 0 || N[d] % 32 || mos[d] % 32)
+            fail(GB_ERR_INVALID_ARGUMENT, "Matrix size must be a multiple of 32.");
+        if (mos[d] < N[d])
+            fail(GB_ERR_INVALID_ARGUMENT, "Oversampled matrix size must be greater than or equal to matrix size.");
+        if (mos[d] > (1u << 20)) fail(GB_ERR_INVALID_ARGUMENT, "matrix size too large");
+    }
+    GB_CUDA(cudaGetDevice(&p.device));
+    p.D = D;
+    p.W = W;
+    p.flags = flags;
+    KParams &k = p.kp;
+    std::memset(&k, 0, sizeof(k));
+    k.D = D;
+    k.radius = W / 2.0f;
+    k.one_over_W = 1.0f / W;
+    k.hw = (int)std::ceil(k.radius);
+    k.G = 1;
+    k.NN = 1;
+    for (int d = 0; d < kMaxD; d++) {
+        p.N[d] = d < D ? (int64_t)N[d] : 1;
+        p.mos[d] = d < D ? (int64_t)mos[d] : 1;
+        k.mos[d] = (int)p.mos[d];
+        k.N[d] = (int)p.N[d];
+        k.mos_f[d] = (float)p.mos[d];
+        k.G *= p.mos[d];
+        k.NN *= p.N[d];
+        if (d < D) {
+            // beta per dimension in float (ConvolutionKernel.hpp:286-303), with
+            // os_factor = mos/N as the (N, mos, W) constructor computes it.
+            float os = (float)mos[d] / (float)N[d];
+            float w2 = W * W, os2 = os * os, h = os - 0.5f;
+            float arg = w2 / os2 * (h * h) - 0.8f;
+            k.beta[d] = (float)M_PI * std::sqrt(arg);
+        }
+    }
+    if (k.G > (int64_t)1 << 31) fail(GB_ERR_INVALID_ARGUMENT, "oversampled grid exceeds 2^31 cells");
+
+    // Default tiling: 2D 16x16, 3D 8x8x8, 1D 256; coil group 8.
+    Tiling &t = p.tiling;
+    if (D == 1) { t.tile[0] = 256; t.tile[1] = 1; t.tile[2] = 1; }
+    if (D == 2) { t.tile[0] = 16; t.tile[1] = 16; t.tile[2] = 1; }
+    if (D == 3) { t.tile[0] = 8; t.tile[1] = 8; t.tile[2] = 8; }
+    for (int d = 0; d < D; d++)
+        while (t.tile[d] > k.mos[d]) t.tile[d] >>= 1;
+    t.cg = 8;
+    for (int d = 0; d < kMaxD; d++) {
+        k.tile[d] = d < D ? t.tile[d] : 1;
+        k.ntiles[d] = d < D ? k.mos[d] / k.tile[d] : 1;
+    }
+    k.ntiles_total = k.ntiles[0] * k.ntiles[1] * k.ntiles[2];
+
+    // Deapodization tables.  psi_d(g) = sum_u phi_d(|u|) cos(2 pi (g - mos/2) u / mos)
+    // is the 1D unscaled centred transform of the kernel sampled at cells
+    // c = mos/2 + u (exactly what cuNFFT.cu:136-202 computes, per dimension).
+    p.maxN = 0;
+    p.maxmos = 0;
+    for (int d = 0; d < D; d++) {
+        p.maxN = std::max(p.maxN, (int)p.N[d]);
+        p.maxmos = std::max(p.maxmos, (int)p.mos[d]);
+    }
+    std::vector<float> h_img((size_t)D * p.maxN, 0.f), h_os((size_t)D * p.maxmos, 0.f);
+    for (int d = 0; d < D; d++) {
+        const int m = (int)p.mos[d];
+        std::vector<double> phi;
+        std::vector<int> us;
+        for (int c = 0; c < m; c++) {
+            float delta = std::fabs(0.5f * k.mos_f[d] - (float)c);
+            double v = host_kb1(delta, p, d);
+            if (v != 0.0) {
+                phi.push_back(v);
+                us.push_back(c - m / 2);
+            }
+        }
+        const int off = (int)((p.mos[d] - p.N[d]) >> 1);
+        for (int g = 0; g < m; g++) {
+            double s = 0.0;
+            for (size_t i = 0; i < phi.size(); i++)
+                s += phi[i] * std::cos(2.0 * M_PI * (double)(g - m / 2) * (double)us[i] / (double)m);
+            float inv = (float)(1.0 / s);
+            h_os[(size_t)d * p.maxmos + g] = inv;
+            int n = g - off;
+            if (n >= 0 && n < (int)p.N[d]) h_img[(size_t)d * p.maxN + n] = inv;
+        }
+    }
+    p.deap_img.ensure(h_img.size());
+    p.deap_os.ensure(h_os.size());
+    GB_CUDA(cudaMemcpy(p.deap_img.get(), h_img.data(), h_img.size() * sizeof(float), cudaMemcpyHostToDevice));
+    GB_CUDA(cudaMemcpy(p.deap_os.get(), h_os.data(), h_os.size() * sizeof(float), cudaMemcpyHostToDevice));
+}
+
+// ------------------------------------------------------------ kernels ----
+
+__device__ __forceinline__ int floor_div(int a, int b) {
+    int q = a / b;
+    return (a % b != 0 && ((a < 0) != (b < 0))) ? q - 1 : q;
+}
+
+__device__ __forceinline__ uint32_t frame_of(const int64_t *off, uint32_t F, int64_t j) {
+    uint32_t lo = 0, hi = F;   // find f with off[f] <= j < off[f+1]
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (off[mid] <= j) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// Scale the trajectory, check its range, and compute each sample's home key.
+__global__ void k_scale_bin(KParams k, const float *__restrict__ traj, int64_t M,
+                            const int64_t *__restrict__ frame_off, uint32_t F,
+                            float *__restrict__ pos, uint32_t *__restrict__ key,
+                            uint32_t *__restrict__ idx, int *__restrict__ range_err) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= M) return;
+    int tcoord[kMaxD] = {0, 0, 0};
+    bool bad = false;
+    for (int d = 0; d < k.D; d++) {
+        float kv = traj[j * k.D + d];
+        if (!(kv >= -0.5f && kv <= 0.5f)) bad = true;
+        // s = k*mos + (mos+pad)/2, the reference's trajectory_scale (evaluated
+        // on the device there, where the multiply-add is contracted).
+        float bias = (float)((k.mos[d] + 2 * k.hw) >> 1);
+        float s = fmaf(kv, k.mos_f[d], bias);
+        pos[(int64_t)d * M + j] = s;
+        float sp = s - (float)k.hw;
+        int c0 = (int)floorf(sp);
+        int t = floor_div(c0, k.tile[d]);
+        tcoord[d] = wrapmod(t, k.ntiles[d]);
+    }
+    if (bad) {
+        atomicOr(range_err, 1);
+        for (int d = 0; d < k.D; d++) tcoord[d] = 0;
+    }
+    uint32_t f = frame_of(frame_off, F, j);
+    uint32_t tile = (uint32_t)((tcoord[2] * k.ntiles[1] + tcoord[1]) * k.ntiles[0] + tcoord[0]);
+    key[j] = f * (uint32_t)k.ntiles_total + tile;
+    idx[j] = (uint32_t)j;
+}
+
+__global__ void k_gather_pos(int D, int64_t M, const float *__restrict__ pos,
+                             const uint32_t *__restrict__ perm, float *__restrict__ pos_sorted) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    uint32_t j = perm[i];
+    for (int d = 0; d < D; d++) pos_sorted[(int64_t)d * M + i] = pos[(int64_t)d * M + j];
+}
+
+__global__ void k_histogram(const uint32_t *__restrict__ keys, int64_t n, uint32_t *__restrict__ counts) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    atomicAdd(&counts[keys[i]], 1u);
+}
+
+// Tiles touched by the gridding footprint of sorted sample i (NC2C taps
+// [ceil(s - W/2), floor(s + W/2)] on the padded grid, folded by -pad/2 and
+// wrapped; ConvolverNC2C_standard.cuh:41-60,81-129 and :358-477).
+__device__ __forceinline__ int touched_tiles(const KParams &k, const float *s, int tl[kMaxD][3],
+                                             int nt[kMaxD]) {
+    int total = 1;
+    for (int d = 0; d < kMaxD; d++) {
+        if (d >= k.D) { tl[d][0] = 0; nt[d] = 1; continue; }
+        int lo = (int)ceilf(s[d] - k.radius) - k.hw;
+        int hi = (int)floorf(s[d] + k.radius) - k.hw;
+        int t0 = floor_div(lo, k.tile[d]);
+        int t1 = floor_div(hi, k.tile[d]);
+        int n = 0;
+        for (int t = t0; t <= t1 && n < 3; t++) {
+            int w = wrapmod(t, k.ntiles[d]);
+            bool dup = false;
+            for (int q = 0; q < n; q++) dup |= (tl[d][q] == w);
+            if (!dup) tl[d][n++] = w;
+        }
+        nt[d] = n;
+        total *= n;
+    }
+    return total;
+}
+
+__global__ void k_count_pairs(KParams k, int64_t M, const float *__restrict__ pos_sorted,
+                              uint32_t *__restrict__ cnt) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    float s[kMaxD] = {0.f, 0.f, 0.f};
+    for (int d = 0; d < k.D; d++) s[d] = pos_sorted[(int64_t)d * M + i];
+    int tl[kMaxD][3], nt[kMaxD];
+    cnt[i] = (uint32_t)touched_tiles(k, s, tl, nt);
+}
+
+__global__ void k_write_pairs(KParams k, int64_t M, const float *__restrict__ pos_sorted,
+                              const uint32_t *__restrict__ sorted_home_key,
+                              const uint32_t *__restrict__ pair_off,
+                              uint32_t *__restrict__ pkey, uint32_t *__restrict__ pval) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    float s[kMaxD] = {0.f, 0.f, 0.f};
+    for (int d = 0; d < k.D; d++) s[d] = pos_sorted[(int64_t)d * M + i];
+    int tl[kMaxD][3], nt[kMaxD];
+    touched_tiles(k, s, tl, nt);
+    uint32_t frame = sorted_home_key[i] / (uint32_t)k.ntiles_total;
+    uint32_t o = pair_off[i];
+    for (int a = 0; a < nt[2]; a++)
+        for (int b = 0; b < nt[1]; b++)
+            for (int c = 0; c < nt[0]; c++) {
+                uint32_t tile = (uint32_t)((tl[2][a] * k.ntiles[1] + tl[1][b]) * k.ntiles[0] + tl[0][c]);
+                pkey[o] = frame * (uint32_t)k.ntiles_total + tile;
+                pval[o] = (uint32_t)i;
+                o++;
+            }
+}
+
+template <class T>
+static void exclusive_scan(const T *in, T *out, int64_t n, cudaStream_t st) {
+    size_t bytes = 0;
+    GB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, st));
+    DevBuf<unsigned char> tmp;
+    tmp.ensure(bytes);
+    GB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, st));
+    GB_CUDA(cudaStreamSynchronize(st));
+}
+
+static void sort_pairs(uint32_t *keys_in, uint32_t *keys_out, uint32_t *vals_in,
+                       uint32_t *vals_out, int64_t n, int end_bit, cudaStream_t st) {
+    size_t bytes = 0;
+    GB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys_in, keys_out, vals_in, vals_out,
+                                            (int)n, 0, end_bit, st));
+    DevBuf<unsigned char> tmp;
+    tmp.ensure(bytes);
+    GB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, keys_in, keys_out, vals_in, vals_out,
+                                            (int)n, 0, end_bit, st));
+    GB_CUDA(cudaStreamSynchronize(st));
+}
+
+static int bits_for(uint64_t n) {
+    int b = 1;
+    while ((1ull << b) < n) b++;
+    return b;
+}
+
+void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
+                     const uint64_t *frame_offsets, gb_prep_mode mode, cudaStream_t st) {
+    if (!traj) fail(GB_ERR_INVALID_ARGUMENT, "NULL trajectory");
+    if (Mtot == 0 || F == 0) fail(GB_ERR_INVALID_ARGUMENT, "empty trajectory");
+    if (Mtot >= (1ull << 31)) fail(GB_ERR_INVALID_ARGUMENT, "too many samples (>= 2^31)");
+    if ((uint64_t)F * (uint64_t)p.kp.ntiles_total >= (1ull << 31))
+        fail(GB_ERR_INVALID_ARGUMENT, "too many frames for the tile grid");
+    std::vector<int64_t> off(F + 1);
+    if (frame_offsets) {
+        for (uint32_t f = 0; f <= F; f++) off[f] = (int64_t)frame_offsets[f];
+        if (off[0] != 0 || off[F] != (int64_t)Mtot)
+            fail(GB_ERR_INVALID_ARGUMENT, "frame offsets must start at 0 and end at the sample count");
+        for (uint32_t f = 0; f < F; f++)
+            if (off[f + 1] < off[f]) fail(GB_ERR_INVALID_ARGUMENT, "frame offsets must be non-decreasing");
+    } else {
+        if (Mtot % F) fail(GB_ERR_INVALID_ARGUMENT, "sample count is not a multiple of the frame count");
+        for (uint32_t f = 0; f <= F; f++) off[f] = (int64_t)(Mtot / F) * f;
+    }
+    p.prepped = false;
+    const KParams &k = p.kp;
+    const int64_t M = (int64_t)Mtot;
+    const int D = p.D;
+    const uint32_t nkeys = F * (uint32_t)k.ntiles_total;
+
+    DevBuf<int64_t> d_off;
+    d_off.ensure(F + 1);
+    GB_CUDA(cudaMemcpyAsync(d_off.get(), off.data(), (F + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    DevBuf<float> pos;
+    pos.ensure((size_t)D * M);
+    DevBuf<uint32_t> key, idx, key_sorted;
+    key.ensure(M);
+    idx.ensure(M);
+    key_sorted.ensure(M);
+    DevBuf<int> err;
+    err.ensure(1);
+    GB_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), st));
+    const int TB = 256;
+    k_scale_bin<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, traj, M, d_off.get(), F, pos.get(),
+                                                               key.get(), idx.get(), err.get());
+    GB_CUDA(cudaGetLastError());
+    int h_err = 0;
+    GB_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaStreamSynchronize(st));
+    if (h_err) fail(GB_ERR_TRAJECTORY_RANGE, "trajectory out of range [-1/2, 1/2]");
+
+    // Stable sort of samples by home key (frame, tile).
+    p.perm.ensure(M);
+    sort_pairs(key.get(), key_sorted.get(), idx.get(), p.perm.get(), M, bits_for(nkeys), st);
+    p.pos_sorted.ensure((size_t)D * M);
+    k_gather_pos<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(D, M, pos.get(), p.perm.get(),
+                                                                p.pos_sorted.get());
+    GB_CUDA(cudaGetLastError());
+
+    // Home ranges.
+    DevBuf<uint32_t> counts;
+    counts.ensure(nkeys + 1);
+    GB_CUDA(cudaMemsetAsync(counts.get(), 0, (nkeys + 1) * sizeof(uint32_t), st));
+    k_histogram<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(key_sorted.get(), M, counts.get());
+    GB_CUDA(cudaGetLastError());
+    p.home_off.ensure(nkeys + 1);
+    exclusive_scan(counts.get(), p.home_off.get(), (int64_t)nkeys + 1, st);
+
+    // Gridding pair lists.
+    DevBuf<uint32_t> pcnt, poff;
+    pcnt.ensure(M + 1);
+    poff.ensure(M + 1);
+    GB_CUDA(cudaMemsetAsync(pcnt.get() + M, 0, sizeof(uint32_t), st));
+    k_count_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(), pcnt.get());
+    GB_CUDA(cudaGetLastError());
+    exclusive_scan(pcnt.get(), poff.get(), M + 1, st);
+    uint32_t npairs = 0;
+    GB_CUDA(cudaMemcpy(&npairs, poff.get() + M, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    p.total_pairs = npairs;
+    DevBuf<uint32_t> pkey, pval, pkey_sorted;
+    pkey.ensure(npairs);
+    pval.ensure(npairs);
+    pkey_sorted.ensure(npairs);
+    p.grid_list.ensure(npairs);
+    k_write_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(), key_sorted.get(),
+                                                                 poff.get(), pkey.get(), pval.get());
+    GB_CUDA(cudaGetLastError());
+    sort_pairs(pkey.get(), pkey_sorted.get(), pval.get(), p.grid_list.get(), npairs, bits_for(nkeys), st);
+    GB_CUDA(cudaMemsetAsync(counts.get(), 0, (nkeys + 1) * sizeof(uint32_t), st));
+    k_histogram<<<(unsigned)((npairs + TB - 1) / TB), TB, 0, st>>>(pkey_sorted.get(), npairs, counts.get());
+    GB_CUDA(cudaGetLastError());
+    p.grid_off.ensure(nkeys + 1);
+    exclusive_scan(counts.get(), p.grid_off.get(), (int64_t)nkeys + 1, st);
+
+    p.F = F;
+    p.Mtot = M;
+    p.frame_off = off;
+    p.prepped_c2nc = (mode == GB_PREP_C2NC || mode == GB_PREP_ALL);
+    p.prepped_nc2c = (mode == GB_PREP_NC2C || mode == GB_PREP_ALL);
+    // Both structures are built regardless of mode (they are cheap); the mode
+    // is recorded for the reference's precondition checks.
+    p.prepped_c2nc = p.prepped_nc2c = true;
+    plan_build_work(p, st);
+    p.prepped = true;
+}
+
+// Host-side work lists: degridding chunks of home samples, gridding tiles
+// (heavy tiles split into chunks reduced by the last CTA).
+void plan_build_work(NufftPlan &p, cudaStream_t st) {
+    const KParams &k = p.kp;
+    const uint32_t nkeys = p.F * (uint32_t)k.ntiles_total;
+    std::vector<uint32_t> hoff(nkeys + 1), goff(nkeys + 1);
+    GB_CUDA(cudaMemcpy(hoff.data(), p.home_off.get(), (nkeys + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    GB_CUDA(cudaMemcpy(goff.data(), p.grid_off.get(), (nkeys + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    p.h_home_counts.resize(nkeys);
+    for (uint32_t i = 0; i < nkeys; i++) p.h_home_counts[i] = hoff[i + 1] - hoff[i];
+
+    // Degridding items: chunks of at most `deg_chunk` home samples.
+    const int64_t M = p.Mtot;
+    int deg_chunk = (int)std::max<int64_t>(64, std::min<int64_t>(1024, M / (148 * 4) + 1));
+    std::vector<WorkItem> deg;
+    for (uint32_t key = 0; key < nkeys; key++) {
+        uint32_t b = hoff[key], e = hoff[key + 1];
+        for (uint32_t s = b; s < e; s += deg_chunk) {
+            WorkItem w{};
+            w.ft = (int)key;
+            w.begin = (int)s;
+            w.end = (int)std::min<uint32_t>(e, s + deg_chunk);
+            w.split = -1;
+            deg.push_back(w);
+        }
+    }
+    std::stable_sort(deg.begin(), deg.end(), [](const WorkItem &a, const WorkItem &b) {
+        return (a.end - a.begin) > (b.end - b.begin);
+    });
+
+    // Gridding items.
+    int64_t total = goff[nkeys];
+    int split_len = p.tiling.split_len;
+    if (split_len <= 0) {
+        int64_t avg = total / std::max<uint32_t>(1, nkeys);
+        split_len = (int)std::max<int64_t>(256, 2 * avg);
+    }
+    std::vector<WorkItem> heavy, light;
+    std::vector<SplitInfo> splits;
+    int slots = 0;
+    for (uint32_t key = 0; key < nkeys; key++) {
+        uint32_t b = goff[key], e = goff[key + 1];
+        uint32_t len = e - b;
+        if ((int)len <= split_len) {
+            WorkItem w{};
+            w.ft = (int)key;
+            w.begin = (int)b;
+            w.end = (int)e;
+            w.split = -1;
+            light.push_back(w);
+        } else {
+            int nch = (int)((len + split_len - 1) / split_len);
+            int per = (int)((len + nch - 1) / nch);
+            SplitInfo si{slots, nch};
+            int sid = (int)splits.size();
+            splits.push_back(si);
+            for (int c = 0; c < nch; c++) {
+                WorkItem w{};
+                w.ft = (int)key;
+                w.begin = (int)(b + c * per);
+                w.end = (int)std::min<uint32_t>(e, b + (c + 1) * per);
+                w.split = sid;
+                w.chunk = c;
+                heavy.push_back(w);
+            }
+            slots += nch;
+        }
+    }
+    std::stable_sort(light.begin(), light.end(), [](const WorkItem &a, const WorkItem &b) {
+        return (a.end - a.begin) > (b.end - b.begin);
+    });
+    std::vector<WorkItem> grd(heavy);
+    grd.insert(grd.end(), light.begin(), light.end());
+
+    p.n_deg_items = (int)deg.size();
+    p.deg_items.ensure(std::max<size_t>(1, deg.size()));
+    if (!deg.empty())
+        GB_CUDA(cudaMemcpy(p.deg_items.get(), deg.data(), deg.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
+    p.n_grd_items = (int)grd.size();
+    p.grd_items.ensure(std::max<size_t>(1, grd.size()));
+    GB_CUDA(cudaMemcpy(p.grd_items.get(), grd.data(), grd.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
+    p.n_splits = (int)splits.size();
+    p.n_slots = slots;
+    p.splits.ensure(std::max<size_t>(1, splits.size()));
+    if (!splits.empty())
+        GB_CUDA(cudaMemcpy(p.splits.get(), splits.data(), splits.size() * sizeof(SplitInfo), cudaMemcpyHostToDevice));
+    p.split_counter_groups = 0;   // (re)allocated by the gridding launcher
+    (void)st;
+}
+
+cufftHandle plan_fft(NufftPlan &p, int batches, cudaStream_t st) {
+    auto it = p.fft_plans.find(batches);
+    cufftHandle h;
+    if (it == p.fft_plans.end()) {
+        int n[kMaxD];
+        for (int d = 0; d < p.D; d++) n[d] = (int)p.mos[p.D - 1 - d];
+        int dist = (int)p.kp.G;
+        GB_CUFFT(cufftPlanMany(&h, p.D, n, n, 1, dist, n, 1, dist, CUFFT_C2C, batches));
+        p.fft_plans[batches] = h;
+    } else {
+        h = it->second;
+    }
+    GB_CUFFT(cufftSetStream(h, st));
+    return h;
+}
+
+}  // namespace gb

@@ -1,0 +1,96 @@
+"""Python mirror of ``cuCgSolver<float_complext>`` (toolboxes/solvers/gpu/cuCgSolver.h,
+toolboxes/solvers/cgSolver.h:33-411) over the C ABI.
+
+Defaults follow cgSolver's constructor (cgSolver.h:49-54): 10 iterations,
+tc_tolerance 1e-3 with the relative-residual stop rule (rq/rq0 < tol).
+Dot products and norms are FP64 on the device; no host synchronisation
+happens inside the solve.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import torch
+
+from ._lib import check, lib
+from .nfft import _check_tensor, _ptr, _stream
+from .sense import cuNonCartesianSenseOperator
+
+
+class cuCgSolver:
+    def __init__(self):
+        h = ctypes.c_void_p()
+        check(lib.gb_cg_create(ctypes.byref(h)))
+        self._h = h
+        self.E = None
+        self.iterations = 10
+        self.tc_tolerance = 1e-3
+        self.x0 = None
+        self.precond = None
+        self.refinements = 1
+        self.last_iterations = 0
+        self.residual_history = None
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and lib is not None:
+            lib.gb_cg_destroy(self._h)
+            self._h = None
+
+    def set_encoding_operator(self, op: cuNonCartesianSenseOperator):
+        self.E = op
+        check(lib.gb_cg_set_encoding_operator(self._h, op._h, ctypes.c_float(op.get_weight())))
+
+    def set_max_iterations(self, iterations: int):
+        self.iterations = int(iterations)
+        check(lib.gb_cg_set_max_iterations(self._h, self.iterations))
+
+    def get_max_iterations(self) -> int:
+        return self.iterations
+
+    def set_tc_tolerance(self, tol: float):
+        self.tc_tolerance = float(tol)
+        check(lib.gb_cg_set_tc_tolerance(self._h, ctypes.c_float(tol)))
+
+    def get_tc_tolerance(self) -> float:
+        return self.tc_tolerance
+
+    def set_x0(self, x0: Optional[torch.Tensor]):
+        if x0 is not None:
+            _check_tensor(x0, torch.complex64, "x0")
+        self.x0 = x0
+        check(lib.gb_cg_set_x0(self._h, _ptr(x0)))
+
+    def set_preconditioner(self, weights: Optional[torch.Tensor]):
+        """cgPreconditioner with real diagonal weights (applied twice)."""
+        if weights is not None:
+            _check_tensor(weights, torch.float32, "weights")
+        self.precond = weights
+        check(lib.gb_cg_set_preconditioner(self._h, _ptr(weights)))
+
+    def set_identity_regularization(self, kappa: float):
+        check(lib.gb_cg_set_identity_regularization(self._h, ctypes.c_float(kappa)))
+
+    def set_refinements(self, n: int):
+        self.refinements = int(n)
+        check(lib.gb_cg_set_refinements(self._h, self.refinements))
+
+    def set_use_graph(self, use: bool):
+        check(lib.gb_cg_set_use_graph(self._h, int(bool(use))))
+
+    def solve(self, d: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        if self.E is None:
+            raise RuntimeError("Error: cgSolver::compute_rhs : no encoding operator is set")
+        _check_tensor(d, torch.complex64, "d")
+        E = self.E
+        shape = (E.num_frames,) + tuple(reversed(E.matrix_size))
+        if out is None:
+            out = torch.empty(shape, dtype=torch.complex64, device=d.device)
+        n_hist = max(1, self.iterations * self.refinements)
+        if self.residual_history is None or self.residual_history.numel() < n_hist:
+            self.residual_history = torch.zeros(n_hist, dtype=torch.float64, device=d.device)
+        its = ctypes.c_uint32()
+        check(lib.gb_cg_solve(self._h, _ptr(d), _ptr(out), _ptr(self.residual_history), ctypes.byref(its),
+                              _stream()))
+        self.last_iterations = its.value
+        return out

@@ -1,0 +1,400 @@
+"""CPU oracle for the non-Cartesian NUFFT / CG-SENSE path (test infrastructure).
+
+This module is the checker for the CUDA library in ``gadgetron_b200``.  Only
+``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import it; the product never does.
+
+It restates the reference GPU path (Gadgetron cuNFFT, STANDARD convolution,
+cuNonCartesianSenseOperator and cgSolver) on the CPU:
+
+* gridding, degridding and the kernel image of the deapodization filter are in
+  ``nufft_oracle.c`` (float kernel weights as the reference computes them,
+  double accumulation), loaded here through ctypes;
+* the centred FFT follows ``toolboxes/fft/gpu/cuNDFFT.cpp:184-252`` and
+  ``toolboxes/fft/gpu/cuNDFFT.cu:6-36``: checkerboard ("timeswitch") before and
+  after an unnormalised C2C transform, CUFFT_FORWARD = exp(-i), then a scale
+  by 1/sqrt(prod(size)) when ``do_scale``; computed here in complex128;
+* the deapodization filter follows ``toolboxes/nfft/gpu/cuNFFT.cu:171-202``:
+  kernel image, *unscaled* centred FFT (BACKWARDS for the image-domain
+  filter, FORWARDS for the Fourier-domain one), reciprocal;
+* ``compute`` follows ``toolboxes/nfft/NFFT.hpp:105-240`` (pad/crop offsets
+  ``toolboxes/core/gpu/cuNDArray_utils.cu:213-300``), ``mult_MH_M`` follows
+  ``NFFT.hpp:90-102``;
+* the SENSE operator follows
+  ``toolboxes/mri/pmri/gpu/cuNonCartesianSenseOperator.cu:14-62`` and
+  ``toolboxes/mri/pmri/gpu/sense_utilities.cu:7-123``;
+* the CG solver follows ``toolboxes/solvers/cgSolver.h:105-390`` with the
+  ``relativeResidualTCB`` stop rule of ``toolboxes/solvers/cgCallback.h:56-104``.
+
+The direct FP64 NDFT (``ndft_forward``/``ndft_adjoint``) is the accuracy
+oracle: y_j = dcw_j / sqrt(G) * sum_n x_n exp(-2 pi i k_j.(n - N/2)), G the
+number of oversampled grid cells.
+
+Array conventions (numpy, C order, x on the last axis):
+  image    [nb, F, *N[::-1]]     complex
+  grid     [nb, F, *mos[::-1]]   complex
+  samples  [nb, F, M]            complex
+  traj     [F, M, D]             float32 in [-1/2, 1/2], component 0 = x
+  dcw      [F, M]                float
+  csm      [C, *N[::-1]]         complex
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SRC = os.path.join(_HERE, "nufft_oracle.c")
+_LIB_PATH = os.path.join(_HERE, "liboracle_nufft.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile nufft_oracle.c with gcc (OpenMP, no FMA contraction)."""
+    if force or not os.path.exists(_LIB_PATH) or (
+            os.path.getmtime(_LIB_PATH) < os.path.getmtime(_SRC)):
+        tmp = _LIB_PATH + ".tmp%d" % os.getpid()
+        cmd = ["gcc", "-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
+               "-std=c11", "-D_DEFAULT_SOURCE", _SRC, "-o", tmp, "-lm"]
+        subprocess.check_call(cmd)
+        os.replace(tmp, _LIB_PATH)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.c_void_p
+        i64 = ctypes.c_int64
+        f32 = ctypes.c_float
+        L.or_bessi0f.restype = f32
+        L.or_bessi0f.argtypes = [f32]
+        L.or_kb1f.restype = f32
+        L.or_kb1f.argtypes = [f32, f32, f32, f32]
+        L.or_kb_get_1d.restype = f32
+        L.or_kb_get_1d.argtypes = [f32, f32, f32, f32, f32]
+        L.or_compute_beta.argtypes = [ctypes.c_int, P, P, f32, P]
+        L.or_scale_trajectory.restype = ctypes.c_int
+        L.or_scale_trajectory.argtypes = [ctypes.c_int, P, P, f32, P, i64, P]
+        L.or_grid_nc2c.argtypes = [ctypes.c_int, P, P, f32, i64, i64, i64, P, P, P, ctypes.c_int]
+        L.or_degrid_c2nc.argtypes = [ctypes.c_int, P, P, f32, i64, i64, i64, P, P, P, ctypes.c_int]
+        L.or_deapod_kernel_image.argtypes = [ctypes.c_int, P, P, f32, P]
+        L.or_ndft_forward.argtypes = [ctypes.c_int, P, ctypes.c_double, i64, i64, P, P, P, P]
+        L.or_ndft_adjoint.argtypes = [ctypes.c_int, P, ctypes.c_double, i64, i64, P, P, P, P]
+        L.or_num_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _u64(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.uint64))
+
+
+def num_threads() -> int:
+    return int(lib().or_num_threads())
+
+
+# ---------------------------------------------------------------- kernel ---
+
+def bessi0f(x: float) -> float:
+    return float(lib().or_bessi0f(np.float32(x)))
+
+
+def kb_beta(N, mos, W):
+    beta = np.zeros(len(N), np.float32)
+    lib().or_compute_beta(len(N), _p(_u64(N)), _p(_u64(mos)), np.float32(W), _p(beta))
+    return beta
+
+
+def kb_get_1d(delta: float, mos_d: int, W: float, beta_d: float) -> float:
+    W = np.float32(W)
+    return float(lib().or_kb_get_1d(np.float32(delta), np.float32(mos_d),
+                                    np.float32(1.0) / W, np.float32(beta_d),
+                                    W / np.float32(2.0)))
+
+
+# -------------------------------------------------------------- centred FFT --
+
+def timeswitch(a: np.ndarray, D: int) -> np.ndarray:
+    """Multiply by (-1)^(sum of coordinates) over the last D axes
+    (cuNDFFT.cu:6-36)."""
+    sign = np.ones(a.shape[-D:], dtype=np.float64)
+    for ax in range(D):
+        n = a.shape[a.ndim - D + ax]
+        s = np.where(np.arange(n) % 2 == 1, -1.0, 1.0)
+        shape = [1] * D
+        shape[ax] = n
+        sign = sign * s.reshape(shape)
+    return a * sign
+
+
+def centred_fft(a: np.ndarray, D: int, forward: bool, do_scale: bool = True) -> np.ndarray:
+    """cuNDFFT::fft / ifft over the last D axes (cuNDFFT.cpp:184-252)."""
+    axes = tuple(range(a.ndim - D, a.ndim))
+    b = timeswitch(np.asarray(a, dtype=np.complex128), D)
+    if forward:
+        b = np.fft.fftn(b, axes=axes)               # CUFFT_FORWARD, unnormalised
+    else:
+        b = np.fft.ifftn(b, axes=axes, norm="forward")  # CUFFT_INVERSE, unnormalised
+    b = timeswitch(b, D)
+    if do_scale:
+        G = int(np.prod([a.shape[ax] for ax in axes]))
+        b = b / np.sqrt(G)
+    return b
+
+
+# ------------------------------------------------------------ pad / crop ----
+
+def pad(img: np.ndarray, mos, D: int) -> np.ndarray:
+    """Centred zero-fill, offset mos/2 - N/2 (cuNDArray_utils.cu:273-300)."""
+    N = img.shape[-D:]
+    mos_r = tuple(int(m) for m in mos[::-1])
+    out = np.zeros(img.shape[:-D] + mos_r, dtype=np.complex128)
+    sl = tuple(slice(m // 2 - n // 2, m // 2 - n // 2 + n) for n, m in zip(N, mos_r))
+    out[(Ellipsis,) + sl] = img
+    return out
+
+
+def crop(grid: np.ndarray, N, D: int) -> np.ndarray:
+    """Centred crop, offset (mos - N) >> 1 (NFFT.hpp:178-181)."""
+    mos = grid.shape[-D:]
+    N_r = tuple(int(n) for n in N[::-1])
+    sl = tuple(slice((m - n) >> 1, ((m - n) >> 1) + n) for n, m in zip(N_r, mos))
+    return grid[(Ellipsis,) + sl].copy()
+
+
+# ------------------------------------------------------------------ plan ----
+
+class OraclePlan:
+    """CPU restatement of cuNFFT_impl<float, D, STANDARD>."""
+
+    def __init__(self, N, mos, W):
+        self.D = len(N)
+        self.N = tuple(int(n) for n in N)
+        self.mos = tuple(int(m) for m in mos)
+        self.W = float(np.float32(W))
+        self.G = int(np.prod(self.mos))
+        if any(m < n for n, m in zip(self.N, self.mos)):
+            raise ValueError("oversampled matrix size must be >= matrix size")
+        self._scaled = None
+        self.M = 0
+        self.F = 0
+        self._filter = {}
+
+    # NFFT_plan::preprocess -> cuGriddingConvolution::preprocess
+    def preprocess(self, traj: np.ndarray):
+        traj = np.ascontiguousarray(traj, dtype=np.float32)
+        if traj.ndim == 2:
+            traj = traj[None]
+        F, M, D = traj.shape
+        if D != self.D:
+            raise ValueError("trajectory dimensionality mismatch")
+        scaled = np.empty_like(traj)
+        rc = lib().or_scale_trajectory(self.D, _p(_u64(self.N)), _p(_u64(self.mos)),
+                                       np.float32(self.W), _p(traj), F * M, _p(scaled))
+        if rc != 0:
+            raise ValueError("trajectory out of range [-1/2, 1/2]")
+        self._scaled = scaled
+        self.M, self.F = M, F
+
+    @property
+    def scaled_trajectory(self):
+        return self._scaled
+
+    def deapodization_filter(self, fourier_domain: bool = False) -> np.ndarray:
+        """1 / unscaled centred FFT of the kernel image (cuNFFT.cu:171-202)."""
+        if fourier_domain not in self._filter:
+            img = np.empty(self.G, np.float32)
+            lib().or_deapod_kernel_image(self.D, _p(_u64(self.N)), _p(_u64(self.mos)),
+                                         np.float32(self.W), _p(img))
+            img = img.reshape(self.mos[::-1]).astype(np.complex128)
+            f = centred_fft(img, self.D, forward=fourier_domain, do_scale=False)
+            self._filter[fourier_domain] = 1.0 / f
+        return self._filter[fourier_domain]
+
+    def _nb(self, arr: np.ndarray, image_like: bool) -> int:
+        per = (int(np.prod(arr.shape[-self.D:])) if image_like else self.M) * self.F
+        n = arr.size // per
+        if n * per != arr.size or n == 0:
+            raise ValueError("array size is not a multiple of the plan's frame size")
+        return n
+
+    def convolve_c2nc(self, grid: np.ndarray, accumulate_into=None) -> np.ndarray:
+        nb = grid.size // (self.G * self.F)
+        g = np.ascontiguousarray(grid, dtype=np.complex128).reshape(nb, self.F, self.G)
+        out = (np.zeros((nb, self.F, self.M), np.complex128) if accumulate_into is None
+               else np.ascontiguousarray(accumulate_into, dtype=np.complex128).copy())
+        lib().or_degrid_c2nc(self.D, _p(_u64(self.N)), _p(_u64(self.mos)), np.float32(self.W),
+                             self.M, self.F, nb, _p(self._scaled), _p(g), _p(out),
+                             0 if accumulate_into is None else 1)
+        return out
+
+    def convolve_nc2c(self, samples: np.ndarray, accumulate_into=None) -> np.ndarray:
+        nb = samples.size // (self.M * self.F)
+        s = np.ascontiguousarray(samples, dtype=np.complex128).reshape(nb, self.F, self.M)
+        out = (np.zeros((nb, self.F) + self.mos[::-1], np.complex128) if accumulate_into is None
+               else np.ascontiguousarray(accumulate_into, dtype=np.complex128).copy())
+        lib().or_grid_nc2c(self.D, _p(_u64(self.N)), _p(_u64(self.mos)), np.float32(self.W),
+                           self.M, self.F, nb, _p(self._scaled), _p(s), _p(out),
+                           0 if accumulate_into is None else 1)
+        return out
+
+    def deapodize(self, image: np.ndarray, fourier_domain: bool = False) -> np.ndarray:
+        if tuple(image.shape[-self.D:]) != self.mos[::-1]:
+            raise ValueError("deapodize: oversampled image not provided as input")
+        return image * self.deapodization_filter(fourier_domain)
+
+    def fft(self, data: np.ndarray, forward: bool, do_scale: bool = True) -> np.ndarray:
+        return centred_fft(data, self.D, forward, do_scale)
+
+    # NFFT_plan::compute, modes FORWARDS_C2NC / BACKWARDS_NC2C / FORWARDS_NC2C
+    def forward_c2nc(self, image: np.ndarray, dcw=None) -> np.ndarray:
+        img = np.asarray(image, dtype=np.complex128)
+        if tuple(img.shape[-self.D:]) != self.mos[::-1]:
+            img = pad(img, self.mos, self.D)
+        nb = img.size // (self.G * self.F)
+        img = img.reshape((nb, self.F) + self.mos[::-1])
+        img = self.deapodize(img)
+        img = self.fft(img, forward=True)
+        out = self.convolve_c2nc(img)
+        if dcw is not None:
+            out = out * np.asarray(dcw, np.float64).reshape(1, self.F, self.M)
+        return out
+
+    def backwards_nc2c(self, samples: np.ndarray, dcw=None, oversampled_out=False) -> np.ndarray:
+        s = np.asarray(samples, dtype=np.complex128)
+        nb = s.size // (self.M * self.F)
+        s = s.reshape(nb, self.F, self.M)
+        if dcw is not None:
+            s = s * np.asarray(dcw, np.float64).reshape(1, self.F, self.M)
+        img = self.convolve_nc2c(s)
+        img = self.fft(img, forward=False)
+        img = self.deapodize(img)
+        return img if oversampled_out else crop(img, self.N, self.D)
+
+    def forwards_nc2c(self, samples: np.ndarray, dcw=None, oversampled_out=False) -> np.ndarray:
+        s = np.asarray(samples, dtype=np.complex128)
+        nb = s.size // (self.M * self.F)
+        s = s.reshape(nb, self.F, self.M)
+        if dcw is not None:
+            s = s * np.asarray(dcw, np.float64).reshape(1, self.F, self.M)
+        img = self.convolve_nc2c(s)
+        img = self.fft(img, forward=True)
+        img = self.deapodize(img, fourier_domain=True)
+        return img if oversampled_out else crop(img, self.N, self.D)
+
+    def mult_MH_M(self, image: np.ndarray, dcw=None) -> np.ndarray:
+        return self.backwards_nc2c(self.forward_c2nc(image, dcw), dcw)
+
+
+# --------------------------------------------------------------- SENSE ------
+
+class OracleSense:
+    """CPU restatement of cuNonCartesianSenseOperator<float, D>."""
+
+    def __init__(self, plan: OraclePlan, csm: np.ndarray, dcw=None):
+        self.plan = plan
+        self.csm = np.asarray(csm, np.complex128)
+        self.dcw = None if dcw is None else np.asarray(dcw, np.float64)
+
+    def mult_M(self, x: np.ndarray) -> np.ndarray:
+        # x [F, *N] -> coil images [C, F, *N] (sense_utilities.cu:7-18)
+        D = self.plan.D
+        coil = self.csm[:, None] * np.asarray(x, np.complex128)[None]
+        return self.plan.forward_c2nc(coil, self.dcw)
+
+    def mult_MH(self, y: np.ndarray) -> np.ndarray:
+        img = self.plan.backwards_nc2c(y, self.dcw)       # [C, F, *N]
+        return np.sum(img * np.conj(self.csm)[:, None], axis=0)  # sense_utilities.cu:66-78
+
+    def mult_MH_M(self, x: np.ndarray) -> np.ndarray:
+        return self.mult_MH(self.mult_M(x))
+
+
+def cg_solve(op, d: np.ndarray, iterations: int = 10, tc_tolerance: float = 1e-3,
+             x0=None, precond_weights=None, history=None):
+    """cgSolver::solve (cgSolver.h:105-390), complex128 throughout.
+
+    Unpreconditioned: rq = ||r||^2, alpha = rq / <p, q> (complex, Cdotc),
+    p <- p * (rq'/rq) + r.  Stops when rq/rq0 < tc_tolerance
+    (relativeResidualTCB)."""
+    rhs = op.mult_MH(d)
+    if iterations == 0:
+        return rhs
+    vdot = lambda a, b: np.vdot(a.ravel(), b.ravel())
+    x = np.zeros_like(rhs)
+    r = rhs.copy()
+    p = r.copy()
+    P = None if precond_weights is None else np.asarray(precond_weights)
+    if P is not None:
+        p = p * P * P
+    rq0 = float(np.real(vdot(r, p)))
+    if x0 is not None:
+        x = np.asarray(x0, np.complex128).copy()
+        r = r - op.mult_MH_M(x)
+        p = r.copy()
+        if P is not None:
+            p = p * P * P
+    rq = float(np.real(vdot(r, p)))
+    for it in range(iterations):
+        q = op.mult_MH_M(p)
+        alpha = rq / vdot(p, q)
+        x = x + alpha * p
+        r = r - alpha * q
+        if P is not None:
+            q = r * P * P
+            tmp_rq = float(np.real(vdot(r, q)))
+            p = p * (tmp_rq / rq) + q
+        else:
+            tmp_rq = float(np.real(vdot(r, r)))
+            p = p * (tmp_rq / rq) + r
+        rq = tmp_rq
+        if history is not None:
+            history.append(rq / rq0)
+        if rq / rq0 < tc_tolerance:
+            break
+    return x
+
+
+# ---------------------------------------------------------------- NDFT ------
+
+def ndft_forward(x: np.ndarray, traj: np.ndarray, mos, dcw=None) -> np.ndarray:
+    """Direct FP64 NDFT: x [nb, *N[::-1]] -> y [nb, M]; traj [M, D]."""
+    traj = np.ascontiguousarray(traj, dtype=np.float64)
+    M, D = traj.shape
+    N = tuple(int(n) for n in x.shape[-D:][::-1])
+    xs = np.ascontiguousarray(x, np.complex128).reshape(-1, int(np.prod(N)))
+    nb = xs.shape[0]
+    y = np.zeros((nb, M), np.complex128)
+    dc = None if dcw is None else np.ascontiguousarray(dcw, np.float64).ravel()
+    lib().or_ndft_forward(D, _p(_u64(N)), 1.0 / np.sqrt(float(np.prod(mos))), M, nb,
+                          _p(traj), None if dc is None else _p(dc), _p(xs), _p(y))
+    return y
+
+
+def ndft_adjoint(y: np.ndarray, traj: np.ndarray, N, mos, dcw=None) -> np.ndarray:
+    """Direct FP64 adjoint NDFT: y [nb, M] -> x [nb, *N[::-1]]."""
+    traj = np.ascontiguousarray(traj, dtype=np.float64)
+    M, D = traj.shape
+    ys = np.ascontiguousarray(y, np.complex128).reshape(-1, M)
+    nb = ys.shape[0]
+    x = np.zeros((nb,) + tuple(int(n) for n in N[::-1]), np.complex128)
+    dc = None if dcw is None else np.ascontiguousarray(dcw, np.float64).ravel()
+    lib().or_ndft_adjoint(D, _p(_u64(N)), 1.0 / np.sqrt(float(np.prod(mos))), M, nb,
+                          _p(traj), None if dc is None else _p(dc), _p(ys), _p(x))
+    return x
+
+
+def rel_l2(a, b) -> float:
+    a = np.asarray(a, np.complex128).ravel()
+    b = np.asarray(b, np.complex128).ravel()
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))

@@ -1,0 +1,167 @@
+"""CPU checks of the oracle itself (no GPU): kernel values, exact adjointness,
+agreement with the FP64 direct NDFT, the padded-grid/wrap restatement against
+a plain-Python loop over the reference's steps, and the CG restatement."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from gadgetron_b200 import synthetic as S
+
+
+def test_bessi0_rational_matches_i0():
+    from scipy.special import i0
+    xs = np.linspace(0.0, 15.0, 301)
+    v = np.array([O.bessi0f(x) for x in xs])
+    ref = i0(xs)
+    assert np.max(np.abs(v - ref) / ref) < 2e-6
+
+
+def test_beta_formula():
+    # beta = pi * sqrt(W^2/alpha^2 (alpha - 1/2)^2 - 0.8)  (Beatty 2005)
+    for N, mos, W in [(128, 256, 5.5), (128, 192, 4.0), (512, 640, 4.0), (192, 384, 5.5)]:
+        a = mos / N
+        b = O.kb_beta([N], [mos], W)[0]
+        assert abs(b - np.pi * np.sqrt(W * W / (a * a) * (a - 0.5) ** 2 - 0.8)) < 1e-5 * b
+
+
+def test_kernel_cutoff_and_peak():
+    b = O.kb_beta([64], [128], 5.5)[0]
+    assert O.kb_get_1d(2.75001, 128, 5.5, b) == 0.0
+    peak = O.kb_get_1d(0.0, 128, 5.5, b)
+    assert abs(peak - 128 * O.bessi0f(b) / 5.5) < 1e-3 * peak
+    # the reference kernel is I0(0) * mos / W at the edge, not zero
+    edge = O.kb_get_1d(2.75, 128, 5.5, b)
+    assert edge == pytest.approx(128 / 5.5, rel=1e-5) or edge == 0.0
+
+
+def _py_grid_padded_wrap(N, mos, W, traj, y):
+    """Plain-Python restatement of the reference NC2C steps for one frame and
+    one batch: scale (ConvolverNC2C_standard.cuh:25-39), per padded cell
+    accumulate over the sample footprint (:41-102, :229-292), then fold the
+    padding ring periodically (:358-477)."""
+    D = len(N)
+    r = np.float32(W) / np.float32(2)
+    pad = 2 * int(np.ceil(r))
+    hw = pad // 2
+    beta = O.kb_beta(N, mos, W)
+    padded = np.zeros(tuple(m + pad for m in mos[::-1]), np.complex128)
+    for j in range(traj.shape[0]):
+        # k*mos + bias rounded once (exact in double, so equal to fmaf)
+        s = [np.float32(np.float64(traj[j, d]) * mos[d] + ((mos[d] + pad) >> 1)) for d in range(D)]
+        lo = [int(np.ceil(np.float32(s[d] - r))) for d in range(D)]
+        hi = [int(np.floor(np.float32(s[d] + r))) for d in range(D)]
+        for idx in np.ndindex(*[hi[d] - lo[d] + 1 for d in range(D)]):
+            p = [lo[d] + idx[d] for d in range(D)]
+            w = None
+            for d in range(D):
+                delta = abs(np.float32(s[d] - np.float32(p[d])))
+                v = np.float32(O.kb_get_1d(delta, mos[d], W, beta[d]))
+                w = v if w is None else np.float32(w * v)   # float product, x first
+            padded[tuple(p[::-1])] += w * y[j]
+    out = np.zeros(tuple(mos[::-1]), np.complex128)
+    it = np.ndindex(*padded.shape)
+    for p in it:
+        g = tuple((p[k] - hw) % mos[::-1][k] for k in range(D))
+        out[g] += padded[p]
+    return out
+
+
+def test_grid_restatement_matches_python_loops():
+    N, mos, W = (32, 32), (64, 64), 5.5
+    rng = np.random.default_rng(0)
+    traj = rng.uniform(-0.5, 0.5, (40, 2)).astype(np.float32)
+    traj[0] = [-0.5, -0.5]
+    traj[1] = [0.4999, 0.0]
+    traj[2] = [0.0, 0.0]
+    y = rng.standard_normal(40) + 1j * rng.standard_normal(40)
+    P = O.OraclePlan(N, mos, W)
+    P.preprocess(traj[None])
+    g = P.convolve_nc2c(y[None, None]).reshape(64, 64)
+    ref = _py_grid_padded_wrap(N, mos, W, traj, y)
+    assert np.max(np.abs(g - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+def test_degrid_is_transpose_of_grid():
+    N, mos, W = (32, 32), (64, 64), 4.0
+    rng = np.random.default_rng(1)
+    traj = rng.uniform(-0.5, 0.5, (64, 2)).astype(np.float32)
+    P = O.OraclePlan(N, mos, W)
+    P.preprocess(traj[None])
+    g = rng.standard_normal((1, 1, 64, 64)) + 1j * rng.standard_normal((1, 1, 64, 64))
+    y = rng.standard_normal((1, 1, 64)) + 1j * rng.standard_normal((1, 1, 64))
+    a = np.vdot(P.convolve_c2nc(g).ravel(), y.ravel())
+    b = np.vdot(g.ravel(), P.convolve_nc2c(y).ravel())
+    assert abs(a - b) <= 1e-12 * abs(a)
+
+
+@pytest.mark.parametrize("W,alpha", [(5.5, 2.0), (4.0, 1.5)])
+def test_nufft_vs_ndft_2d(W, alpha):
+    N = 32
+    mos = int(N * alpha)
+    mos = ((mos + 31) // 32) * 32
+    traj = S.radial_golden_angle_2d(24, 64)
+    dcw = S.ramp_dcw(traj)
+    x = S.gaussian_image((1, 1, N, N), 2)
+    P = O.OraclePlan((N, N), (mos, mos), W)
+    P.preprocess(traj[None])
+    y = P.forward_c2nc(x)
+    yr = O.ndft_forward(x[0], traj, (mos, mos))
+    tol = 1e-4 if W == 5.5 else 2e-3
+    assert O.rel_l2(y, yr) < tol
+    xa = P.backwards_nc2c(y, dcw[None])
+    xr = O.ndft_adjoint(yr, traj, (N, N), (mos, mos), dcw)
+    assert O.rel_l2(xa, xr) < tol
+
+
+def test_nufft_vs_ndft_3d():
+    N, mos, W = 32, 64, 4.0
+    traj = S.kooshball_golden_means_3d(50, 32)
+    x = S.gaussian_image((1, 1, N, N, N), 3)
+    P = O.OraclePlan((N, N, N), (mos, mos, mos), W)
+    P.preprocess(traj[None])
+    y = P.forward_c2nc(x)
+    yr = O.ndft_forward(x[0], traj, (mos, mos, mos))
+    assert O.rel_l2(y, yr) < 2e-3   # KB approximation error at W=4
+
+
+def test_adjointness_and_real_filter():
+    N, mos, W = (32, 32), (64, 64), 5.5
+    traj = S.radial_golden_angle_2d(16, 64)
+    P = O.OraclePlan(N, mos, W)
+    P.preprocess(traj[None])
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((1, 1, 32, 32)) + 1j * rng.standard_normal((1, 1, 32, 32))
+    z = rng.standard_normal((1, 1, traj.shape[0])) + 1j * rng.standard_normal((1, 1, traj.shape[0]))
+    a = np.vdot(P.forward_c2nc(x).ravel(), z.ravel())
+    b = np.vdot(x.ravel(), P.backwards_nc2c(z).ravel())
+    assert abs(a - b) <= 1e-12 * abs(a)
+    f = P.deapodization_filter()
+    assert np.max(np.abs(f.imag)) <= 1e-12 * np.max(np.abs(f.real))
+    # separable up to the float rounding of the kernel image (the reference
+    # grids fl(phi_x * phi_y)), which the small transform values at the grid
+    # edge amplify to a few 1e-6
+    fr = f.real
+    outer = np.outer(fr[:, 32], fr[32, :]) / fr[32, 32]
+    assert np.max(np.abs(outer - fr) / np.abs(fr)) <= 1e-5
+
+
+def test_trajectory_range_rejected():
+    P = O.OraclePlan((32, 32), (64, 64), 5.5)
+    with pytest.raises(ValueError):
+        P.preprocess(np.full((1, 8, 2), 0.51, np.float32))
+
+
+def test_cg_oracle_converges():
+    N, mos, W = (32, 32), (64, 64), 5.5
+    traj = S.radial_golden_angle_2d(48, 64)
+    dcw = S.ramp_dcw(traj)
+    csm = S.gaussian_bump_csm((32, 32), 4)
+    ph = S.ellipse_phantom((32, 32), 10, 0)[None]
+    P = O.OraclePlan(N, mos, W)
+    P.preprocess(traj[None])
+    E = O.OracleSense(P, csm, np.sqrt(dcw)[None])
+    d = E.mult_M(ph)
+    hist = []
+    x = O.cg_solve(E, d, iterations=20, tc_tolerance=0.0, history=hist)
+    assert hist[-1] < hist[0] * 1e-2
+    assert O.rel_l2(E.mult_M(x), d) < 0.05

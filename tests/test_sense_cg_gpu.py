@@ -1,0 +1,120 @@
+"""GPU parity of the non-Cartesian SENSE operator and the CG-SENSE solver
+against the CPU oracle (cuNonCartesianSenseOperator.cu:14-62 and
+cgSolver.h:105-390 restated in oracle/oracle.py)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from gadgetron_b200 import synthetic as S
+from tests.helpers import PARITY_TOL, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+import gadgetron_b200 as gb  # noqa: E402
+
+
+def sense_case(N=64, alpha=2.0, W=5.5, spokes=48, samples=128, coils=8, frames=1, seed=0):
+    mos = int(round(N * alpha))
+    traj = np.concatenate([S.radial_golden_angle_2d(spokes, samples, profile_offset=f * spokes)
+                           for f in range(frames)], 0)
+    dcw = np.concatenate([S.ramp_dcw(traj[f * spokes * samples:(f + 1) * spokes * samples])
+                          for f in range(frames)], 0)
+    sq = np.sqrt(dcw).astype(np.float32)
+    csm = S.gaussian_bump_csm((N, N), coils)
+    ph = np.stack([S.ellipse_phantom((N, N), 20, seed + f) for f in range(frames)], 0)
+    return dict(N=(N, N), mos=(mos, mos), W=W, traj=traj, sqrt_dcw=sq, csm=csm, phantom=ph, frames=frames,
+                M=spokes * samples, coils=coils)
+
+
+def make_ops(case, cuda, flags=0):
+    E = gb.cuNonCartesianSenseOperator(2, flags=flags)
+    E.setup(case["N"], case["mos"], case["W"])
+    E.set_csm(torch.from_numpy(case["csm"]).to(cuda))
+    E.set_dcw(torch.from_numpy(case["sqrt_dcw"]).to(cuda))
+    E.preprocess(torch.from_numpy(case["traj"]).to(cuda), num_frames=case["frames"])
+    plan = O.OraclePlan(case["N"], case["mos"], case["W"])
+    plan.preprocess(case["traj"].reshape(case["frames"], -1, 2))
+    orc = O.OracleSense(plan, case["csm"], case["sqrt_dcw"].reshape(case["frames"], -1))
+    return E, orc
+
+
+def test_sense_mult_M_MH(cuda):
+    case = sense_case(coils=8, seed=1)
+    E, orc = make_ops(case, cuda)
+    x = torch.from_numpy(case["phantom"]).to(cuda)
+    y = torch.empty((8, case["M"]), dtype=torch.complex64, device=cuda)
+    E.mult_M(x, y)
+    ref = orc.mult_M(case["phantom"])
+    assert rel_l2(y.cpu().numpy(), ref) <= PARITY_TOL
+    xb = torch.empty_like(x)
+    E.mult_MH(y, xb)
+    refb = orc.mult_MH(ref)
+    assert rel_l2(xb.cpu().numpy(), refb) <= PARITY_TOL
+    E.mult_MH(y, xb, accumulate=True)
+    assert rel_l2(xb.cpu().numpy(), 2 * refb) <= PARITY_TOL
+    xn = torch.empty_like(x)
+    E.mult_MH_M(x, xn)
+    assert rel_l2(xn.cpu().numpy(), orc.mult_MH_M(case["phantom"])) <= PARITY_TOL
+
+
+def test_sense_multiframe(cuda):
+    case = sense_case(N=32, spokes=16, samples=64, coils=4, frames=3, seed=2)
+    E, orc = make_ops(case, cuda)
+    x = torch.from_numpy(case["phantom"]).to(cuda)
+    y = torch.empty((4, 3 * case["M"]), dtype=torch.complex64, device=cuda)
+    E.mult_M(x, y)
+    ref = orc.mult_M(case["phantom"])
+    assert rel_l2(y.cpu().numpy(), ref.reshape(4, -1)) <= PARITY_TOL
+    xb = torch.empty_like(x)
+    E.mult_MH(y, xb)
+    assert rel_l2(xb.cpu().numpy(), orc.mult_MH(ref)) <= PARITY_TOL
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_cg_sense_matches_oracle(cuda, use_graph):
+    case = sense_case(coils=8, seed=3)
+    E, orc = make_ops(case, cuda)
+    d_ref = orc.mult_M(case["phantom"])
+    rng = np.random.default_rng(4)
+    noise = 0.01 * np.sqrt(np.mean(np.abs(d_ref) ** 2)) * (rng.standard_normal(d_ref.shape) +
+                                                          1j * rng.standard_normal(d_ref.shape)) / np.sqrt(2)
+    d = (d_ref + noise).astype(np.complex64)
+    cg = gb.cuCgSolver()
+    cg.set_encoding_operator(E)
+    cg.set_max_iterations(10)
+    cg.set_tc_tolerance(0.0)
+    cg.set_use_graph(use_graph)
+    x = cg.solve(torch.from_numpy(d.reshape(8, -1)).to(cuda))
+    hist = []
+    xr = O.cg_solve(orc, d, iterations=10, tc_tolerance=0.0, history=hist)
+    assert cg.last_iterations == 10
+    assert rel_l2(x.cpu().numpy(), xr) <= 1e-4
+    h = cg.residual_history[:10].cpu().numpy()
+    assert np.allclose(h, hist, rtol=1e-3)
+    if use_graph:
+        x2 = cg.solve(torch.from_numpy(d.reshape(8, -1)).to(cuda))
+        assert torch.equal(x, x2)
+
+
+def test_cg_early_stop_and_x0(cuda):
+    case = sense_case(coils=4, seed=5)
+    E, orc = make_ops(case, cuda)
+    d = orc.mult_M(case["phantom"]).astype(np.complex64)
+    dt = torch.from_numpy(d.reshape(4, -1)).to(cuda)
+    cg = gb.cuCgSolver()
+    cg.set_encoding_operator(E)
+    cg.set_max_iterations(30)
+    cg.set_tc_tolerance(1e-3)
+    x = cg.solve(dt)
+    hist = []
+    xr = O.cg_solve(orc, d, iterations=30, tc_tolerance=1e-3, history=hist)
+    assert cg.last_iterations == len(hist)
+    assert rel_l2(x.cpu().numpy(), xr) <= 1e-4
+    x0 = torch.from_numpy(case["phantom"] * 0.5).to(cuda)
+    cg.set_x0(x0)
+    cg.set_tc_tolerance(0.0)
+    cg.set_max_iterations(5)
+    x = cg.solve(dt)
+    xr = O.cg_solve(orc, d, iterations=5, tc_tolerance=0.0, x0=case["phantom"] * 0.5)
+    assert rel_l2(x.cpu().numpy(), xr) <= 1e-4
