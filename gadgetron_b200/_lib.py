@@ -42,7 +42,7 @@ class NotPreprocessedError(GadgetronB200Error):
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            "libgadgetron_b200.so is not built (%s); run `python -m gadgetron_b200.build`" % LIB_PATH)
+            "libgadgetron_b200.so is not built (%s); run `python gadgetron_b200/build.py`" % LIB_PATH)
     L = ctypes.CDLL(LIB_PATH)
     P = ctypes.c_void_p
     u32 = ctypes.c_uint32
@@ -52,6 +52,7 @@ def _load():
     sig = {
         "gb_last_error_message": (ctypes.c_char_p, []),
         "gb_version": (ctypes.c_char_p, []),
+        "gb_kernel_launch_count": (ctypes.c_uint64, []),
         "gb_nufft_plan_create": (i32, [i32, P, P, f32, u32, P]),
         "gb_nufft_plan_destroy": (i32, [P]),
         "gb_nufft_preprocess": (i32, [P, P, u64, u32, P, i32, P]),
@@ -95,7 +96,7 @@ def _load():
 
 lib = _load()
 EXPORTED = (
-    "gb_last_error_message gb_version gb_nufft_plan_create gb_nufft_plan_destroy gb_nufft_preprocess "
+    "gb_last_error_message gb_version gb_kernel_launch_count gb_nufft_plan_create gb_nufft_plan_destroy gb_nufft_preprocess "
     "gb_nufft_compute gb_nufft_mult_MH_M gb_nufft_convolve gb_nufft_fft gb_nufft_deapodize "
     "gb_nufft_traj_grad gb_nufft_traj_grad_from_grid gb_nufft_get_info gb_nufft_get_tiling "
     "gb_nufft_set_tiling gb_sense_create gb_sense_destroy gb_sense_preprocess gb_sense_set_csm "

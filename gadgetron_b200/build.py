@@ -3,7 +3,8 @@
 Every CUDA source under csrc/ is compiled with nvcc for
 ``-gencode arch=compute_100a,code=sm_100a`` and linked, with cuFFT, into one
 shared library placed next to this file (in-tree, so it travels with the
-repository).  Run ``python -m gadgetron_b200.build`` or call ``build()``.
+repository).  Run ``python gadgetron_b200/build.py`` (this file does not
+import the package, which needs the built library).
 """
 from __future__ import annotations
 

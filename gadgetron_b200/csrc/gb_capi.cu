@@ -1,5 +1,6 @@
 // extern "C" boundary: status codes instead of exceptions, thread-local
 // error messages, caller-owned device pointers.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -12,6 +13,10 @@
 namespace gb {
 
 static thread_local std::string g_last_error;
+static std::atomic<uint64_t> g_launches{0};
+
+void note_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void set_error(const std::string &msg) { g_last_error = msg; }
 
@@ -123,6 +128,8 @@ extern "C" {
 GB_API const char *gb_last_error_message(void) { return g_last_error.c_str(); }
 
 GB_API const char *gb_version(void) { return "gadgetron_b200 0.1 (sm_100a)"; }
+
+GB_API uint64_t gb_kernel_launch_count(void) { return launch_count(); }
 
 static void default_tiling(NufftPlan &p) {
     int t[3] = {16, 16, 1};

@@ -488,7 +488,7 @@ static int choose_cg(int requested, int nb) {
 
 template <int CG, int CPT, bool COMP>
 static void grid_dispatch(const ConvArgs &a, dim3 g, const float2 *s, float2 *o, cudaStream_t st) {
-    k_grid_nc2c<CG, CPT, COMP><<<g, kThreads, 0, st>>>(a, s, o);
+    k_grid_nc2c<CG, CPT, COMP><<<g, kThreads, 0, st>>>(a, s, o); ::gb::note_launch();
 }
 
 template <int CG, bool COMP>
@@ -580,7 +580,7 @@ static void degrid_launch(const ConvArgs &a, dim3 g, size_t smem, const float2 *
     auto kern = k_degrid_c2nc<CG, COMP, GRAD>;
     if (smem > 48 * 1024)
         GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<g, kThreads, smem, st>>>(a, grid, out, gw, gout);
+    kern<<<g, kThreads, smem, st>>>(a, grid, out, gw, gout); ::gb::note_launch();
 }
 
 template <bool COMP, bool GRAD>
@@ -642,7 +642,7 @@ void launch_traj_grad(NufftPlan &p, const float2 *grid, const float2 *weights, i
         GB_CUDA(cudaGetLastError());
     }
     if (ncg > 1) {
-        k_sum_groups<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part.get(), ncg, n, grad);
+        k_sum_groups<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part.get(), ncg, n, grad); ::gb::note_launch();
         GB_CUDA(cudaGetLastError());
         GB_CUDA(cudaStreamSynchronize(st));   // `part` is freed on return
     }

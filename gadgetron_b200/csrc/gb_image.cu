@@ -216,10 +216,10 @@ void launch_pad_forward(NufftPlan &p, const float2 *src, const float2 *csm, floa
     if (src_oversampled) {
         ImgArgs a = img_args(p, true);
         const int64_t nbf = (int64_t)nb * p.F;
-        k_pad_forward_os<<<grid_for(nbf * p.kp.G), 256, 0, st>>>(a, src, dst, nbf);
+        k_pad_forward_os<<<grid_for(nbf * p.kp.G), 256, 0, st>>>(a, src, dst, nbf); ::gb::note_launch();
     } else {
         ImgArgs a = img_args(p, false);
-        k_pad_forward<<<grid_for((int64_t)p.F * p.kp.NN), 256, 0, st>>>(a, src, csm, dst, nb, (int)p.F);
+        k_pad_forward<<<grid_for((int64_t)p.F * p.kp.NN), 256, 0, st>>>(a, src, csm, dst, nb, (int)p.F); ::gb::note_launch();
     }
     GB_CUDA(cudaGetLastError());
 }
@@ -232,28 +232,28 @@ void launch_crop_adjoint(NufftPlan &p, const float2 *grid, const float2 *csm, fl
         ImgArgs a = img_args(p, true);
         a.scale *= weight;
         const int64_t nbf = (int64_t)nb * p.F;
-        k_crop_adjoint_os<<<grid_for(nbf * p.kp.G), 256, 0, st>>>(a, grid, dst, nbf, accumulate ? 1 : 0);
+        k_crop_adjoint_os<<<grid_for(nbf * p.kp.G), 256, 0, st>>>(a, grid, dst, nbf, accumulate ? 1 : 0); ::gb::note_launch();
     } else {
         ImgArgs a = img_args(p, false);
         k_crop_adjoint<<<grid_for((int64_t)p.F * p.kp.NN), 256, 0, st>>>(a, grid, csm, dst, nb, (int)p.F,
-                                                                         accumulate ? 1 : 0, weight);
+                                                                         accumulate ? 1 : 0, weight); ::gb::note_launch();
     }
     GB_CUDA(cudaGetLastError());
 }
 
 void launch_timeswitch_scale(NufftPlan &p, float2 *data, int nbf, float scale, cudaStream_t st) {
-    k_timeswitch_scale<<<grid_for((int64_t)nbf * p.kp.G), 256, 0, st>>>(p.kp, data, nbf, scale);
+    k_timeswitch_scale<<<grid_for((int64_t)nbf * p.kp.G), 256, 0, st>>>(p.kp, data, nbf, scale); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 }
 
 void launch_deapodize_os(NufftPlan &p, float2 *data, int nbf, cudaStream_t st) {
     ImgArgs a = img_args(p, true);
-    k_deapodize_os<<<grid_for((int64_t)nbf * p.kp.G), 256, 0, st>>>(a, data, nbf);
+    k_deapodize_os<<<grid_for((int64_t)nbf * p.kp.G), 256, 0, st>>>(a, data, nbf); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 }
 
 void launch_multiply_dcw(const float *dcw, float2 *data, int64_t M, int nb, cudaStream_t st) {
-    k_multiply_dcw<<<grid_for(M * nb), 256, 0, st>>>(dcw, data, M, nb);
+    k_multiply_dcw<<<grid_for(M * nb), 256, 0, st>>>(dcw, data, M, nb); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 }
 

@@ -39,6 +39,9 @@ struct Error {
 };
 
 void set_error(const std::string &msg);
+// Counts kernel launches of this library (gb_kernel_launch_count).
+void note_launch(uint64_t n = 1);
+uint64_t launch_count();
 [[noreturn]] void fail(gb_status st, const std::string &msg);
 void check_cuda(cudaError_t e, const char *what);
 void check_cufft(cufftResult r, const char *what);
@@ -134,6 +137,7 @@ struct NufftPlan {
 
     // preprocess state
     bool prepped = false;
+    uint64_t generation = 0;       // bumped by every preprocess (invalidates captured graphs)
     bool prepped_c2nc = false, prepped_nc2c = false;
     uint32_t F = 0;
     int64_t Mtot = 0;

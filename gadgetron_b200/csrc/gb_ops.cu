@@ -411,7 +411,7 @@ static void cg_normal_dot(CgSolver &cg, cudaStream_t st) {
     k_cg_crop_dot<<<blocks_for(n), 256, 0, st>>>(p.kp, p.deap_img.get(), p.maxN,
                                                  (float)(1.0 / std::sqrt((double)p.kp.G)), kg, s.csm, nb,
                                                  (int)p.F, cg.p.get(), cg.q.get(), cg.weight, cg.kappa, cg.S.get(),
-                                                 cg.partials.get());
+                                                 cg.partials.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 }
 
@@ -420,9 +420,9 @@ static void cg_iteration(CgSolver &cg, cudaStream_t st, double *hist) {
     const int64_t n = (int64_t)p.F * p.kp.NN;
     cg_normal_dot(cg, st);
     k_cg_update<<<blocks_for(n), 256, 0, st>>>(n, cg.x.get(), cg.r.get(), cg.p.get(), cg.q.get(), cg.precond, n,
-                                                cg.S.get(), cg.partials.get(), hist);
+                                                cg.S.get(), cg.partials.get(), hist); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
-    k_cg_pupdate<<<blocks_for(n), 256, 0, st>>>(n, cg.p.get(), cg.r.get(), cg.precond, n, cg.S.get());
+    k_cg_pupdate<<<blocks_for(n), 256, 0, st>>>(n, cg.p.get(), cg.r.get(), cg.precond, n, cg.S.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 }
 
@@ -438,13 +438,13 @@ static void cg_solve_once(CgSolver &cg, const float2 *rhs, const float2 *x0, dou
     NufftPlan &p = cg.E->plan;
     const int64_t n = (int64_t)p.F * p.kp.NN;
     k_cg_init<<<blocks_for(n), 256, 0, st>>>(n, rhs, nullptr, cg.x.get(), x0, cg.r.get(), cg.p.get(), cg.precond,
-                                              n, cg.S.get(), cg.partials.get(), 1, (double)cg.tol, hist_base);
+                                              n, cg.S.get(), cg.partials.get(), 1, (double)cg.tol, hist_base); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
     if (x0) {
         cg_apply_normal(cg, x0, cg.q.get(), st);
         k_cg_init<<<blocks_for(n), 256, 0, st>>>(n, cg.r.get(), cg.q.get(), cg.x.get(), x0, cg.r.get(), cg.p.get(),
                                                   cg.precond, n, cg.S.get(), cg.partials.get(), 0, (double)cg.tol,
-                                                  hist_base);
+                                                  hist_base); ::gb::note_launch();
         GB_CUDA(cudaGetLastError());
     }
     for (uint32_t it = 0; it < cg.iterations; it++) cg_iteration(cg, st, hist);
@@ -482,7 +482,7 @@ static void cg_record(CgSolver &cg, const float2 *d, float2 *x_out, double *hist
                   CUFFT_INVERSE, st);
     if (cg.refinements <= 1) {
         cg_solve_once(cg, cg.rhs0.get(), cg.x0, hist, 0, st);
-        k_copy_f2<<<blocks_for(n), 256, 0, st>>>(n, cg.x.get(), x_out);
+        k_copy_f2<<<blocks_for(n), 256, 0, st>>>(n, cg.x.get(), x_out); ::gb::note_launch();
         GB_CUDA(cudaGetLastError());
         return;
     }
@@ -491,12 +491,12 @@ static void cg_record(CgSolver &cg, const float2 *d, float2 *x_out, double *hist
         const float2 *rhs = cg.rhs0.get();
         if (k > 0) {
             cg_apply_normal(cg, x_out, cg.q.get(), st);
-            k_refine_residual<<<blocks_for(n), 256, 0, st>>>(n, cg.rhs0.get(), cg.q.get(), cg.rhs.get());
+            k_refine_residual<<<blocks_for(n), 256, 0, st>>>(n, cg.rhs0.get(), cg.q.get(), cg.rhs.get()); ::gb::note_launch();
             GB_CUDA(cudaGetLastError());
             rhs = cg.rhs.get();
         }
         cg_solve_once(cg, rhs, (k == 0) ? cg.x0 : nullptr, hist, (int)(k * cg.iterations), st);
-        k_refine_accumulate<<<blocks_for(n), 256, 0, st>>>(n, cg.x64.get(), cg.x.get(), x_out);
+        k_refine_accumulate<<<blocks_for(n), 256, 0, st>>>(n, cg.x64.get(), cg.x.get(), x_out); ::gb::note_launch();
         GB_CUDA(cudaGetLastError());
     }
 }
@@ -521,15 +521,18 @@ void cg_solve(CgSolver &cg, const void *d, void *x_out, double *hist, uint32_t *
     cg_prepare(cg, st);
     if (cg.use_graph) {
         GraphKey key{d, x_out, hist, cg.iterations, cg.refinements, cg.x0, cg.precond, cg.kappa, cg.weight,
-                     cg.tol, s.csm, s.dcw, s.ncoils};
+                     cg.tol, s.csm, s.dcw, s.ncoils, s.plan.generation};
         if (!cg.graph_exec || !(key == cg.graph_key)) {
             cudaStream_t cs;
             GB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
             GB_CUDA(cudaStreamSynchronize(st));
             cudaGraph_t g;
+            const uint64_t before = launch_count();
             GB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
             try {
                 cg_record(cg, dd, xo, hist, cs);
+                cg.graph_kernels = launch_count() - before;
+                note_launch(0 - cg.graph_kernels);   // captured, not launched
             } catch (...) {
                 cudaGraph_t tmp;
                 cudaStreamEndCapture(cs, &tmp);
@@ -553,6 +556,7 @@ void cg_solve(CgSolver &cg, const void *d, void *x_out, double *hist, uint32_t *
             cg.graph_key = key;
         }
         GB_CUDA(cudaGraphLaunch(cg.graph_exec, st));
+        note_launch(cg.graph_kernels);
     } else {
         cg_record(cg, dd, xo, hist, st);
     }

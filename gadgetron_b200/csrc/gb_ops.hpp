@@ -23,8 +23,9 @@ struct GraphKey {
     const float2 *csm;
     const float *dcw;
     int ncoils;
+    uint64_t generation;
     bool operator==(const GraphKey &o) const {
-        return d == o.d && x == o.x && hist == o.hist && iterations == o.iterations &&
+        return generation == o.generation && d == o.d && x == o.x && hist == o.hist && iterations == o.iterations &&
                refinements == o.refinements && x0 == o.x0 && precond == o.precond && kappa == o.kappa &&
                weight == o.weight && tol == o.tol && csm == o.csm && dcw == o.dcw && ncoils == o.ncoils;
     }
@@ -48,6 +49,7 @@ struct CgSolver {
     DevBuf<CgScalars> S;
     cudaGraphExec_t graph_exec = nullptr;
     GraphKey graph_key{};
+    uint64_t graph_kernels = 0;   // kernels of this library inside the graph
     ~CgSolver();
 };
 

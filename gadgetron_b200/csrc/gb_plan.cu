@@ -306,6 +306,7 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
         for (uint32_t f = 0; f <= F; f++) off[f] = (int64_t)(Mtot / F) * f;
     }
     p.prepped = false;
+    p.generation++;
     const KParams &k = p.kp;
     const int64_t M = (int64_t)Mtot;
     const int D = p.D;
@@ -325,7 +326,7 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     GB_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), st));
     const int TB = 256;
     k_scale_bin<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, traj, M, d_off.get(), F, pos.get(),
-                                                               key.get(), idx.get(), err.get());
+                                                               key.get(), idx.get(), err.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
     int h_err = 0;
     GB_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -337,14 +338,14 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     sort_pairs(key.get(), key_sorted.get(), idx.get(), p.perm.get(), M, bits_for(nkeys), st);
     p.pos_sorted.ensure((size_t)D * M);
     k_gather_pos<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(D, M, pos.get(), p.perm.get(),
-                                                                p.pos_sorted.get());
+                                                                p.pos_sorted.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 
     // Home ranges.
     DevBuf<uint32_t> counts;
     counts.ensure(nkeys + 1);
     GB_CUDA(cudaMemsetAsync(counts.get(), 0, (nkeys + 1) * sizeof(uint32_t), st));
-    k_histogram<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(key_sorted.get(), M, counts.get());
+    k_histogram<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(key_sorted.get(), M, counts.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
     p.home_off.ensure(nkeys + 1);
     exclusive_scan(counts.get(), p.home_off.get(), (int64_t)nkeys + 1, st);
@@ -354,7 +355,7 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     pcnt.ensure(M + 1);
     poff.ensure(M + 1);
     GB_CUDA(cudaMemsetAsync(pcnt.get() + M, 0, sizeof(uint32_t), st));
-    k_count_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(), pcnt.get());
+    k_count_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(), pcnt.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
     exclusive_scan(pcnt.get(), poff.get(), M + 1, st);
     uint32_t npairs = 0;
@@ -366,11 +367,11 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     pkey_sorted.ensure(npairs);
     p.grid_list.ensure(npairs);
     k_write_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(), key_sorted.get(),
-                                                                 poff.get(), pkey.get(), pval.get());
+                                                                 poff.get(), pkey.get(), pval.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
     sort_pairs(pkey.get(), pkey_sorted.get(), pval.get(), p.grid_list.get(), npairs, bits_for(nkeys), st);
     GB_CUDA(cudaMemsetAsync(counts.get(), 0, (nkeys + 1) * sizeof(uint32_t), st));
-    k_histogram<<<(unsigned)((npairs + TB - 1) / TB), TB, 0, st>>>(pkey_sorted.get(), npairs, counts.get());
+    k_histogram<<<(unsigned)((npairs + TB - 1) / TB), TB, 0, st>>>(pkey_sorted.get(), npairs, counts.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
     p.grid_off.ensure(nkeys + 1);
     exclusive_scan(counts.get(), p.grid_off.get(), (int64_t)nkeys + 1, st);

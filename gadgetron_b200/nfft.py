@@ -188,6 +188,8 @@ class cuNFFT_plan:
                 raise ValueError("dcw must hold one weight per sample")
         image = inp if mode in (NFFT_comp_mode.FORWARDS_C2NC, NFFT_comp_mode.BACKWARDS_C2NC) else out
         samples = out if image is inp else inp
+        if self.num_samples == 0:   # let the library report the missing preprocess
+            check(lib.gb_nufft_compute(self._h, _ptr(inp), _ptr(out), _ptr(dcw), int(mode), 1, 0, _stream()))
         os_, nb = self._image_info(image)
         if samples.numel() != nb * self.num_samples:
             raise ValueError("The number of samples is not a multiple of #samples/frame x #frames")

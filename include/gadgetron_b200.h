@@ -83,6 +83,11 @@ typedef struct gb_cg_solver_s *gb_cg_solver;
 GB_API const char *gb_last_error_message(void);
 GB_API const char *gb_version(void);
 
+/* Number of CUDA kernels of this library launched so far in the process
+ * (kernels inside a replayed CUDA graph count once per replay; cuFFT's own
+ * kernels are not counted).  Instrumentation, no reference counterpart. */
+GB_API uint64_t gb_kernel_launch_count(void);
+
 /* ------------------------------------------------------------------ NUFFT */
 
 /* Replaces NFFT<cuNDArray,float,D>::make_plan(matrix_size, matrix_size_os, W,

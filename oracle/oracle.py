@@ -136,11 +136,27 @@ def timeswitch(a: np.ndarray, D: int) -> np.ndarray:
     return a * sign
 
 
+_FFT_WORKERS = 1
+
+
+def set_fft_workers(n: int):
+    """Use scipy.fft (pocketfft) with n threads for the oracle's FFTs (n > 1),
+    as the timed CPU baseline does; numpy's FFT otherwise."""
+    global _FFT_WORKERS
+    _FFT_WORKERS = int(n)
+
+
 def centred_fft(a: np.ndarray, D: int, forward: bool, do_scale: bool = True) -> np.ndarray:
     """cuNDFFT::fft / ifft over the last D axes (cuNDFFT.cpp:184-252)."""
     axes = tuple(range(a.ndim - D, a.ndim))
     b = timeswitch(np.asarray(a, dtype=np.complex128), D)
-    if forward:
+    if _FFT_WORKERS > 1:
+        import scipy.fft as sfft
+        if forward:
+            b = sfft.fftn(b, axes=axes, workers=_FFT_WORKERS)
+        else:
+            b = sfft.ifftn(b, axes=axes, norm="forward", workers=_FFT_WORKERS)
+    elif forward:
         b = np.fft.fftn(b, axes=axes)               # CUFFT_FORWARD, unnormalised
     else:
         b = np.fft.ifftn(b, axes=axes, norm="forward")  # CUFFT_INVERSE, unnormalised

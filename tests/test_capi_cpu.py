@@ -33,7 +33,10 @@ def test_library_exports_header_symbols():
 
 
 def test_build_targets_sm100a_only():
-    from gadgetron_b200 import build as B
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_gb_build", os.path.join(ROOT, "gadgetron_b200", "build.py"))
+    B = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(B)
     flags = " ".join(B.ARCH + B.CFLAGS)
     assert set(re.findall(r"arch=(\S+?),code=(\S+)", flags)) == {("compute_100a", "sm_100a")}
 
