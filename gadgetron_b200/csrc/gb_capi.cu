@@ -123,6 +123,30 @@ struct gb_cg_solver_s {
     CgSolver c;
 };
 
+namespace gb {
+NufftPlan *plan_from_handle(gb_nufft_plan h) { return h ? h->p : nullptr; }
+
+// Maps the exception being handled to a status code and records its message
+// (the same mapping the entry points of this file use).
+gb_status current_exception_status() {
+    try {
+        throw;
+    } catch (const Failure &e) {
+        set_error(e.msg);
+        return e.st;
+    } catch (const std::bad_alloc &) {
+        set_error("host allocation failed");
+        return GB_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception &e) {
+        set_error(e.what());
+        return GB_ERR_INTERNAL;
+    } catch (...) {
+        set_error("unknown error");
+        return GB_ERR_INTERNAL;
+    }
+}
+}  // namespace gb
+
 extern "C" {
 
 GB_API const char *gb_last_error_message(void) { return g_last_error.c_str(); }

@@ -570,6 +570,60 @@ void launch_grid(NufftPlan &p, const float2 *samples, float2 *grid, int nb, Samp
     GB_CUDA(cudaGetLastError());
 }
 
+// Scratch (split-tile partial tiles and their counters) that launch_grid
+// needs for `nb` batches, in elements.
+void grid_scratch_need(const NufftPlan &p, int nb, size_t *partial_elems, size_t *counter_elems) {
+    const KParams &k = p.kp;
+    const int cpt = (k.tile[0] * k.tile[1] * k.tile[2] + kThreads - 1) / kThreads;
+    const bool comp = (p.flags & GB_FLAG_COMPENSATED) != 0;
+    int cg = choose_cg(p.tiling.cg, nb);
+    if (cpt * cg > (comp ? 16 : 32)) cg = std::max(1, (comp ? 16 : 32) / cpt);
+    const int ncg = (nb + cg - 1) / cg;
+    *partial_elems = p.n_splits > 0 ? (size_t)p.n_slots * ncg * cg * kThreads * cpt : 0;
+    *counter_elems = p.n_splits > 0 ? (size_t)p.n_splits * ncg : 0;
+}
+
+// The gridding launch of launch_grid with caller-provided scratch: no device
+// allocation.  `counters` must hold counter_elems zeros on entry (the kernel
+// leaves them zero again when it completes).
+void launch_grid_external_scratch(NufftPlan &p, const float2 *samples, float2 *grid, int nb, bool accumulate,
+                                  float2 *partials, unsigned int *counters, cudaStream_t st) {
+    if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
+    const KParams &k = p.kp;
+    const int cpt = (k.tile[0] * k.tile[1] * k.tile[2] + kThreads - 1) / kThreads;
+    const bool comp = (p.flags & GB_FLAG_COMPENSATED) != 0;
+    const int cg = grid_cg(p, nb, cpt, comp);
+    const int ncg = (nb + cg - 1) / cg;
+    ConvArgs a = make_args(p, nb, LAYOUT_ORIGINAL, nullptr, 1, false, accumulate);
+    a.list = p.grid_list.get();
+    a.items = p.grd_items.get();
+    a.n_items = p.n_grd_items;
+    a.splits = p.splits.get();
+    a.ncg = ncg;
+    a.partials = partials;
+    a.counters = counters;
+    if (p.n_grd_items == 0) return;
+    dim3 g(p.n_grd_items, ncg);
+    if (comp) {
+        switch (cg) {
+            case 1: grid_dispatch_cpt<1, true>(cpt, a, g, samples, grid, st); break;
+            case 2: grid_dispatch_cpt<2, true>(cpt, a, g, samples, grid, st); break;
+            case 4: grid_dispatch_cpt<4, true>(cpt, a, g, samples, grid, st); break;
+            case 8: grid_dispatch_cpt<8, true>(cpt, a, g, samples, grid, st); break;
+            default: grid_dispatch_cpt<16, true>(cpt, a, g, samples, grid, st); break;
+        }
+    } else {
+        switch (cg) {
+            case 1: grid_dispatch_cpt<1, false>(cpt, a, g, samples, grid, st); break;
+            case 2: grid_dispatch_cpt<2, false>(cpt, a, g, samples, grid, st); break;
+            case 4: grid_dispatch_cpt<4, false>(cpt, a, g, samples, grid, st); break;
+            case 8: grid_dispatch_cpt<8, false>(cpt, a, g, samples, grid, st); break;
+            default: grid_dispatch_cpt<16, false>(cpt, a, g, samples, grid, st); break;
+        }
+    }
+    GB_CUDA(cudaGetLastError());
+}
+
 static size_t degrid_smem(const KParams &k, int cg) {
     return (size_t)region_dim(k, 0) * region_dim(k, 1) * region_dim(k, 2) * cg * sizeof(float2);
 }

@@ -76,6 +76,15 @@ void nufft_traj_grad(NufftPlan &p, const float2 *img, const float2 *weights, con
 void nufft_traj_grad_from_grid(NufftPlan &p, const float2 *grid, const float2 *weights, float *grad, int nb,
                                cudaStream_t st);
 
+// Gridding with caller-provided scratch (no device allocation).
+void grid_scratch_need(const NufftPlan &p, int nb, size_t *partial_elems, size_t *counter_elems);
+void launch_grid_external_scratch(NufftPlan &p, const float2 *samples, float2 *grid, int nb, bool accumulate,
+                                  float2 *partials, unsigned int *counters, cudaStream_t st);
+// The plan behind a C handle (defined with the C ABI).
+NufftPlan *plan_from_handle(gb_nufft_plan h);
+// Status code (and error message) for the exception being handled.
+gb_status current_exception_status();
+
 // SENSE
 void sense_mult_M(SenseOp &s, const void *in, void *out, bool accumulate, cudaStream_t st);
 void sense_mult_MH(SenseOp &s, const void *in, void *out, bool accumulate, cudaStream_t st);

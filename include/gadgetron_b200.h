@@ -142,6 +142,22 @@ GB_API gb_status gb_nufft_convolve(gb_nufft_plan plan, const void *in, void *out
                                    gb_conv_mode mode, int accumulate,
                                    uint32_t num_batches, void *stream);
 
+/* Gridding (NC2C convolution, samples -> oversampled grid) exactly as
+ * gb_nufft_convolve with GB_CONV_NC2C, but without allocating device memory.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code running in a host callback or a real-time thread with a fixed memory
+ * budget, under another allocator that must not be bypassed, or inside a
+ * stream capture.  Its scratch (the partial tiles of heavily loaded tiles) is
+ * a fixed 16 MiB array in device memory that each GPU loading this library
+ * keeps until exit; a plan and batch count needing more is rejected with
+ * GB_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress), so make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race and
+ * must be serialised by the caller.  The plan must be preprocessed. */
+GB_API gb_status gb_nufft_convolve_nc2c_noalloc(gb_nufft_plan plan, const void *samples,
+                                                void *grid, int accumulate,
+                                                uint32_t num_batches, void *stream);
+
 /* Replaces cuNFFT_impl::fft(data, NFFT_fft_mode, do_scale)
  * (toolboxes/nfft/gpu/cuNFFT.cu:58-70 -> cuNDFFT::fft/ifft): centred C2C
  * transform over the D grid dimensions of an oversampled array, in place. */
