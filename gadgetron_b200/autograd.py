@@ -48,13 +48,13 @@ class _NufftForward(torch.autograd.Function):
         image, dcw = ctx.saved_tensors
         dcw = dcw if ctx.has_dcw else None
         plan = ctx.plan
-        grad_y = grad_y.contiguous()
+        grad_y = grad_y.resolve_conj().resolve_neg().contiguous()
         g_img = g_traj = None
         if ctx.needs_input_grad[0]:
             g_img = torch.empty_like(image)
             plan.compute(grad_y, g_img, dcw, NFFT_comp_mode.BACKWARDS_NC2C)
         if ctx.needs_input_grad[1]:
-            g_traj = plan.traj_grad(image.contiguous(), grad_y.conj().contiguous(), dcw)
+            g_traj = plan.traj_grad(image.contiguous(), torch.conj_physical(grad_y).contiguous(), dcw)
         return g_img, g_traj, None, None
 
 
@@ -75,13 +75,13 @@ class _NufftAdjoint(torch.autograd.Function):
         samples, dcw = ctx.saved_tensors
         dcw = dcw if ctx.has_dcw else None
         plan = ctx.plan
-        grad_x = grad_x.contiguous()
+        grad_x = grad_x.resolve_conj().resolve_neg().contiguous()
         g_s = g_traj = None
         if ctx.needs_input_grad[0]:
             g_s = torch.empty_like(samples)
             plan.compute(grad_x, g_s, dcw, NFFT_comp_mode.FORWARDS_C2NC)
         if ctx.needs_input_grad[1]:
-            g_traj = plan.traj_grad(grad_x, samples.conj().contiguous(), dcw)
+            g_traj = plan.traj_grad(grad_x, torch.conj_physical(samples).contiguous(), dcw)
         return g_s, g_traj, None, None
 
 

@@ -162,7 +162,7 @@ static void default_tiling(NufftPlan &p) {
     // shrink for small grids while keeping >= 256 cells per tile
     for (int d = 0; d < p.D; d++)
         if (t[d] > p.kp.mos[d]) t[d] = (int)p.kp.mos[d];
-    set_tiling(p, t, 8);
+    set_tiling(p, t, 16);
 }
 
 GB_API gb_status gb_nufft_plan_create(int D, const uint64_t *matrix_size, const uint64_t *matrix_size_os,
@@ -470,6 +470,13 @@ GB_API gb_status gb_cg_set_refinements(gb_cg_solver solver, uint32_t refinements
         if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
         if (refinements == 0) fail(GB_ERR_INVALID_ARGUMENT, "refinements must be >= 1");
         solver->c.refinements = refinements;
+    });
+}
+
+GB_API gb_status gb_cg_set_frame_independent(gb_cg_solver solver, int independent) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
+        solver->c.independent_frames = independent != 0;
     });
 }
 

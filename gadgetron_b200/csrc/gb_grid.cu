@@ -85,6 +85,7 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
     __shared__ int s_n[kChunk][3];
     __shared__ float s_w[kChunk][3][kWMax];
     __shared__ float2 s_v[kChunk][CG];
+    __shared__ uint32_t s_mask[kChunk];
     __shared__ int s_last;
 
     // Cell ownership: warp patches of PX x PY cells.
@@ -160,7 +161,40 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
             s_v[i][c] = v;
         }
         __syncthreads();
-        for (int i = 0; i < cnt; i++) {
+        // Which warps' cell patches each staged sample overlaps.
+        if (threadIdx.x < kChunk) {
+            const int i = threadIdx.x;
+            uint32_t m = 0;
+            if (i < cnt) {
+                int lo[3], hi[3];
+                for (int d = 0; d < 3; d++) {
+                    const int T = k.tile[d];
+                    if (k.ntiles[d] == 1) {   // footprint may wrap inside the tile
+                        lo[d] = 0;
+                        hi[d] = T - 1;
+                    } else {
+                        const int a_ = s_a[i][d];
+                        const int st = (a_ < T) ? a_ : a_ - k.mos[d];
+                        lo[d] = max(st, 0);
+                        hi[d] = min(st + s_n[i][d] - 1, T - 1);
+                    }
+                }
+                for (int w = 0; w < 8; w++)
+                    for (int c = 0; c < CPT; c++) {
+                        const int q = w + 8 * c;
+                        const int x0 = (q % npx) * PX, y0 = ((q / npx) % npy) * PY, z0 = q / (npx * npy);
+                        if (x0 <= hi[0] && x0 + PX - 1 >= lo[0] && y0 <= hi[1] && y0 + PY - 1 >= lo[1] &&
+                            z0 <= hi[2] && z0 >= lo[2])
+                            m |= 1u << w;
+                    }
+            }
+            s_mask[i] = m;
+        }
+        __syncthreads();
+        uint32_t bits = __ballot_sync(0xffffffffu, lane < cnt && ((s_mask[lane] >> warp) & 1u));
+        while (bits) {
+            const int i = __ffs(bits) - 1;
+            bits &= bits - 1;
             const int a0 = s_a[i][0], a1 = s_a[i][1], a2 = s_a[i][2];
             const int n0 = s_n[i][0], n1 = s_n[i][1], n2 = s_n[i][2];
 #pragma unroll
@@ -276,12 +310,37 @@ __host__ __device__ __forceinline__ int region_dim(const KParams &k, int d) {
     return d < k.D ? k.tile[d] + 2 * k.hw : 1;
 }
 
+// Per-warp staging area of the degridding kernel: separable weights (and
+// their derivatives), region-local footprint starts and tap counts for the
+// SPW samples a warp serves at once.
+template <int SPW, bool GRAD>
+struct DegridStage {
+    float w[SPW][3][kWMax];
+    float dw[GRAD ? SPW : 1][3][kWMax];
+    int rs[SPW][3];
+    int n[SPW][3];
+};
+
+template <int CG>
+struct DegridShape {
+    static constexpr int CPL = (CG >= 2) ? 2 : 1;   // coils per lane
+    static constexpr int LPS = CG / CPL;            // lanes per sample
+    static constexpr int SPW = 32 / LPS;            // samples per warp pass
+};
+
+// Degridding: a CTA stages its home tile plus a halo of pad/2 cells (coil
+// fastest, so one sample's coil group is one contiguous row of CG complex
+// values) and serves a range of the tile's home samples.  A warp serves SPW
+// samples at once: LPS lanes per sample, CPL coils per lane, one 16-byte
+// shared-memory load and 4 FMAs per tap per lane.
 template <int CG, bool COMP, bool GRAD>
 __global__ void __launch_bounds__(kThreads)
 k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ out,
               const float2 *__restrict__ gweights, float *__restrict__ gout) {
+    using Sh = DegridShape<CG>;
+    constexpr int CPL = Sh::CPL, LPS = Sh::LPS, SPW = Sh::SPW;
+    using Stage = DegridStage<SPW, GRAD>;
     extern __shared__ float4 smem_raw[];
-    float2 *tile_s = reinterpret_cast<float2 *>(smem_raw);
     const KParams &k = a.k;
     const WorkItem it = a.items[blockIdx.x];
     const int grp = blockIdx.y;
@@ -295,6 +354,8 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
     const int R0 = region_dim(k, 0), R1 = region_dim(k, 1), R2 = region_dim(k, 2);
     const int cellsR = R0 * R1 * R2;
     const int h0 = k.D > 0 ? k.hw : 0, h1 = k.D > 1 ? k.hw : 0, h2 = k.D > 2 ? k.hw : 0;
+    float2 *tile_s = reinterpret_cast<float2 *>(smem_raw);
+    Stage *stages = reinterpret_cast<Stage *>(tile_s + (((size_t)cellsR * CG + 1) & ~(size_t)1));
 
     // Stage the region, coil fastest.
     for (int e = threadIdx.x; e < cellsR * CG; e += kThreads) {
@@ -312,142 +373,181 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
     __syncthreads();
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int LPS = 2 * CG;              // lanes per slot (coil x re/im)
-    constexpr int NS = 32 / LPS;             // slots: split of the y taps
-    const int slot = lane / LPS;
-    const int cl = lane % LPS;               // coil*2 + comp
-    const float *tile_f = reinterpret_cast<const float *>(tile_s);
+    const int sl = lane / LPS, ll = lane % LPS;
+    Stage &S = stages[warp];
+    const bool D3 = k.D > 2;
 
-    for (int i = it.begin + warp; i < it.end; i += 8) {
-        // Lanes 0..23 compute the (dim, tap) weights.
-        const int wd = lane / kWMax, wt = lane % kWMax;
-        float w = 0.f, dw = 0.f;
-        int lo = 0, n = 1;
-        float sp = 0.f;
-        if (wd < k.D) {
-            sp = a.pos[(int64_t)wd * a.Mtot + i] - (float)k.hw;
-            lo = (int)ceilf(sp - k.radius);
-            n = min((int)floorf(sp + k.radius) - lo + 1, kWMax);
-            if (wt < n) {
-                const int g = lo + wt;
-                const float diff = sp - (float)g;
-                w = kb_weight_1d(fabsf(diff), k.mos_f[wd], k.one_over_W, k.beta[wd], k.radius);
-                if (GRAD) {
-                    dw = kb_deriv_1d(fabsf(diff), k.mos_f[wd], k.one_over_W, k.beta[wd], k.radius);
-                    dw = (diff < 0.f) ? -dw : dw;
+    for (int base = it.begin + warp * SPW; base < it.end; base += 8 * SPW) {
+        // Separable weights of the warp's SPW samples, (sample, dim, tap) over lanes.
+        for (int e = lane; e < SPW * 3 * kWMax; e += 32) {
+            const int s = e / (3 * kWMax), d = (e / kWMax) % 3, t = e % kWMax;
+            const int i = base + s;
+            float w = 0.f, dw = 0.f;
+            if (i < it.end && d < k.D) {
+                const float sp = a.pos[(int64_t)d * a.Mtot + i] - (float)k.hw;
+                const int lo = (int)ceilf(sp - k.radius);
+                const int n = min((int)floorf(sp + k.radius) - lo + 1, kWMax);
+                if (t < n) {
+                    const int g = lo + t;
+                    const float diff = sp - (float)g;
+                    w = kb_weight_1d(fabsf(diff), k.mos_f[d], k.one_over_W, k.beta[d], k.radius);
+                    if (GRAD) {
+                        dw = kb_deriv_1d(fabsf(diff), k.mos_f[d], k.one_over_W, k.beta[d], k.radius);
+                        dw = (diff < 0.f) ? -dw : dw;
+                    }
+                    if (a.sign_fold) {
+                        const float sg = sign_of(wrapmod(g, k.mos[d]));
+                        w *= sg;
+                        dw *= sg;
+                    }
                 }
-                if (a.sign_fold) {
-                    const float sg = sign_of(wrapmod(g, k.mos[wd]));
-                    w *= sg;
-                    dw *= sg;
+                if (t == 0) {
+                    S.rs[s][d] = wrapmod(lo - org[d] + k.hw, k.mos[d]);
+                    S.n[s][d] = n;
                 }
+            } else if (i < it.end) {
+                w = (t == 0) ? 1.f : 0.f;
+                if (t == 0) { S.rs[s][d] = 0; S.n[s][d] = 1; }
+            } else if (t == 0) {
+                S.rs[s][d] = 0;
+                S.n[s][d] = 0;
             }
-        } else if (wd < 3) {
-            w = (wt == 0) ? 1.f : 0.f;
+            S.w[s][d][t] = w;
+            if (GRAD) S.dw[s][d][t] = dw;
         }
-        // Region-local start of the footprint per dim and tap counts.
-        int rs[3], nn[3];
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            const int lo_d = __shfl_sync(0xffffffffu, lo, d * kWMax);
-            const int n_d = __shfl_sync(0xffffffffu, n, d * kWMax);
-            if (d < k.D) {
-                rs[d] = wrapmod(lo_d - org[d] + k.hw, k.mos[d]);
-                nn[d] = n_d;
-            } else {
-                rs[d] = 0;
-                nn[d] = 1;
-            }
-        }
-        float wx[kWMax], dwx[kWMax];
+        __syncwarp();
+
+        const int i = base + sl;
+        const int rs0 = S.rs[sl][0], rs1 = S.rs[sl][1], rs2 = S.rs[sl][2];
+        const int n0 = S.n[sl][0], n1 = S.n[sl][1], n2 = S.n[sl][2];
+        float wx[kWMax], dwx[GRAD ? kWMax : 1];
 #pragma unroll
         for (int t = 0; t < kWMax; t++) {
-            wx[t] = __shfl_sync(0xffffffffu, w, t);
-            if (GRAD) dwx[t] = __shfl_sync(0xffffffffu, dw, t);
-            // taps outside the staged region carry zero weight (see header)
-            if (t >= nn[0] || rs[0] + t >= R0) { wx[t] = 0.f; if (GRAD) dwx[t] = 0.f; }
+            const bool in = (t < n0) && (rs0 + t < R0);
+            wx[t] = in ? S.w[sl][0][t] : 0.f;
+            if (GRAD) dwx[t] = in ? S.dw[sl][0][t] : 0.f;
         }
-        float acc = 0.f, cmp = 0.f;
-        float gx_acc = 0.f, gy_acc = 0.f, gz_acc = 0.f;
-        for (int tzi = 0; tzi < nn[2]; tzi++) {
-            const float wz = __shfl_sync(0xffffffffu, w, 2 * kWMax + tzi);
-            const float dwz = GRAD ? __shfl_sync(0xffffffffu, dw, 2 * kWMax + tzi) : 0.f;
-            const int rz = rs[2] + tzi;
-            for (int tyi = 0; tyi < nn[1]; tyi++) {
-                const float wy = __shfl_sync(0xffffffffu, w, kWMax + tyi);
-                const float dwy = GRAD ? __shfl_sync(0xffffffffu, dw, kWMax + tyi) : 0.f;
-                const int ry = rs[1] + tyi;
-                if ((tyi % NS) != slot || ry >= R1 || rz >= R2) continue;
-                const float *row = tile_f + ((int64_t)(rz * R1 + ry) * R0 + rs[0]) * LPS + cl;
-                if (GRAD) {
+        float acc[CPL][2], cmp[COMP ? CPL : 1][2];
+        float gacc[GRAD ? CPL : 1][3][2];
 #pragma unroll
-                    for (int t = 0; t < kWMax; t++) {
-                        const float gv = (wx[t] != 0.f || dwx[t] != 0.f) ? row[t * LPS] : 0.f;
-                        gx_acc = fmaf(dwx[t] * wy * wz, gv, gx_acc);
-                        gy_acc = fmaf(wx[t] * dwy * wz, gv, gy_acc);
-                        gz_acc = fmaf(wx[t] * wy * dwz, gv, gz_acc);
+        for (int c = 0; c < CPL; c++) {
+            acc[c][0] = acc[c][1] = 0.f;
+            if (COMP) cmp[c][0] = cmp[c][1] = 0.f;
+            if (GRAD)
+                for (int d = 0; d < 3; d++) gacc[c][d][0] = gacc[c][d][1] = 0.f;
+        }
+        for (int tzi = 0; tzi < n2; tzi++) {
+            const int rz = rs2 + tzi;
+            if (rz >= R2) break;
+            const float wz = S.w[sl][2][tzi];
+            const float dwz = GRAD ? S.dw[sl][2][tzi] : 0.f;
+            for (int tyi = 0; tyi < n1; tyi++) {
+                const int ry = rs1 + tyi;
+                if (ry >= R1) break;
+                const float wy = S.w[sl][1][tyi];
+                const float dwy = GRAD ? S.dw[sl][1][tyi] : 0.f;
+                const float2 *row = tile_s + ((size_t)(rz * R1 + ry) * R0 + rs0) * CG + ll * CPL;
+#pragma unroll
+                for (int t = 0; t < kWMax; t++) {
+                    if (GRAD) {
+                        if (wx[t] == 0.f && dwx[t] == 0.f) continue;
+                    } else if (wx[t] == 0.f) {
+                        continue;
                     }
-                } else {
+                    float2 v[CPL];
+                    if (CPL == 2) {
+                        const float4 q = *reinterpret_cast<const float4 *>(row + t * CG);
+                        v[0] = make_float2(q.x, q.y);
+                        v[CPL - 1] = make_float2(q.z, q.w);
+                    } else {
+                        v[0] = row[t * CG];
+                    }
+                    if (GRAD) {
+                        const float ax = (dwx[t] * wy) * wz, ay = (wx[t] * dwy) * wz, az = (wx[t] * wy) * dwz;
 #pragma unroll
-                    for (int t = 0; t < kWMax; t++) {
-                        if (wx[t] != 0.f) {
-                            const float wt2 = (wx[t] * wy) * wz;
-                            const float gv = row[t * LPS];
+                        for (int c = 0; c < CPL; c++) {
+                            gacc[c][0][0] = fmaf(ax, v[c].x, gacc[c][0][0]);
+                            gacc[c][0][1] = fmaf(ax, v[c].y, gacc[c][0][1]);
+                            gacc[c][1][0] = fmaf(ay, v[c].x, gacc[c][1][0]);
+                            gacc[c][1][1] = fmaf(ay, v[c].y, gacc[c][1][1]);
+                            gacc[c][2][0] = fmaf(az, v[c].x, gacc[c][2][0]);
+                            gacc[c][2][1] = fmaf(az, v[c].y, gacc[c][2][1]);
+                        }
+                    } else {
+                        float w = wx[t] * wy;
+                        if (D3) w *= wz;
+#pragma unroll
+                        for (int c = 0; c < CPL; c++) {
                             if (COMP) {
-                                float y = wt2 * gv - cmp;
-                                float tt = acc + y;
-                                cmp = (tt - acc) - y;
-                                acc = tt;
+                                float y0 = w * v[c].x - cmp[c][0];
+                                float s0 = acc[c][0] + y0;
+                                cmp[c][0] = (s0 - acc[c][0]) - y0;
+                                acc[c][0] = s0;
+                                float y1 = w * v[c].y - cmp[c][1];
+                                float s1 = acc[c][1] + y1;
+                                cmp[c][1] = (s1 - acc[c][1]) - y1;
+                                acc[c][1] = s1;
                             } else {
-                                acc = fmaf(wt2, gv, acc);
+                                acc[c][0] = fmaf(w, v[c].x, acc[c][0]);
+                                acc[c][1] = fmaf(w, v[c].y, acc[c][1]);
                             }
                         }
                     }
                 }
             }
         }
-        const uint32_t j = a.perm[i];
+        const bool valid = i < it.end;
+        const uint32_t j = valid ? a.perm[i] : 0u;
+        const int64_t idx = (a.layout == LAYOUT_SORTED) ? (int64_t)i : (int64_t)j;
         if (!GRAD) {
-            if (COMP) acc -= cmp;
-#pragma unroll
-            for (int off = LPS; off < 32; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-            const int coil = b0 + (cl >> 1);
-            if (slot == 0 && coil < a.nb) {
-                float val = acc;
+            if (valid) {
+                float scale = 1.f;
                 if (a.dcw) {
                     const float dw2 = a.dcw[j];
-                    val = (a.dcw_pow == 2) ? (val * dw2) * dw2 : val * dw2;
+                    scale = (a.dcw_pow == 2) ? dw2 * dw2 : dw2;
                 }
-                const int64_t idx = (a.layout == LAYOUT_SORTED) ? (int64_t)i : (int64_t)j;
-                float *o = reinterpret_cast<float *>(out + (int64_t)coil * a.Mtot + idx) + (cl & 1);
-                if (a.accumulate) val += *o;
-                *o = val;
+#pragma unroll
+                for (int c = 0; c < CPL; c++) {
+                    const int coil = b0 + ll * CPL + c;
+                    if (coil >= a.nb) break;
+                    float2 val = make_float2(acc[c][0], acc[c][1]);
+                    if (a.dcw) {
+                        if (a.dcw_pow == 2) {
+                            const float dw2 = a.dcw[j];
+                            val.x = (val.x * dw2) * dw2;
+                            val.y = (val.y * dw2) * dw2;
+                        } else {
+                            val.x *= scale;
+                            val.y *= scale;
+                        }
+                    }
+                    float2 *o = out + (int64_t)coil * a.Mtot + idx;
+                    if (a.accumulate) { const float2 ov = *o; val.x += ov.x; val.y += ov.y; }
+                    *o = val;
+                }
             }
         } else {
-            // sum_coil Re(v * g):  lane (c, re) contributes v.re*g.re,
-            // lane (c, im) contributes -v.im*g.im.
-            const int coil = b0 + (cl >> 1);
-            float vcomp = 0.f;
-            if (coil < a.nb) {
-                const int64_t idx = (a.layout == LAYOUT_SORTED) ? (int64_t)i : (int64_t)j;
-                const float2 v = gweights[(int64_t)coil * a.Mtot + idx];
-                vcomp = (cl & 1) ? -v.y : v.x;
-            }
-            float r0 = vcomp * gx_acc, r1 = vcomp * gy_acc, r2 = vcomp * gz_acc;
+            float r[3] = {0.f, 0.f, 0.f};
+            if (valid) {
 #pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                r0 += __shfl_xor_sync(0xffffffffu, r0, off);
-                r1 += __shfl_xor_sync(0xffffffffu, r1, off);
-                r2 += __shfl_xor_sync(0xffffffffu, r2, off);
+                for (int c = 0; c < CPL; c++) {
+                    const int coil = b0 + ll * CPL + c;
+                    if (coil >= a.nb) break;
+                    const float2 v = gweights[(int64_t)coil * a.Mtot + idx];
+                    for (int d = 0; d < 3; d++) r[d] += v.x * gacc[c][d][0] - v.y * gacc[c][d][1];
+                }
             }
-            if (lane == 0) {
+#pragma unroll
+            for (int off = 1; off < LPS; off <<= 1)
+                for (int d = 0; d < 3; d++) r[d] += __shfl_xor_sync(0xffffffffu, r[d], off);
+            if (valid && ll == 0) {
                 float scale = 1.f;
                 if (a.dcw) scale = (a.dcw_pow == 2) ? a.dcw[j] * a.dcw[j] : a.dcw[j];
-                float *g = gout + ((int64_t)grp * a.Mtot + j) * k.D;
-                const float r[3] = {r0, r1, r2};
-                for (int d = 0; d < k.D; d++) g[d] = r[d] * k.mos_f[d] * scale;
+                float *gp = gout + ((int64_t)grp * a.Mtot + j) * k.D;
+                for (int d = 0; d < k.D; d++) gp[d] = r[d] * k.mos_f[d] * scale;
             }
         }
+        __syncwarp();
     }
 }
 
@@ -624,8 +724,21 @@ void launch_grid_external_scratch(NufftPlan &p, const float2 *samples, float2 *g
     GB_CUDA(cudaGetLastError());
 }
 
-static size_t degrid_smem(const KParams &k, int cg) {
-    return (size_t)region_dim(k, 0) * region_dim(k, 1) * region_dim(k, 2) * cg * sizeof(float2);
+template <int CG, bool GRAD>
+static size_t degrid_smem_t(const KParams &k) {
+    const size_t tile = (((size_t)region_dim(k, 0) * region_dim(k, 1) * region_dim(k, 2) * CG + 1) & ~(size_t)1) *
+                        sizeof(float2);
+    return tile + 8 * sizeof(DegridStage<DegridShape<CG>::SPW, GRAD>);
+}
+
+static size_t degrid_smem(const KParams &k, int cg, bool grad = false) {
+    switch (cg) {
+        case 1: return grad ? degrid_smem_t<1, true>(k) : degrid_smem_t<1, false>(k);
+        case 2: return grad ? degrid_smem_t<2, true>(k) : degrid_smem_t<2, false>(k);
+        case 4: return grad ? degrid_smem_t<4, true>(k) : degrid_smem_t<4, false>(k);
+        case 8: return grad ? degrid_smem_t<8, true>(k) : degrid_smem_t<8, false>(k);
+        default: return grad ? degrid_smem_t<16, true>(k) : degrid_smem_t<16, false>(k);
+    }
 }
 
 template <int CG, bool COMP, bool GRAD>
@@ -649,10 +762,10 @@ static void degrid_dispatch(int cg, const ConvArgs &a, dim3 g, size_t smem, cons
     }
 }
 
-static int degrid_cg(NufftPlan &p, int nb) {
+static int degrid_cg(NufftPlan &p, int nb, bool grad = false) {
     int cg = choose_cg(p.tiling.cg, nb);
-    while (cg > 1 && degrid_smem(p.kp, cg) > 200 * 1024) cg /= 2;
-    if (degrid_smem(p.kp, cg) > 220 * 1024) fail(GB_ERR_INVALID_ARGUMENT, "tile too large for shared memory");
+    while (cg > 1 && degrid_smem(p.kp, cg, grad) > 200 * 1024) cg /= 2;
+    if (degrid_smem(p.kp, cg, grad) > 220 * 1024) fail(GB_ERR_INVALID_ARGUMENT, "tile too large for shared memory");
     return cg;
 }
 
@@ -677,7 +790,7 @@ void launch_degrid(NufftPlan &p, const float2 *grid, float2 *samples, int nb, Sa
 void launch_traj_grad(NufftPlan &p, const float2 *grid, const float2 *weights, int nb,
                       const float *dcw, float *grad, bool sign_fold, cudaStream_t st) {
     if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
-    const int cg = degrid_cg(p, nb);
+    const int cg = degrid_cg(p, nb, true);
     const int ncg = (nb + cg - 1) / cg;
     ConvArgs a = make_args(p, nb, LAYOUT_ORIGINAL, dcw, 1, sign_fold, false);
     a.items = p.deg_items.get();
@@ -692,7 +805,7 @@ void launch_traj_grad(NufftPlan &p, const float2 *grid, const float2 *weights, i
     GB_CUDA(cudaMemsetAsync(target, 0, (size_t)ncg * n * sizeof(float), st));
     if (p.n_deg_items > 0) {
         dim3 g(p.n_deg_items, ncg);
-        degrid_dispatch<false, true>(cg, a, g, degrid_smem(p.kp, cg), grid, nullptr, weights, target, st);
+        degrid_dispatch<false, true>(cg, a, g, degrid_smem(p.kp, cg, true), grid, nullptr, weights, target, st);
         GB_CUDA(cudaGetLastError());
     }
     if (ncg > 1) {

@@ -181,11 +181,20 @@ void sense_mult_MH_M(SenseOp &s, const void *in, void *out, bool accumulate, cud
 
 // ------------------------------------------------------------------- CG ---
 
-// Device scalar block.
-struct CgScalars {
-    double rq, rq0, alpha_re, alpha_im, beta, pq_re, pq_im, tol;
-    int done, iters, hist_base, pad;
-    unsigned int ctr_dot, ctr_upd, ctr_init, ctr_pad;
+// Device scalars.  The CG vector is cut into `nseg` segments that iterate
+// independently (one per frame when frames are solved independently, a
+// single segment for the reference's coupled solve): each segment has its own
+// rq, rq0, alpha, beta and stop flag.
+struct CgSeg {
+    double rq, rq0, alpha_re, alpha_im, beta, metric;
+    int done, pad;
+    unsigned int ctr_dot, ctr_upd, ctr_init, pad2;
+};
+
+struct CgGlobal {
+    double tol;
+    int iters, hist_base, all_done, pad;
+    unsigned int seg_ctr, pad2;
 };
 
 constexpr int kDotBlocks = 296;
@@ -208,14 +217,17 @@ __device__ __forceinline__ double2 block_reduce_d2(double2 v, double2 *sh) {
     return v;
 }
 
-// Returns true in every thread of the last block to finish; that block then
-// holds the ordered sum of all block partials in `total`.
+// Per-segment reduction: blocks (blockIdx.x, seg) write their partial; the
+// last block of the segment to arrive sums the segment's partials in a fixed
+// order (bit-reproducible) and returns true in all its threads.  No block
+// waits for another.
 __device__ bool last_block_sum(double2 mine, double2 *partials, unsigned int *ctr, double2 *total) {
     __shared__ double2 sh[32];
     __shared__ int s_last;
+    double2 *seg_part = partials + (size_t)blockIdx.y * gridDim.x;
     double2 v = block_reduce_d2(mine, sh);
     if (threadIdx.x == 0) {
-        partials[blockIdx.x] = v;
+        seg_part[blockIdx.x] = v;
         __threadfence();
         const unsigned int old = atomicAdd(ctr, 1u);
         s_last = (old == gridDim.x - 1);
@@ -225,7 +237,7 @@ __device__ bool last_block_sum(double2 mine, double2 *partials, unsigned int *ct
     __threadfence();
     double2 acc = make_double2(0.0, 0.0);
     for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-        const double2 q = __ldcg(&partials[b]);
+        const double2 q = __ldcg(&seg_part[b]);
         acc.x += q.x;
         acc.y += q.y;
     }
@@ -236,17 +248,19 @@ __device__ bool last_block_sum(double2 mine, double2 *partials, unsigned int *ct
     return true;
 }
 
-// q = weight * crop(...) + kappa * p, then <p, q> -> alpha = rq / <p, q>.
+// q = weight * crop(...) + kappa * p, then <p, q> per segment -> alpha = rq / <p, q>.
 __global__ void k_cg_crop_dot(KParams k, const float *deap, int deap_stride, float scale,
                               const float2 *__restrict__ grid, const float2 *__restrict__ csm, int nb, int F,
                               const float2 *__restrict__ p, float2 *__restrict__ q, float weight, float kappa,
-                              CgScalars *S, double2 *partials) {
-    if (S->done) return;
-    const int64_t total = (int64_t)F * k.NN;
+                              CgSeg *segs, int64_t seg_len, double2 *partials) {
+    CgSeg &S = segs[blockIdx.y];
+    if (S.done) return;
     const int ox = (k.mos[0] - k.N[0]) >> 1, oy = (k.mos[1] - k.N[1]) >> 1, oz = (k.mos[2] - k.N[2]) >> 1;
+    const int64_t e0 = (int64_t)blockIdx.y * seg_len;
     double2 acc = make_double2(0.0, 0.0);
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-         e += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < seg_len;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = e0 + l;
         const int f = (int)(e / k.NN);
         const int64_t n = e - (int64_t)f * k.NN;
         const int x = (int)(n % k.N[0]);
@@ -276,54 +290,82 @@ __global__ void k_cg_crop_dot(KParams k, const float *deap, int deap_stride, flo
         acc.y += (double)pv.x * s.y - (double)pv.y * s.x;
     }
     double2 tot;
-    if (last_block_sum(acc, partials, &S->ctr_dot, &tot) && threadIdx.x == 0) {
-        S->pq_re = tot.x;
-        S->pq_im = tot.y;
+    if (last_block_sum(acc, partials, &S.ctr_dot, &tot) && threadIdx.x == 0) {
         const double den = tot.x * tot.x + tot.y * tot.y;
-        // alpha = rq / pq  (rq real)
-        S->alpha_re = S->rq * tot.x / den;
-        S->alpha_im = -S->rq * tot.y / den;
+        // alpha = rq / pq  (rq real), cgSolver.h:318
+        S.alpha_re = S.rq * tot.x / den;
+        S.alpha_im = -S.rq * tot.y / den;
     }
 }
 
-// x += alpha p ; r -= alpha q ; rq' = Re<r, P^2 r> ; beta = rq'/rq ; stop rule.
-__global__ void k_cg_update(int64_t n, float2 *__restrict__ x, float2 *__restrict__ r,
+// x += alpha p ; r -= alpha q ; rq' = Re<r, P^2 r> ; beta = rq'/rq ; stop rule
+// per segment; the last segment to finish records max(rq/rq0) in the history.
+__global__ void k_cg_update(int64_t seg_len, float2 *__restrict__ x, float2 *__restrict__ r,
                             const float2 *__restrict__ p, const float2 *__restrict__ q,
-                            const float *__restrict__ P, int64_t Pn, CgScalars *S, double2 *partials,
-                            double *hist) {
-    if (S->done) return;
-    const float ar = (float)S->alpha_re, ai = (float)S->alpha_im;
+                            const float *__restrict__ P, int64_t Pn, CgSeg *segs, CgGlobal *G,
+                            double2 *partials, double *hist) {
+    CgSeg &S = segs[blockIdx.y];
+    const bool was_done = S.done != 0;
     double2 acc = make_double2(0.0, 0.0);
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-        const float2 pv = p[e], qv = q[e];
-        float2 xv = x[e], rv = r[e];
-        xv.x += ar * pv.x - ai * pv.y;
-        xv.y += ar * pv.y + ai * pv.x;
-        rv.x -= ar * qv.x - ai * qv.y;
-        rv.y -= ar * qv.y + ai * qv.x;
-        x[e] = xv;
-        r[e] = rv;
-        float w2 = 1.f;
-        if (P) { const float w = P[e % Pn]; w2 = w * w; }
-        acc.x += (double)rv.x * (double)(rv.x * w2) + (double)rv.y * (double)(rv.y * w2);
+    if (!was_done) {
+        const float ar = (float)S.alpha_re, ai = (float)S.alpha_im;
+        const int64_t e0 = (int64_t)blockIdx.y * seg_len;
+        for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < seg_len;
+             l += (int64_t)gridDim.x * blockDim.x) {
+            const int64_t e = e0 + l;
+            const float2 pv = p[e], qv = q[e];
+            float2 xv = x[e], rv = r[e];
+            xv.x += ar * pv.x - ai * pv.y;
+            xv.y += ar * pv.y + ai * pv.x;
+            rv.x -= ar * qv.x - ai * qv.y;
+            rv.y -= ar * qv.y + ai * qv.x;
+            x[e] = xv;
+            r[e] = rv;
+            float w2 = 1.f;
+            if (P) { const float w = P[e % Pn]; w2 = w * w; }
+            acc.x += (double)rv.x * (double)(rv.x * w2) + (double)rv.y * (double)(rv.y * w2);
+        }
     }
     double2 tot;
-    if (last_block_sum(acc, partials, &S->ctr_upd, &tot) && threadIdx.x == 0) {
-        const double rq_new = tot.x;
-        S->beta = rq_new / S->rq;
-        S->rq = rq_new;
-        const double metric = rq_new / S->rq0;
-        if (hist) hist[S->hist_base + S->iters] = metric;
-        S->iters += 1;
-        if (metric < S->tol) S->done = 1;
+    if (last_block_sum(acc, partials, &S.ctr_upd, &tot) && threadIdx.x == 0) {
+        if (!was_done) {
+            const double rq_new = tot.x;
+            S.beta = rq_new / S.rq;
+            S.rq = rq_new;
+            S.metric = rq_new / S.rq0;
+            if (S.metric < G->tol) S.done = 1;
+        }
+        __threadfence();
+        const unsigned int old = atomicAdd(&G->seg_ctr, 1u);
+        if (old == gridDim.y - 1) {   // last segment of this iteration
+            __threadfence();
+            G->seg_ctr = 0u;
+            if (!G->all_done) {
+                double mx = 0.0;
+                int all = 1;
+                for (unsigned s = 0; s < gridDim.y; s++) {
+                    const double m = *((volatile double *)&segs[s].metric);
+                    mx = m > mx ? m : mx;
+                    all &= (*((volatile int *)&segs[s].done) != 0);
+                }
+                if (hist) hist[G->hist_base + G->iters] = mx;
+                G->iters += 1;
+                if (all) G->all_done = 1;
+            }
+        }
     }
 }
 
-// p = beta p + P^2 r
-__global__ void k_cg_pupdate(int64_t n, float2 *__restrict__ p, const float2 *__restrict__ r,
-                             const float *__restrict__ P, int64_t Pn, const CgScalars *S) {
-    const float b = (float)S->beta;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+// p = beta p + P^2 r (per segment)
+__global__ void k_cg_pupdate(int64_t seg_len, float2 *__restrict__ p, const float2 *__restrict__ r,
+                             const float *__restrict__ P, int64_t Pn, const CgSeg *segs) {
+    const CgSeg &S = segs[blockIdx.y];
+    if (S.done) return;
+    const float b = (float)S.beta;
+    const int64_t e0 = (int64_t)blockIdx.y * seg_len;
+    for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < seg_len;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = e0 + l;
         float2 rv = r[e];
         if (P) { const float w = P[e % Pn]; const float w2 = w * w; rv.x *= w2; rv.y *= w2; }
         float2 pv = p[e];
@@ -331,14 +373,19 @@ __global__ void k_cg_pupdate(int64_t n, float2 *__restrict__ p, const float2 *__
     }
 }
 
-// Initialisation: r = rhs - q (q optional), p = P^2 r, rq = Re<r, p>;
-// set_rq0 also records rq0 and clears the iteration state.
-__global__ void k_cg_init(int64_t n, const float2 *__restrict__ rhs, const float2 *__restrict__ q,
+// Initialisation per segment: r = rhs - q (q optional), p = P^2 r,
+// rq = Re<r, p>; set_rq0 also records rq0 and clears the iteration state
+// (cgSolver.h:219-288).
+__global__ void k_cg_init(int64_t seg_len, const float2 *__restrict__ rhs, const float2 *__restrict__ q,
                           float2 *__restrict__ x, const float2 *__restrict__ x0, float2 *__restrict__ r,
-                          float2 *__restrict__ p, const float *__restrict__ P, int64_t Pn, CgScalars *S,
-                          double2 *partials, int set_rq0, double tol, int hist_base) {
+                          float2 *__restrict__ p, const float *__restrict__ P, int64_t Pn, CgSeg *segs,
+                          CgGlobal *G, double2 *partials, int set_rq0, double tol, int hist_base) {
+    CgSeg &S = segs[blockIdx.y];
+    const int64_t e0 = (int64_t)blockIdx.y * seg_len;
     double2 acc = make_double2(0.0, 0.0);
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < seg_len;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = e0 + l;
         float2 rv = rhs[e];
         if (q) { const float2 qv = q[e]; rv.x -= qv.x; rv.y -= qv.y; }
         r[e] = rv;
@@ -350,14 +397,19 @@ __global__ void k_cg_init(int64_t n, const float2 *__restrict__ rhs, const float
         acc.x += (double)rv.x * pv.x + (double)rv.y * pv.y;
     }
     double2 tot;
-    if (last_block_sum(acc, partials, &S->ctr_init, &tot) && threadIdx.x == 0) {
-        S->rq = tot.x;
+    if (last_block_sum(acc, partials, &S.ctr_init, &tot) && threadIdx.x == 0) {
+        S.rq = tot.x;
         if (set_rq0) {
-            S->rq0 = tot.x;
-            S->done = 0;
-            S->iters = 0;
-            S->tol = tol;
-            S->hist_base = hist_base;
+            S.rq0 = tot.x;
+            S.done = 0;
+            S.metric = 1.0;
+            if (blockIdx.y == 0) {
+                G->tol = tol;
+                G->iters = 0;
+                G->hist_base = hist_base;
+                G->all_done = 0;
+                G->seg_ctr = 0u;
+            }
         }
     }
 }
@@ -392,6 +444,13 @@ static unsigned blocks_for(int64_t n) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, kDotBlocks));
 }
 
+// Launch shape of the segmented CG kernels: (blocks per segment, segments).
+static dim3 seg_grid(const CgSolver &cg) {
+    const int64_t bx = std::max<int64_t>(1, std::min<int64_t>((cg.seg_len + 255) / 256,
+                                                              std::max<int64_t>(1, kDotBlocks / cg.nseg)));
+    return dim3((unsigned)bx, (unsigned)cg.nseg);
+}
+
 CgSolver::~CgSolver() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
 }
@@ -407,11 +466,10 @@ static void cg_normal_dot(CgSolver &cg, cudaStream_t st) {
     float2 *kg = ensure_kgrid(p, nbf);
     launch_grid(p, samp, kg, nb, LAYOUT_SORTED, nullptr, true, false, st);
     exec_fft(p, kg, kg, (int)nbf, CUFFT_INVERSE, st);
-    const int64_t n = (int64_t)p.F * p.kp.NN;
-    k_cg_crop_dot<<<blocks_for(n), 256, 0, st>>>(p.kp, p.deap_img.get(), p.maxN,
-                                                 (float)(1.0 / std::sqrt((double)p.kp.G)), kg, s.csm, nb,
-                                                 (int)p.F, cg.p.get(), cg.q.get(), cg.weight, cg.kappa, cg.S.get(),
-                                                 cg.partials.get()); ::gb::note_launch();
+    k_cg_crop_dot<<<seg_grid(cg), 256, 0, st>>>(p.kp, p.deap_img.get(), p.maxN,
+                                                (float)(1.0 / std::sqrt((double)p.kp.G)), kg, s.csm, nb,
+                                                (int)p.F, cg.p.get(), cg.q.get(), cg.weight, cg.kappa, cg.segs.get(),
+                                                cg.seg_len, cg.partials.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 }
 
@@ -419,10 +477,10 @@ static void cg_iteration(CgSolver &cg, cudaStream_t st, double *hist) {
     NufftPlan &p = cg.E->plan;
     const int64_t n = (int64_t)p.F * p.kp.NN;
     cg_normal_dot(cg, st);
-    k_cg_update<<<blocks_for(n), 256, 0, st>>>(n, cg.x.get(), cg.r.get(), cg.p.get(), cg.q.get(), cg.precond, n,
-                                                cg.S.get(), cg.partials.get(), hist); ::gb::note_launch();
+    k_cg_update<<<seg_grid(cg), 256, 0, st>>>(cg.seg_len, cg.x.get(), cg.r.get(), cg.p.get(), cg.q.get(),
+                                              cg.precond, n, cg.segs.get(), cg.G.get(), cg.partials.get(), hist); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
-    k_cg_pupdate<<<blocks_for(n), 256, 0, st>>>(n, cg.p.get(), cg.r.get(), cg.precond, n, cg.S.get()); ::gb::note_launch();
+    k_cg_pupdate<<<seg_grid(cg), 256, 0, st>>>(cg.seg_len, cg.p.get(), cg.r.get(), cg.precond, n, cg.segs.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 }
 
@@ -437,14 +495,15 @@ static void cg_solve_once(CgSolver &cg, const float2 *rhs, const float2 *x0, dou
                           cudaStream_t st) {
     NufftPlan &p = cg.E->plan;
     const int64_t n = (int64_t)p.F * p.kp.NN;
-    k_cg_init<<<blocks_for(n), 256, 0, st>>>(n, rhs, nullptr, cg.x.get(), x0, cg.r.get(), cg.p.get(), cg.precond,
-                                              n, cg.S.get(), cg.partials.get(), 1, (double)cg.tol, hist_base); ::gb::note_launch();
+    k_cg_init<<<seg_grid(cg), 256, 0, st>>>(cg.seg_len, rhs, nullptr, cg.x.get(), x0, cg.r.get(), cg.p.get(),
+                                            cg.precond, n, cg.segs.get(), cg.G.get(), cg.partials.get(), 1,
+                                            (double)cg.tol, hist_base); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
     if (x0) {
         cg_apply_normal(cg, x0, cg.q.get(), st);
-        k_cg_init<<<blocks_for(n), 256, 0, st>>>(n, cg.r.get(), cg.q.get(), cg.x.get(), x0, cg.r.get(), cg.p.get(),
-                                                  cg.precond, n, cg.S.get(), cg.partials.get(), 0, (double)cg.tol,
-                                                  hist_base); ::gb::note_launch();
+        k_cg_init<<<seg_grid(cg), 256, 0, st>>>(cg.seg_len, cg.r.get(), cg.q.get(), cg.x.get(), x0, cg.r.get(),
+                                                cg.p.get(), cg.precond, n, cg.segs.get(), cg.G.get(),
+                                                cg.partials.get(), 0, (double)cg.tol, hist_base); ::gb::note_launch();
         GB_CUDA(cudaGetLastError());
     }
     for (uint32_t it = 0; it < cg.iterations; it++) cg_iteration(cg, st, hist);
@@ -461,8 +520,12 @@ static void cg_prepare(CgSolver &cg, cudaStream_t st) {
     cg.q.ensure(n);
     cg.rhs0.ensure(n);
     cg.rhs.ensure(n);
-    cg.partials.ensure(kDotBlocks);
-    if (cg.S.ensure(1)) GB_CUDA(cudaMemsetAsync(cg.S.get(), 0, sizeof(CgScalars), st));
+    cg.nseg = cg.independent_frames ? (int)p.F : 1;
+    cg.seg_len = n / cg.nseg;
+    const dim3 sg = seg_grid(cg);
+    cg.partials.ensure((size_t)sg.x * sg.y);
+    if (cg.segs.ensure(cg.nseg)) GB_CUDA(cudaMemsetAsync(cg.segs.get(), 0, cg.segs.n * sizeof(CgSeg), st));
+    if (cg.G.ensure(1)) GB_CUDA(cudaMemsetAsync(cg.G.get(), 0, sizeof(CgGlobal), st));
     if (cg.refinements > 1) cg.x64.ensure(n);
     // Workspaces and FFT plans must exist before any graph capture.
     ensure_img_os(p, (int64_t)nb * p.F, st);
@@ -521,7 +584,7 @@ void cg_solve(CgSolver &cg, const void *d, void *x_out, double *hist, uint32_t *
     cg_prepare(cg, st);
     if (cg.use_graph) {
         GraphKey key{d, x_out, hist, cg.iterations, cg.refinements, cg.x0, cg.precond, cg.kappa, cg.weight,
-                     cg.tol, s.csm, s.dcw, s.ncoils, s.plan.generation};
+                     cg.tol, s.csm, s.dcw, s.ncoils, s.plan.generation, cg.independent_frames};
         if (!cg.graph_exec || !(key == cg.graph_key)) {
             cudaStream_t cs;
             GB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
@@ -560,8 +623,8 @@ void cg_solve(CgSolver &cg, const void *d, void *x_out, double *hist, uint32_t *
     } else {
         cg_record(cg, dd, xo, hist, st);
     }
-    CgScalars hs;
-    GB_CUDA(cudaMemcpyAsync(&hs, cg.S.get(), sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+    CgGlobal hs;
+    GB_CUDA(cudaMemcpyAsync(&hs, cg.G.get(), sizeof(CgGlobal), cudaMemcpyDeviceToHost, st));
     GB_CUDA(cudaStreamSynchronize(st));
     if (iters_run) *iters_run = (uint32_t)(hs.hist_base + hs.iters);
     (void)n;

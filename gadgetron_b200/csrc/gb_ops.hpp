@@ -24,14 +24,16 @@ struct GraphKey {
     const float *dcw;
     int ncoils;
     uint64_t generation;
+    bool independent;
     bool operator==(const GraphKey &o) const {
-        return generation == o.generation && d == o.d && x == o.x && hist == o.hist && iterations == o.iterations &&
+        return generation == o.generation && independent == o.independent && d == o.d && x == o.x && hist == o.hist && iterations == o.iterations &&
                refinements == o.refinements && x0 == o.x0 && precond == o.precond && kappa == o.kappa &&
                weight == o.weight && tol == o.tol && csm == o.csm && dcw == o.dcw && ncoils == o.ncoils;
     }
 };
 
-struct CgScalars;
+struct CgSeg;
+struct CgGlobal;
 
 struct CgSolver {
     SenseOp *E = nullptr;
@@ -43,10 +45,14 @@ struct CgSolver {
     float kappa = 0.f;
     uint32_t refinements = 1;
     bool use_graph = false;
+    bool independent_frames = false;   // per-frame CG scalars (frames solved independently)
+    int nseg = 1;
+    int64_t seg_len = 0;
 
     DevBuf<float2> x, r, p, q, rhs0, rhs;
     DevBuf<double2> x64, partials;
-    DevBuf<CgScalars> S;
+    DevBuf<CgSeg> segs;
+    DevBuf<CgGlobal> G;
     cudaGraphExec_t graph_exec = nullptr;
     GraphKey graph_key{};
     uint64_t graph_kernels = 0;   // kernels of this library inside the graph

@@ -82,6 +82,10 @@ def _check_tensor(t: torch.Tensor, dtype, name: str):
         raise TypeError("%s must have dtype %s, got %s" % (name, dtype, t.dtype))
     if not t.is_contiguous():
         raise ValueError("%s must be contiguous" % name)
+    if t.is_conj() or t.is_neg():
+        # a lazy conjugate/negation view: the memory holds the unconjugated
+        # values, which is what the library would read
+        raise ValueError("%s is a lazy conj/neg view; call resolve_conj()/resolve_neg() first" % name)
 
 
 class cuNFFT_plan:

@@ -78,6 +78,11 @@ class cuCgSolver:
     def set_use_graph(self, use: bool):
         check(lib.gb_cg_set_use_graph(self._h, int(bool(use))))
 
+    def set_frame_independent(self, independent: bool):
+        """Per-frame CG scalars: each frame of a multi-frame operator is solved
+        as its own problem, all frames still in one launch per kernel."""
+        check(lib.gb_cg_set_frame_independent(self._h, int(bool(independent))))
+
     def solve(self, d: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
         if self.E is None:
             raise RuntimeError("Error: cgSolver::compute_rhs : no encoding operator is set")

@@ -271,6 +271,12 @@ GB_API gb_status gb_cg_set_identity_regularization(gb_cg_solver solver, float ka
 /* Outer iterative refinement: solve `refinements` times, each from the FP64
  * residual of the previous solution (x <- x + CG(E^H d - E^H E x)).  1 = off. */
 GB_API gb_status gb_cg_set_refinements(gb_cg_solver solver, uint32_t refinements);
+/* Solve the frames of a multi-frame operator as independent problems: each
+ * frame gets its own CG scalars (rq, alpha, beta, stop flag) while every
+ * kernel still covers all frames in one launch.  0 (default) = the
+ * reference's coupled solve over the whole multi-frame vector.  With 1, the
+ * result equals one solve per frame.  No reference counterpart. */
+GB_API gb_status gb_cg_set_frame_independent(gb_cg_solver solver, int independent);
 /* Capture each CG iteration (all kernels and FFTs, no host synchronisation)
  * into one CUDA graph on first use and replay it; 0 = plain launches. */
 GB_API gb_status gb_cg_set_use_graph(gb_cg_solver solver, int use_graph);

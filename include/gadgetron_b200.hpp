@@ -134,6 +134,7 @@ public:
     void set_x0(const void *x0) { check(gb_cg_set_x0(h_, x0)); }
     void set_preconditioner(const float *weights) { check(gb_cg_set_preconditioner(h_, weights)); }
     void set_use_graph(bool on) { check(gb_cg_set_use_graph(h_, on ? 1 : 0)); }
+    void set_frame_independent(bool on) { check(gb_cg_set_frame_independent(h_, on ? 1 : 0)); }
     void set_refinements(uint32_t n) { check(gb_cg_set_refinements(h_, n)); }
 
     // solve(d) -> x (written to x_out); returns the number of iterations run.

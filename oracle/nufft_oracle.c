@@ -407,3 +407,93 @@ int or_num_threads(void)
     return 1;
 #endif
 }
+
+/* d/du of the 1D kernel value for u in [0, radius], derivative of the same
+ * rational approximation: phi(u) = mos/W * R(beta^2 (1 - (2u/W)^2)) with
+ * R(z) = -num(z)/den(z) the function bessi0 evaluates at z = x^2
+ * (ConvolutionKernel.hpp:39-68), so phi'(u) = -(8 mos beta^2 u / W^3) R'(z).
+ * Double precision. */
+static double or_kb_deriv_1d(double u, double mos_f, double W, double beta, double radius)
+{
+    static const double a[15] = {0.144048298227235e10, 0.356644482244025e9, 0.216415572361227e8,
+                                 0.571661130563785e6,  0.830792541809429e4, 0.754337328948189e2,
+                                 0.463076284721000e0,  0.202591084143397e-2, 0.654858370096785e-5,
+                                 0.160224679395361e-7, 0.300931127112960e-10, 0.435125971262668e-13,
+                                 0.479440257548300e-16, 0.380715242345326e-19, 0.210580722890567e-22};
+    if (u > radius)
+        return 0.0;
+    double t = 2.0 * u / W;
+    double z = beta * beta * (1.0 - t * t);
+    double num = a[14], dnum = 0.0;
+    for (int i = 13; i >= 0; --i) {
+        dnum = dnum * z + num;
+        num = num * z + a[i];
+    }
+    const double b2 = -0.307646912682801e4, b1 = 0.347626332405882e7, b0 = -0.144048298227235e10;
+    double den = ((z + b2) * z + b1) * z + b0;
+    double dden = (3.0 * z + 2.0 * b2) * z + b1;
+    double dR = -(dnum * den - num * dden) / (den * den);
+    return -8.0 * mos_f * beta * beta * u / (W * W * W) * dR;
+}
+
+/* Trajectory gradient of the degridding convolution (oracle for the CUDA
+ * gradient kernel): for each sample j and dimension d,
+ *   out[j][d] = mos_d * sum_b Re( w[b][j] * sum_taps dphi/ds_d * grid[b][tap] )
+ * with the taps, wrap and float kernel values of or_degrid_c2nc.  grid:
+ * [nb][F][G] complex double; w: [nb][F][M] complex double; out: [F*M][D]. */
+void or_degrid_traj_grad(int D, const uint64_t *N, const uint64_t *mos, float W,
+                         int64_t M, int64_t F, int64_t nb, const float *scaled,
+                         const double *grid_in, const double *w, double *out)
+{
+    or_plan p;
+    or_plan_init(&p, D, N, mos, W);
+    int64_t G = 1;
+    for (int d = 0; d < D; d++) G *= p.mos[d];
+    const float hw_f = (float)(p.pad >> 1);
+
+#pragma omp parallel for schedule(static)
+    for (int64_t fj = 0; fj < F * M; fj++) {
+        const int64_t f = fj / M, j = fj % M;
+        const float *sp = scaled + fj * D;
+        float s[OR_MAXD];
+        int64_t lo[OR_MAXD], cnt[OR_MAXD];
+        int64_t ntaps = 1;
+        for (int d = 0; d < D; d++) {
+            s[d] = sp[d] - hw_f;
+            lo[d] = (int64_t)(int)ceilf(s[d] - p.radius);
+            int64_t hi = (int64_t)(int)floorf(s[d] + p.radius);
+            cnt[d] = hi - lo[d] + 1;
+            if (cnt[d] < 0) cnt[d] = 0;
+            ntaps *= cnt[d];
+        }
+        double acc[OR_MAXD];
+        for (int d = 0; d < D; d++) acc[d] = 0.0;
+        for (int64_t b = 0; b < nb; b++) {
+            const double *grid = grid_in + 2 * (b * F + f) * G;
+            const double wr = w[2 * ((b * F + f) * M + j)], wi = w[2 * ((b * F + f) * M + j) + 1];
+            for (int64_t t = 0; t < ntaps; t++) {
+                int64_t rem = t, idx = 0, stride = 1;
+                double val[OR_MAXD], der[OR_MAXD];
+                for (int d = 0; d < D; d++) {
+                    int64_t g = lo[d] + rem % cnt[d];
+                    rem /= cnt[d];
+                    double diff = (double)s[d] - (double)g;
+                    float delta = fabsf(s[d] - (float)g);
+                    val[d] = (double)or_kb_get_1d(delta, p.mos_f[d], p.one_over_W, p.beta[d], p.radius);
+                    der[d] = or_kb_deriv_1d(fabs(diff), p.mos_f[d], p.W, p.beta[d], p.radius) * (diff < 0 ? -1.0 : 1.0);
+                    idx += or_wrap(g, p.mos[d]) * stride;
+                    stride *= p.mos[d];
+                }
+                const double gr = grid[2 * idx], gi = grid[2 * idx + 1];
+                for (int d = 0; d < D; d++) {
+                    double c = der[d];
+                    for (int e = 0; e < D; e++)
+                        if (e != d) c *= val[e];
+                    /* Re(w * c * g) */
+                    acc[d] += c * (wr * gr - wi * gi);
+                }
+            }
+        }
+        for (int d = 0; d < D; d++) out[fj * D + d] = acc[d] * (double)p.mos_f[d];
+    }
+}

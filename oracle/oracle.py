@@ -86,6 +86,7 @@ def lib():
         L.or_ndft_forward.argtypes = [ctypes.c_int, P, ctypes.c_double, i64, i64, P, P, P, P]
         L.or_ndft_adjoint.argtypes = [ctypes.c_int, P, ctypes.c_double, i64, i64, P, P, P, P]
         L.or_num_threads.restype = ctypes.c_int
+        L.or_degrid_traj_grad.argtypes = [ctypes.c_int, P, P, f32, i64, i64, i64, P, P, P, P]
         _lib = L
     return _lib
 
@@ -309,6 +310,35 @@ class OraclePlan:
 
     def mult_MH_M(self, image: np.ndarray, dcw=None) -> np.ndarray:
         return self.backwards_nc2c(self.forward_c2nc(image, dcw), dcw)
+
+    def forward_grid(self, image: np.ndarray) -> np.ndarray:
+        """The oversampled k-space grid the forward NUFFT degrids from."""
+        img = np.asarray(image, dtype=np.complex128)
+        if tuple(img.shape[-self.D:]) != self.mos[::-1]:
+            img = pad(img, self.mos, self.D)
+        nb = img.size // (self.G * self.F)
+        img = img.reshape((nb, self.F) + self.mos[::-1])
+        return self.fft(self.deapodize(img), forward=True)
+
+    def traj_grad_from_grid(self, grid: np.ndarray, weights: np.ndarray) -> np.ndarray:
+        """out[j, d] = sum_b Re(weights[b, j] * d(degrid(grid))[b, j] / d k[j, d]),
+        the derivative of the taps' weights of or_degrid_c2nc (new surface; the
+        reference has no trajectory derivative)."""
+        nb = grid.size // (self.G * self.F)
+        g = np.ascontiguousarray(grid, dtype=np.complex128).reshape(nb, self.F, self.G)
+        w = np.ascontiguousarray(weights, dtype=np.complex128).reshape(nb, self.F, self.M)
+        out = np.zeros((self.F * self.M, self.D), np.float64)
+        lib().or_degrid_traj_grad(self.D, _p(_u64(self.N)), _p(_u64(self.mos)), np.float32(self.W),
+                                  self.M, self.F, nb, _p(self._scaled), _p(g), _p(w), _p(out))
+        return out
+
+    def traj_grad_forward(self, image: np.ndarray, weights: np.ndarray, dcw=None) -> np.ndarray:
+        """Gradient of the forward NUFFT (FORWARDS_C2NC, dcw on the output)
+        with respect to the trajectory, contracted with complex weights."""
+        w = np.asarray(weights, np.complex128).reshape(-1, self.F, self.M)
+        if dcw is not None:
+            w = w * np.asarray(dcw, np.float64).reshape(1, self.F, self.M)
+        return self.traj_grad_from_grid(self.forward_grid(image), w)
 
 
 # --------------------------------------------------------------- SENSE ------

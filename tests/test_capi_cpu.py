@@ -102,3 +102,11 @@ def test_product_fails_loudly_without_library(tmp_path):
              "try:\n    L._load()\nexcept ImportError as e:\n    print('IMPORT-ERROR', e)\n" % ROOT)
     r = subprocess.run(["python", "-c", code2], capture_output=True, text=True)
     assert "IMPORT-ERROR" in r.stdout
+
+
+def test_lazy_conj_views_are_rejected():
+    import torch
+    from gadgetron_b200.nfft import _check_tensor
+    t = torch.zeros(4, dtype=torch.complex64)
+    with pytest.raises(ValueError):
+        _check_tensor(t.conj(), torch.complex64, "x")

@@ -165,3 +165,43 @@ def test_cg_oracle_converges():
     x = O.cg_solve(E, d, iterations=20, tc_tolerance=0.0, history=hist)
     assert hist[-1] < hist[0] * 1e-2
     assert O.rel_l2(E.mult_M(x), d) < 0.05
+
+
+def test_oracle_traj_grad_matches_finite_differences():
+    """The oracle's analytic trajectory derivative (derivative of the same
+    rational Kaiser-Bessel approximation) against central differences of the
+    oracle forward, away from the points where a tap enters the support."""
+    N, mos, W = (32, 32), (64, 64), 5.5
+    traj = (S.radial_golden_angle_2d(24, 64).astype(np.float64) * 0.999).astype(np.float32)
+    M = traj.shape[0]
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((2, 1, 32, 32)) + 1j * rng.standard_normal((2, 1, 32, 32))
+    v = rng.standard_normal((2, M)) + 1j * rng.standard_normal((2, M))
+    P = O.OraclePlan(N, mos, W)
+    P.preprocess(traj[None])
+    g = P.traj_grad_forward(x, np.conj(v))
+    h = 1e-4
+    fd = np.zeros((M, 2))
+    for d in range(2):
+        vals = []
+        for sg in (1, -1):
+            tp = traj.copy()
+            tp[:, d] = (tp[:, d].astype(np.float64) + sg * h).astype(np.float32)
+            P2 = O.OraclePlan(N, mos, W)
+            P2.preprocess(tp[None])
+            y = P2.forward_c2nc(x).reshape(2, M)
+            vals.append((np.conj(v) * y).real.sum(0))
+        dk = ((traj[:, d].astype(np.float64) + h).astype(np.float32).astype(np.float64) -
+              (traj[:, d].astype(np.float64) - h).astype(np.float32).astype(np.float64))
+        fd[:, d] = (vals[0] - vals[1]) / dk
+    ok = np.ones(M, bool)
+    r = W / 2
+    for d in range(2):
+        lo = (traj[:, d].astype(np.float64) - h) * mos[d] + mos[d] / 2
+        hi = (traj[:, d].astype(np.float64) + h) * mos[d] + mos[d] / 2
+        for sgn in (-1.0, 1.0):
+            ok &= np.ceil(lo + sgn * r - 1e-3) == np.ceil(hi + sgn * r + 1e-3)
+            ok &= np.floor(lo + sgn * r - 1e-3) == np.floor(hi + sgn * r + 1e-3)
+    idx = np.nonzero(ok)[0]
+    assert len(idx) > 0.5 * M
+    assert np.linalg.norm(g[idx] - fd[idx]) / np.linalg.norm(fd[idx]) < 1e-3
