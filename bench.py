@@ -409,6 +409,299 @@ def run_reference(args):
     }
 
 
+# ------------------------------------------------------ other workloads ------
+
+def _timed(fn, steps, warmup, flush, stream):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    total = 0.0
+    for _ in range(steps):
+        if flush is not None:
+            flush.fill_(1.0)
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        fn()
+        e.record(stream)
+        e.synchronize()
+        total += s.elapsed_time(e)
+    return total / steps
+
+
+def run_nufft(args, dims):
+    """NUFFT forward (C2NC) + adjoint (NC2C, ramp dcw) throughput.
+    2D: 128^2, 1 coil, 128 golden-angle spokes x 256 (32768 samples), alpha 2, W 5.5.
+    3D: 128^3, 32 coils (Gaussian-bump coil images), 20000 golden-means
+    spokes x 256 (5.12M samples), alpha 1.5 (192^3), W 4."""
+    import torch
+    import gadgetron_b200 as gb
+    from gadgetron_b200 import synthetic as S
+    from gadgetron_b200._lib import lib
+    from oracle import oracle as O
+    dev = torch.device("cuda:0")
+    if dims == 2:
+        N, mos, W, C = (128, 128), (256, 256), 5.5, 1
+        traj = S.radial_golden_angle_2d(128, 256)
+        img = S.gaussian_image((C, 1, 128, 128), 11)
+    else:
+        N, mos, W, C = (128, 128, 128), (192, 192, 192), 4.0, 32
+        traj = S.kooshball_golden_means_3d(20000, 256)
+        x = S.gaussian_image((128, 128, 128), 12)
+        img = (S.gaussian_bump_csm((128, 128, 128), C) * x[None])[:, None].astype(np.complex64)
+    M = traj.shape[0]
+    dcw = S.ramp_dcw(traj)
+    plan = gb.NFFT.make_plan(N, mos, W)
+    t_prep0 = time.perf_counter()
+    traj_d = torch.from_numpy(traj).to(dev)
+    plan.preprocess(traj_d)
+    torch.cuda.synchronize()
+    t_prep = (time.perf_counter() - t_prep0) * 1e3
+    x_d = torch.from_numpy(img).to(dev)
+    dcw_d = torch.from_numpy(dcw).to(dev)
+    y_d = torch.empty((C, M), dtype=torch.complex64, device=dev)
+    xb_d = torch.empty_like(x_d)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        plan.compute(x_d, y_d, None, gb.NFFT_comp_mode.FORWARDS_C2NC)
+        plan.compute(y_d, xb_d, dcw_d, gb.NFFT_comp_mode.BACKWARDS_NC2C)
+
+    l0 = lib.gb_kernel_launch_count()
+    ms = _timed(step, args.steps, args.warmup, flush, stream)
+    launches = (lib.gb_kernel_launch_count() - l0) // (args.steps + args.warmup) * args.steps
+    t_fwd = _timed(lambda: plan.compute(x_d, y_d, None, gb.NFFT_comp_mode.FORWARDS_C2NC), 5, 2, flush, stream)
+    t_adj = _timed(lambda: plan.compute(y_d, xb_d, dcw_d, gb.NFFT_comp_mode.BACKWARDS_NC2C), 5, 2, flush, stream)
+    value = M * C / (ms * 1e-3) / 1e6
+    # accuracy: forward vs FP64 direct NDFT on a subset of samples (coil 0)
+    idx = np.random.default_rng(5).choice(M, 1024 if dims == 3 else 4096, replace=False)
+    O.set_fft_workers(os.cpu_count() or 1)
+    yn = O.ndft_forward(img[0, 0][None], traj[idx], mos)
+    err_ndft = O.rel_l2(y_d[0].cpu().numpy()[idx], yn[0])
+    res = {
+        "metric": "NUFFT fwd+adj Msample-coils/s (%dD)" % dims, "value": round(value, 2),
+        "unit": "Msample-coils/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64 (fp32)", "data": "synthetic",
+        "config": {"workload": "nufft-%dd" % dims, "matrix": N[0], "matrix_os": mos[0], "W": W, "coils": C,
+                   "samples": M, "l2": "flushed before every timed step"},
+        "ms_forward": round(t_fwd, 4), "ms_adjoint": round(t_adj, 4), "ms_preprocess_wall": round(t_prep, 2),
+        "forward_rel_l2_vs_fp64_ndft": err_ndft, "gpu_launches": int(launches),
+    }
+    if dims == 2:
+        P = O.OraclePlan(N, mos, W)
+        P.preprocess(traj[None])
+        yr = P.forward_c2nc(img)
+        xr = P.backwards_nc2c(yr, dcw[None])
+        res["forward_rel_l2_vs_oracle"] = O.rel_l2(y_d.cpu().numpy(), yr)
+        res["adjoint_rel_l2_vs_oracle"] = O.rel_l2(xb_d.cpu().numpy(), xr)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            yr = P.forward_c2nc(img)
+            P.backwards_nc2c(yr, dcw[None])
+        cpu_ms = (time.perf_counter() - t0) / 3 * 1e3
+        res["cpu_baseline"] = {"value": round(M * C / (cpu_ms * 1e-3) / 1e6, 3), "unit": "Msample-coils/s",
+                               "cores": os.cpu_count(), "kind": "port", "sample": "3 fwd+adj pairs"}
+    else:
+        res["fd_gradient"] = fd_gradient_check_3d(plan, x_d, traj, dcw_d, N, mos, W)
+    return res
+
+
+def fd_gradient_check_3d(plan, x_d, traj, dcw_d, N, mos, W, n_check=64, h=1e-4):
+    """Trajectory gradient through the autograd wrapper against central
+    differences (step h in k units) on n_check random samples whose tap ranges
+    do not change within +-h."""
+    import torch
+    import gadgetron_b200 as gb
+    from gadgetron_b200.autograd import nufft_forward
+    dev = x_d.device
+    rng = np.random.default_rng(9)
+    M = traj.shape[0]
+    C = x_d.shape[0]
+    traj = (traj.astype(np.float64) * 0.999).astype(np.float32)
+    p = gb.NFFT.make_plan(N, mos, W)
+    t_d = torch.from_numpy(traj).to(dev).requires_grad_(True)
+    p.preprocess(t_d.detach())
+    v = torch.from_numpy((rng.standard_normal((C, M)) + 1j * rng.standard_normal((C, M))).astype(np.complex64)).to(dev)
+    x_g = x_d.clone().requires_grad_(True)
+    y = nufft_forward(x_g, t_d, p, dcw_d)
+    (v.conj() * y).real.sum().backward()
+    g_ad = t_d.grad.cpu().numpy().astype(np.float64)
+    r = W / 2
+    ok = np.ones(M, bool)
+    for d in range(3):
+        lo = (traj[:, d].astype(np.float64) - h) * mos[d] + mos[d] / 2
+        hi = (traj[:, d].astype(np.float64) + h) * mos[d] + mos[d] / 2
+        for sgn in (-1.0, 1.0):
+            ok &= np.ceil(lo + sgn * r - 1e-3) == np.ceil(hi + sgn * r + 1e-3)
+            ok &= np.floor(lo + sgn * r - 1e-3) == np.floor(hi + sgn * r + 1e-3)
+    pick = rng.choice(np.nonzero(ok)[0], n_check, replace=False)
+    g_fd = np.zeros((n_check, 3))
+    out = torch.empty((C, M), dtype=torch.complex64, device=dev)
+    for d in range(3):
+        vals = []
+        for sg in (1.0, -1.0):
+            tp = traj.copy()
+            tp[:, d] = (tp[:, d].astype(np.float64) + sg * h).astype(np.float32)
+            p2 = gb.NFFT.make_plan(N, mos, W)
+            p2.preprocess(torch.from_numpy(tp).to(dev))
+            p2.compute(x_d, out, dcw_d, gb.NFFT_comp_mode.FORWARDS_C2NC)
+            vals.append((v.conj() * out).real.double().sum(0).cpu().numpy()[pick])
+            del p2
+        dk = ((traj[pick, d].astype(np.float64) + h).astype(np.float32).astype(np.float64) -
+              (traj[pick, d].astype(np.float64) - h).astype(np.float32).astype(np.float64))
+        g_fd[:, d] = (vals[0] - vals[1]) / dk
+    err = float(np.linalg.norm(g_ad[pick] - g_fd) / np.linalg.norm(g_fd))
+    return {"samples": n_check, "step_k": h, "rel_err": err, "valid_fraction": float(ok.mean())}
+
+
+def run_batched(args):
+    """64 frames of 192^2, frame f has 13 + (f*37 mod 77) golden-angle spokes of
+    384 samples; 12 coils; alpha 2, W 5.5 (not stated by the workload; chosen);
+    15 CG iterations.  Batched: one operator over all frames (uneven sample
+    counts), per-frame CG scalars, one CUDA graph for the whole solve.  Plain:
+    one operator + solve per frame, no graph."""
+    import torch
+    import gadgetron_b200 as gb
+    from gadgetron_b200 import synthetic as S
+    from gadgetron_b200._lib import lib
+    dev = torch.device("cuda:0")
+    F, N, mos, W, C, S_per, iters = 64, 192, 384, 5.5, 12, 384, 15
+    spokes = S.uneven_frame_spokes(F)
+    trajs = [S.radial_golden_angle_2d(s, S_per, profile_offset=sum(spokes[:f])) for f, s in enumerate(spokes)]
+    offs = np.cumsum([0] + [t.shape[0] for t in trajs]).tolist()
+    traj = np.concatenate(trajs, 0)
+    sq = np.concatenate([np.sqrt(S.ramp_dcw(t)) for t in trajs]).astype(np.float32)
+    csm = S.gaussian_bump_csm((N, N), C)
+    base = S.ellipse_phantom((N, N), 20, 77)
+    amp = np.random.default_rng(78).uniform(0.9, 1.1, F)
+    ph = (base[None] * amp[:, None, None]).astype(np.complex64)
+    csm_d = torch.from_numpy(csm).to(dev)
+    E = gb.cuNonCartesianSenseOperator(2)
+    E.setup((N, N), (mos, mos), W)
+    E.set_csm(csm_d)
+    sq_d = torch.from_numpy(sq).to(dev)
+    E.set_dcw(sq_d)
+    E.preprocess(torch.from_numpy(traj).to(dev), frame_offsets=offs)
+    y = torch.empty((C, offs[-1]), dtype=torch.complex64, device=dev)
+    E.mult_M(torch.from_numpy(ph).to(dev), y)
+    rms = float(y.abs().pow(2).mean().sqrt())
+    rng = np.random.default_rng(79)
+    noise = torch.from_numpy((0.01 * rms * (rng.standard_normal(y.shape) + 1j * rng.standard_normal(y.shape)) /
+                              np.sqrt(2)).astype(np.complex64)).to(dev)
+    d = (y + noise).contiguous()
+    cg = gb.cuCgSolver()
+    cg.set_encoding_operator(E)
+    cg.set_max_iterations(iters)
+    cg.set_tc_tolerance(0.0)
+    cg.set_frame_independent(True)
+    cg.set_use_graph(True)
+    xb = torch.empty((F, N, N), dtype=torch.complex64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    l0 = lib.gb_kernel_launch_count()
+    ms_b = _timed(lambda: cg.solve(d, xb), args.steps, args.warmup, flush, stream)
+    launches = (lib.gb_kernel_launch_count() - l0) // (args.steps + args.warmup)
+    # plain per-frame form
+    ops, solvers, ds, xs = [], [], [], []
+    for f in range(F):
+        Ef = gb.cuNonCartesianSenseOperator(2)
+        Ef.setup((N, N), (mos, mos), W)
+        Ef.set_csm(csm_d)
+        Ef.set_dcw(sq_d[offs[f]:offs[f + 1]].contiguous())
+        Ef.preprocess(torch.from_numpy(trajs[f]).to(dev))
+        cf = gb.cuCgSolver()
+        cf.set_encoding_operator(Ef)
+        cf.set_max_iterations(iters)
+        cf.set_tc_tolerance(0.0)
+        ops.append(Ef)
+        solvers.append(cf)
+        ds.append(d[:, offs[f]:offs[f + 1]].contiguous())
+        xs.append(torch.empty((1, N, N), dtype=torch.complex64, device=dev))
+
+    def plain():
+        for f in range(F):
+            solvers[f].solve(ds[f], xs[f])
+
+    ms_p = _timed(plain, max(2, args.steps // 4), 2, flush, stream)
+    xp = torch.cat(xs, 0)
+    err = float((xb - xp).abs().pow(2).sum().sqrt() / xp.abs().pow(2).sum().sqrt())
+    return {
+        "metric": "batched CG-SENSE ms/batch (64 uneven frames, 192^2, 12 coils, 15 it)",
+        "value": round(ms_b, 3), "unit": "ms/batch", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_b, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64 (fp32), fp64 CG reductions", "data": "synthetic",
+        "config": {"workload": "batched-uneven-cg-sense", "frames": F, "matrix": N, "matrix_os": mos, "W": W,
+                   "coils": C, "samples_total": offs[-1], "iterations": iters, "alpha_W": "chosen: 2.0, 5.5"},
+        "plain_per_frame_ms": round(ms_p, 3), "speedup_vs_plain": round(ms_p / ms_b, 2),
+        "batched_vs_plain_rel_l2": err, "gpu_launches_per_batch": int(launches),
+    }
+
+
+def run_precision(args):
+    """512^2 ellipse phantom, 24 variable-density Archimedean interleaves x 4096
+    (density 4x at the centre to 1x at the edge), 32 coils, alpha 1.25 (640^2),
+    W 4; compensated gridding, FP64 CG reductions, 3 refinements x 8 CG
+    iterations.  Errors vs FP64 direct NDFT (4096-sample subset) and vs the
+    oracle."""
+    import torch
+    import gadgetron_b200 as gb
+    from gadgetron_b200 import synthetic as S
+    from oracle import oracle as O
+    dev = torch.device("cuda:0")
+    N, mos, W, C = 512, 640, 4.0, 32
+    traj = S.spiral_archimedean_2d(24, 4096, N, 4.0)
+    M = traj.shape[0]
+    sq = np.sqrt(S.ramp_dcw(traj)).astype(np.float32)
+    csm = S.gaussian_bump_csm((N, N), C)
+    ph = S.ellipse_phantom((N, N), 20, 91)[None]
+    res = {"metric": "precision study (spiral 512^2, 32 coils, 3x8 refinement)", "unit": "ms/recon",
+           "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "config": {"workload": "precision-spiral", "matrix": N, "matrix_os": mos, "W": W, "coils": C,
+                      "samples": M, "refinements": 3, "iterations_each": 8}}
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    csm_d = torch.from_numpy(csm).to(dev)
+    sq_d = torch.from_numpy(sq).to(dev)
+    traj_d = torch.from_numpy(traj).to(dev)
+    out = {}
+    for flags, name in ((gb.FLAG_COMPENSATED, "compensated"), (0, "plain")):
+        E = gb.cuNonCartesianSenseOperator(2, flags=flags)
+        E.setup((N, N), (mos, mos), W)
+        E.set_csm(csm_d)
+        E.set_dcw(sq_d)
+        E.preprocess(traj_d)
+        y = torch.empty((C, M), dtype=torch.complex64, device=dev)
+        E.mult_M(torch.from_numpy(ph).to(dev), y)
+        cg = gb.cuCgSolver()
+        cg.set_encoding_operator(E)
+        cg.set_max_iterations(8)
+        cg.set_tc_tolerance(0.0)
+        cg.set_refinements(3)
+        cg.set_use_graph(True)
+        x = torch.empty((1, N, N), dtype=torch.complex64, device=dev)
+        ms = _timed(lambda: cg.solve(y, x), args.steps, args.warmup, flush, stream)
+        out[name] = (ms, y.cpu().numpy(), x.cpu().numpy())
+    ms, y, x = out["compensated"]
+    res["value"] = round(ms, 3)
+    res["ms_plain_accumulation"] = round(out["plain"][0], 3)
+    O.set_fft_workers(os.cpu_count() or 1)
+    idx = np.random.default_rng(4).choice(M, 4096, replace=False)
+    coil_imgs = csm[:4] * ph
+    yn = O.ndft_forward(coil_imgs, traj[idx], (mos, mos), dcw=sq[idx])
+    res["forward_rel_l2_vs_fp64_ndft_4096"] = O.rel_l2(y[:4][:, idx], yn)
+    P = O.OraclePlan((N, N), (mos, mos), W)
+    P.preprocess(traj[None])
+    yr = P.forward_c2nc(coil_imgs[:, None], sq[None])
+    res["forward_rel_l2_vs_oracle"] = O.rel_l2(y[:4], yr.reshape(4, -1))
+    res["forward_rel_l2_vs_oracle_plain_accumulation"] = O.rel_l2(out["plain"][1][:4], yr.reshape(4, -1))
+    res["recon_rel_l2_vs_phantom"] = O.rel_l2(x, ph)
+    res["recon_rel_l2_compensated_vs_plain"] = O.rel_l2(x, out["plain"][2])
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -416,6 +709,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="cg-sense-2d",
+                    choices=["cg-sense-2d", "nufft-2d", "nufft-3d", "batched", "precision"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -426,6 +721,13 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)
+        return 0
+
+    if args.workload != "cg-sense-2d":
+        fn = {"nufft-2d": lambda: run_nufft(args, 2), "nufft-3d": lambda: run_nufft(args, 3),
+              "batched": lambda: run_batched(args), "precision": lambda: run_precision(args)}[args.workload]
+        if rank == 0:
+            print(json.dumps(fn()), flush=True)
         return 0
 
     if world > 1:

@@ -6,6 +6,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "gb_internal.cuh"
 #include "gb_ops.hpp"
@@ -76,37 +77,6 @@ struct DeviceGuard {
     }
 };
 
-static void set_tiling(NufftPlan &p, const int *tile, int cg) {
-    const KParams &k = p.kp;
-    int t[kMaxD] = {1, 1, 1};
-    for (int d = 0; d < p.D; d++) t[d] = tile[d];
-    int cells = t[0] * t[1] * t[2];
-    for (int d = 0; d < p.D; d++)
-        if (t[d] <= 0 || k.mos[d] % t[d]) fail(GB_ERR_INVALID_ARGUMENT, "tile size must divide the oversampled size");
-    if (p.D == 1) {
-        if (t[0] % 32) fail(GB_ERR_INVALID_ARGUMENT, "1D tile must be a multiple of 32");
-    } else if (t[0] % 8 || t[1] % 4) {
-        fail(GB_ERR_INVALID_ARGUMENT, "tile x must be a multiple of 8 and y a multiple of 4");
-    }
-    if (cells > 4 * kThreads || (cells > kThreads && cells % kThreads) || (cells < kThreads && kThreads % cells))
-        fail(GB_ERR_INVALID_ARGUMENT, "tile must hold a divisor of 256 cells, or 512 or 1024 cells");
-    if (2 * k.hw + 1 > kWMax) fail(GB_ERR_INVALID_ARGUMENT, "kernel width too large");
-    // A footprint of at most 2*hw+1 cells must span at most 3 tiles per
-    // dimension (the binning records up to 3 tiles per dimension).
-    for (int d = 0; d < p.D; d++)
-        if (t[d] < 2 * k.hw && t[d] != k.mos[d])
-            fail(GB_ERR_INVALID_ARGUMENT, "tile must be at least W cells wide in every dimension");
-    if (cg != 1 && cg != 2 && cg != 4 && cg != 8 && cg != 16)
-        fail(GB_ERR_INVALID_ARGUMENT, "coil group must be 1, 2, 4, 8 or 16");
-    p.tiling.cg = cg;
-    for (int d = 0; d < kMaxD; d++) {
-        p.tiling.tile[d] = t[d];
-        p.kp.tile[d] = t[d];
-        p.kp.ntiles[d] = p.kp.mos[d] / t[d];
-    }
-    p.kp.ntiles_total = p.kp.ntiles[0] * p.kp.ntiles[1] * p.kp.ntiles[2];
-}
-
 }  // namespace gb
 
 using namespace gb;
@@ -162,7 +132,7 @@ static void default_tiling(NufftPlan &p) {
     // shrink for small grids while keeping >= 256 cells per tile
     for (int d = 0; d < p.D; d++)
         if (t[d] > p.kp.mos[d]) t[d] = (int)p.kp.mos[d];
-    set_tiling(p, t, 16);
+    plan_set_tiling(p, t, 16);
 }
 
 GB_API gb_status gb_nufft_plan_create(int D, const uint64_t *matrix_size, const uint64_t *matrix_size_os,
@@ -200,6 +170,7 @@ GB_API gb_status gb_nufft_preprocess(gb_nufft_plan plan, const float *trajectory
         if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
         DeviceGuard g((*plan->p).device);
         plan_preprocess((*plan->p), trajectory, num_samples_total, num_frames, frame_offsets, mode, S(stream));
+        if ((*plan->p).flags & GB_FLAG_AUTOTUNE) plan_autotune(*plan->p, 1, S(stream));
     });
 }
 
@@ -291,6 +262,14 @@ GB_API gb_status gb_nufft_get_info(gb_nufft_plan plan, int *D, uint64_t *matrix_
     });
 }
 
+GB_API gb_status gb_nufft_autotune(gb_nufft_plan plan, uint32_t num_batches, void *stream) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
+        DeviceGuard g((*plan->p).device);
+        plan_autotune(*plan->p, (int)num_batches, S(stream));
+    });
+}
+
 GB_API gb_status gb_nufft_get_tiling(gb_nufft_plan plan, int *tile, int *coil_group) {
     return guarded([&] {
         if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
@@ -305,10 +284,10 @@ GB_API gb_status gb_nufft_set_tiling(gb_nufft_plan plan, const int *tile, int co
         if (!plan || !tile) fail(GB_ERR_INVALID_ARGUMENT, "NULL argument");
         DeviceGuard g((*plan->p).device);
         NufftPlan &p = (*plan->p);
-        set_tiling(p, tile, coil_group);
-        if (p.prepped) {
-            // Re-bin with the new tiles: rebuild from the stored sorted data.
-            fail(GB_ERR_INVALID_ARGUMENT, "set the tiling before preprocess");
+        plan_set_tiling(p, tile, coil_group);
+        if (p.prepped) {   // re-bin the stored trajectory with the new tiles
+            std::vector<uint64_t> offs(p.frame_off.begin(), p.frame_off.end());
+            plan_preprocess(p, p.traj_copy.get(), (uint64_t)p.Mtot, p.F, offs.data(), p.prep_mode, nullptr);
         }
     });
 }
@@ -348,6 +327,8 @@ GB_API gb_status gb_sense_preprocess(gb_sense_op op, const float *trajectory, ui
         DeviceGuard g(op->s.plan.device);
         plan_preprocess(op->s.plan, trajectory, num_samples_total, num_frames, frame_offsets, GB_PREP_ALL,
                         S(stream));
+        if ((op->s.plan.flags & GB_FLAG_AUTOTUNE) && op->s.csm && op->s.ncoils > 0)
+            plan_autotune(op->s.plan, op->s.ncoils, S(stream));
     });
 }
 
@@ -389,6 +370,15 @@ GB_API gb_status gb_sense_mult_MH_M(gb_sense_op op, const void *in, void *out, i
         if (!op) fail(GB_ERR_INVALID_ARGUMENT, "NULL operator");
         DeviceGuard g(op->s.plan.device);
         sense_mult_MH_M(op->s, in, out, accumulate != 0, S(stream));
+    });
+}
+
+GB_API gb_status gb_sense_autotune(gb_sense_op op, void *stream) {
+    return guarded([&] {
+        if (!op) fail(GB_ERR_INVALID_ARGUMENT, "NULL operator");
+        if (!op->s.csm || op->s.ncoils <= 0) fail(GB_ERR_INVALID_ARGUMENT, "set_csm before autotune");
+        DeviceGuard g(op->s.plan.device);
+        plan_autotune(op->s.plan, op->s.ncoils, S(stream));
     });
 }
 

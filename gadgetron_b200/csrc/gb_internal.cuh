@@ -138,6 +138,8 @@ struct NufftPlan {
     // preprocess state
     bool prepped = false;
     uint64_t generation = 0;       // bumped by every preprocess (invalidates captured graphs)
+    DevBuf<float> traj_copy;       // the preprocessed trajectory (for re-binning)
+    gb_prep_mode prep_mode = GB_PREP_ALL;
     bool prepped_c2nc = false, prepped_nc2c = false;
     uint32_t F = 0;
     int64_t Mtot = 0;
@@ -183,6 +185,10 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
                      const uint64_t *frame_offsets, gb_prep_mode mode, cudaStream_t st);
 void plan_build_work(NufftPlan &p, cudaStream_t st);
 cufftHandle plan_fft(NufftPlan &p, int batches, cudaStream_t st);
+void plan_set_tiling(NufftPlan &p, const int *tile, int cg);
+// Times candidate tilings on the preprocessed trajectory with `nb` batches and
+// keeps the fastest (cached per workload key for later plans).
+void plan_autotune(NufftPlan &p, int nb, cudaStream_t st);
 
 // Sample-array layout flags for the convolution kernels.
 enum SampleLayout { LAYOUT_ORIGINAL = 0, LAYOUT_SORTED = 1 };

@@ -312,6 +312,11 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     const int D = p.D;
     const uint32_t nkeys = F * (uint32_t)k.ntiles_total;
 
+    // Keep the trajectory (re-binning for the autotuner needs it).
+    if (traj != p.traj_copy.get()) {
+        p.traj_copy.ensure((size_t)D * M);
+        GB_CUDA(cudaMemcpyAsync(p.traj_copy.get(), traj, (size_t)D * M * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    }
     DevBuf<int64_t> d_off;
     d_off.ensure(F + 1);
     GB_CUDA(cudaMemcpyAsync(d_off.get(), off.data(), (F + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
@@ -384,6 +389,7 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     // Both structures are built regardless of mode (they are cheap); the mode
     // is recorded for the reference's precondition checks.
     p.prepped_c2nc = p.prepped_nc2c = true;
+    p.prep_mode = mode;
     plan_build_work(p, st);
     p.prepped = true;
 }
@@ -477,6 +483,39 @@ void plan_build_work(NufftPlan &p, cudaStream_t st) {
     p.split_counter_groups = 0;   // (re)allocated by the gridding launcher
     (void)st;
 }
+
+// Validates and installs a tiling (tile shape and coil group).
+void plan_set_tiling(NufftPlan &p, const int *tile, int cg) {
+    const KParams &k = p.kp;
+    int t[kMaxD] = {1, 1, 1};
+    for (int d = 0; d < p.D; d++) t[d] = tile[d];
+    int cells = t[0] * t[1] * t[2];
+    for (int d = 0; d < p.D; d++)
+        if (t[d] <= 0 || k.mos[d] % t[d]) fail(GB_ERR_INVALID_ARGUMENT, "tile size must divide the oversampled size");
+    if (p.D == 1) {
+        if (t[0] % 32) fail(GB_ERR_INVALID_ARGUMENT, "1D tile must be a multiple of 32");
+    } else if (t[0] % 8 || t[1] % 4) {
+        fail(GB_ERR_INVALID_ARGUMENT, "tile x must be a multiple of 8 and y a multiple of 4");
+    }
+    if (cells > 4 * kThreads || (cells > kThreads && cells % kThreads) || (cells < kThreads && kThreads % cells))
+        fail(GB_ERR_INVALID_ARGUMENT, "tile must hold a divisor of 256 cells, or 512 or 1024 cells");
+    if (2 * k.hw + 1 > kWMax) fail(GB_ERR_INVALID_ARGUMENT, "kernel width too large");
+    // A footprint of at most 2*hw+1 cells must span at most 3 tiles per
+    // dimension (the binning records up to 3 tiles per dimension).
+    for (int d = 0; d < p.D; d++)
+        if (t[d] < 2 * k.hw && t[d] != k.mos[d])
+            fail(GB_ERR_INVALID_ARGUMENT, "tile must be at least W cells wide in every dimension");
+    if (cg != 1 && cg != 2 && cg != 4 && cg != 8 && cg != 16)
+        fail(GB_ERR_INVALID_ARGUMENT, "coil group must be 1, 2, 4, 8 or 16");
+    p.tiling.cg = cg;
+    for (int d = 0; d < kMaxD; d++) {
+        p.tiling.tile[d] = t[d];
+        p.kp.tile[d] = t[d];
+        p.kp.ntiles[d] = p.kp.mos[d] / t[d];
+    }
+    p.kp.ntiles_total = p.kp.ntiles[0] * p.kp.ntiles[1] * p.kp.ntiles[2];
+}
+
 
 cufftHandle plan_fft(NufftPlan &p, int batches, cudaStream_t st) {
     auto it = p.fft_plans.find(batches);

@@ -134,6 +134,10 @@ class cuNFFT_plan:
         check(lib.gb_nufft_get_tiling(self._h, tile, ctypes.byref(cg)))
         return tuple(tile[: self.D]), cg.value
 
+    def autotune(self, num_batches: int = 1):
+        """Time candidate tilings on this trajectory and keep the fastest."""
+        check(lib.gb_nufft_autotune(self._h, int(num_batches), _stream()))
+
     def set_tiling(self, tile: Sequence[int], coil_group: int):
         t = (ctypes.c_int * 3)(*(list(tile) + [1] * (3 - len(tile))))
         check(lib.gb_nufft_set_tiling(self._h, t, int(coil_group)))

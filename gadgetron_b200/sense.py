@@ -140,6 +140,10 @@ class cuNonCartesianSenseOperator:
         _check_tensor(out, torch.complex64, "out")
         check(lib.gb_sense_mult_MH_M(self._h, _ptr(inp), _ptr(out), int(bool(accumulate)), _stream()))
 
+    def autotune(self):
+        """Time candidate tilings for this trajectory and coil count; keep the fastest."""
+        check(lib.gb_sense_autotune(self._h, _stream()))
+
     def get_plan(self) -> cuNFFT_plan:
         h = ctypes.c_void_p()
         check(lib.gb_sense_get_nufft_plan(self._h, ctypes.byref(h)))

@@ -74,7 +74,7 @@ typedef enum gb_fft_mode { GB_FFT_FORWARDS = 0, GB_FFT_BACKWARDS = 1 } gb_fft_mo
 
 /* Plan flags. */
 #define GB_FLAG_COMPENSATED 0x1u   /* compensated (TwoSum) in-tile accumulation */
-#define GB_FLAG_AUTOTUNE    0x2u   /* time tile/coil-group candidates at preprocess */
+#define GB_FLAG_AUTOTUNE    0x2u   /* autotune at preprocess (plans: 1 batch; SENSE: its coils) */
 
 typedef struct gb_nufft_plan_s *gb_nufft_plan;
 typedef struct gb_sense_op_s *gb_sense_op;
@@ -197,6 +197,13 @@ GB_API gb_status gb_nufft_get_info(gb_nufft_plan plan, int *D, uint64_t *matrix_
                                    uint64_t *matrix_size_os, float *W,
                                    uint64_t *num_samples_total, uint32_t *num_frames);
 
+/* Autotuner: on a preprocessed plan, times candidate tile shapes and coil
+ * groups for num_batches batches (one gridding + one degridding pass each on
+ * this trajectory) and keeps the fastest; the choice is cached per
+ * (dimensions, sizes, W, frames, sample count, batches) for later plans.
+ * Synchronises the stream.  No reference counterpart. */
+GB_API gb_status gb_nufft_autotune(gb_nufft_plan plan, uint32_t num_batches, void *stream);
+
 /* Tile configuration used by the gridding kernels (chosen by the autotuner
  * when GB_FLAG_AUTOTUNE is set, else defaults), for inspection. */
 GB_API gb_status gb_nufft_get_tiling(gb_nufft_plan plan, int *tile, int *coil_group);
@@ -243,6 +250,9 @@ GB_API gb_status gb_sense_mult_MH_M(gb_sense_op op, const void *in, void *out,
                                     int accumulate, void *stream);
 
 GB_API gb_status gb_sense_get_nufft_plan(gb_sense_op op, gb_nufft_plan *plan);
+
+/* Autotunes the operator's plan for its coil count (csm must be set). */
+GB_API gb_status gb_sense_autotune(gb_sense_op op, void *stream);
 
 /* --------------------------------------------------------------------- CG */
 

@@ -217,3 +217,26 @@ def test_error_paths(cuda):
         gb.NFFT.make_plan((30, 30), (64, 64), 5.5)
     with pytest.raises(gb.GadgetronB200Error):
         gb.NFFT.make_plan((32, 32), (64, 64), 1.5)
+
+
+def test_autotune_keeps_parity(cuda):
+    case = radial_case(N=64, spokes=48, samples=128, batches=8, seed=21)
+    plan, orc, _ = _plan_and_oracle(case)
+    before = plan.get_tiling()
+    plan.autotune(8)
+    tile, cg = plan.get_tiling()
+    assert cg in (4, 8, 16) and len(tile) == 2
+    x = torch.from_numpy(case["img"]).to(cuda)
+    y = torch.empty((8, case["M"]), dtype=torch.complex64, device=cuda)
+    plan.compute(x, y, None, gb.NFFT_comp_mode.FORWARDS_C2NC)
+    ref = orc.forward_c2nc(case["img"])
+    assert rel_l2(y.cpu().numpy(), ref) <= PARITY_TOL
+    back = torch.empty_like(x)
+    plan.compute(y, back, None, gb.NFFT_comp_mode.BACKWARDS_NC2C)
+    assert rel_l2(back.cpu().numpy(), orc.backwards_nc2c(ref)) <= PARITY_TOL
+    # an explicit tiling re-bins the preprocessed trajectory
+    plan.set_tiling((32, 16), 8)
+    assert plan.get_tiling() == ((32, 16), 8)
+    plan.compute(x, y, None, gb.NFFT_comp_mode.FORWARDS_C2NC)
+    assert rel_l2(y.cpu().numpy(), ref) <= PARITY_TOL
+    del before
