@@ -66,6 +66,16 @@ __device__ __forceinline__ float sign_of(int g) { return (g & 1) ? -1.f : 1.f; }
 
 // --------------------------------------------------------------- NC2C -----
 
+// Shared-memory stage of one chunk of kChunk samples for the gridding kernel.
+template <int CG>
+struct GridStage {
+    float w[kChunk][3][kWMax];   // separable weights (checkerboard folded in)
+    float2 v[kChunk][CG];        // sample values (density weights folded in)
+    int a[kChunk][3];            // tile-local start of the footprint (wrapped)
+    int n[kChunk][3];            // taps per dimension
+    uint32_t mask[kChunk];       // warps whose cell patches the footprint overlaps
+};
+
 template <int CG, int CPT, bool COMP>
 __global__ void __launch_bounds__(kThreads)
 k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__ grid) {
@@ -81,11 +91,7 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
     const int tz = tile / (k.ntiles[0] * k.ntiles[1]);
     const int org[3] = {tx * k.tile[0], ty * k.tile[1], tz * k.tile[2]};
 
-    __shared__ int s_a[kChunk][3];
-    __shared__ int s_n[kChunk][3];
-    __shared__ float s_w[kChunk][3][kWMax];
-    __shared__ float2 s_v[kChunk][CG];
-    __shared__ uint32_t s_mask[kChunk];
+    __shared__ GridStage<CG> stage[2];
     __shared__ int s_last;
 
     // Cell ownership: warp patches of PX x PY cells.
@@ -113,70 +119,108 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
             if (COMP) cmp[c][q][0] = cmp[c][q][1] = 0.f;
         }
 
-    for (int base = it.begin; base < it.end; base += kChunk) {
-        const int cnt = min(kChunk, it.end - base);
-        // Stage weights: one (sample, dim, tap) per thread-iteration.
-        for (int e = threadIdx.x; e < kChunk * 3 * kWMax; e += kThreads) {
-            const int i = e / (3 * kWMax);
-            const int d = (e / kWMax) % 3;
-            const int t = e % kWMax;
+    // Staging work per thread: weight entries (sample, dim, tap), value
+    // entries (sample, coil) and, for threads < kChunk, one sample's
+    // footprint and warp mask.  Raw global values are prefetched into
+    // registers one chunk ahead so their latency overlaps the accumulation.
+    constexpr int kWE = (kChunk * 3 * kWMax + kThreads - 1) / kThreads;
+    constexpr int kVE = (kChunk * CG + kThreads - 1) / kThreads;
+    float pw[kWE];
+    float2 pv[kVE];
+    float pd[kVE];
+    float ps[3];
+
+    auto prefetch = [&](int base, int cnt) {
+#pragma unroll
+        for (int q = 0; q < kWE; q++) {
+            const int e = threadIdx.x + q * kThreads;
+            const int i = e / (3 * kWMax), d = (e / kWMax) % 3;
+            pw[q] = 0.f;
+            if (e < kChunk * 3 * kWMax && i < cnt && d < k.D)
+                pw[q] = a.pos[(int64_t)d * a.Mtot + a.list[base + i]];
+        }
+#pragma unroll
+        for (int q = 0; q < kVE; q++) {
+            const int e = threadIdx.x + q * kThreads;
+            const int i = e / CG, c = e % CG;
+            pv[q] = make_float2(0.f, 0.f);
+            pd[q] = 1.f;
+            if (e < kChunk * CG && i < cnt && b0 + c < a.nb) {
+                const uint32_t si = a.list[base + i];
+                const uint32_t j = a.perm[si];
+                const int64_t idx = (a.layout == LAYOUT_SORTED) ? (int64_t)si : (int64_t)j;
+                pv[q] = samples[(int64_t)(b0 + c) * a.Mtot + idx];
+                if (a.dcw) pd[q] = a.dcw[j];
+            }
+        }
+        if (threadIdx.x < kChunk) {
+            const int i = threadIdx.x;
+            for (int d = 0; d < 3; d++)
+                ps[d] = (i < cnt && d < k.D) ? a.pos[(int64_t)d * a.Mtot + a.list[base + i]] : 0.f;
+        }
+    };
+
+    auto stage_chunk = [&](GridStage<CG> &S, int cnt) {
+#pragma unroll
+        for (int q = 0; q < kWE; q++) {
+            const int e = threadIdx.x + q * kThreads;
+            if (e >= kChunk * 3 * kWMax) break;
+            const int i = e / (3 * kWMax), d = (e / kWMax) % 3, t = e % kWMax;
             float w = 0.f;
             if (i < cnt) {
                 if (d < k.D) {
-                    const uint32_t si = a.list[base + i];
-                    const float s = a.pos[(int64_t)d * a.Mtot + si];
+                    const float s = pw[q];
                     const int lo = (int)ceilf(s - k.radius);
                     const int n = (int)floorf(s + k.radius) - lo + 1;
                     if (t < n) {
                         const int p = lo + t;
                         w = kb_weight_1d(fabsf(s - (float)p), k.mos_f[d], k.one_over_W, k.beta[d], k.radius);
-                        if (a.sign_fold) w *= sign_of(wrapmod(p - k.hw, k.mos[d]));
-                    }
-                    if (t == 0) {
-                        s_a[i][d] = wrapmod(lo - k.hw - org[d], k.mos[d]);
-                        s_n[i][d] = min(n, kWMax);
+                        if (a.sign_fold) {
+                            int g = p - k.hw;   // parity of (p - hw) mod mos (mos is even)
+                            w *= sign_of(g & 1);
+                        }
                     }
                 } else {
                     w = (t == 0) ? 1.f : 0.f;
-                    if (t == 0) { s_a[i][d] = 0; s_n[i][d] = 1; }
                 }
             }
-            s_w[i][d][t] = w;
+            S.w[i][d][t] = w;
         }
-        // Stage values (density weights folded in).
-        for (int e = threadIdx.x; e < kChunk * CG; e += kThreads) {
+#pragma unroll
+        for (int q = 0; q < kVE; q++) {
+            const int e = threadIdx.x + q * kThreads;
+            if (e >= kChunk * CG) break;
             const int i = e / CG, c = e % CG;
-            float2 v = make_float2(0.f, 0.f);
-            if (i < cnt && b0 + c < a.nb) {
-                const uint32_t si = a.list[base + i];
-                const uint32_t j = a.perm[si];
-                const int64_t idx = (a.layout == LAYOUT_SORTED) ? (int64_t)si : (int64_t)j;
-                v = samples[(int64_t)(b0 + c) * a.Mtot + idx];
-                if (a.dcw) {
-                    const float dw = a.dcw[j];
-                    v.x = dw * v.x;
-                    v.y = dw * v.y;
-                }
+            float2 v = pv[q];
+            if (a.dcw) {
+                v.x = pd[q] * v.x;
+                v.y = pd[q] * v.y;
             }
-            s_v[i][c] = v;
+            S.v[i][c] = v;
         }
-        __syncthreads();
-        // Which warps' cell patches each staged sample overlaps.
         if (threadIdx.x < kChunk) {
             const int i = threadIdx.x;
             uint32_t m = 0;
             if (i < cnt) {
                 int lo[3], hi[3];
                 for (int d = 0; d < 3; d++) {
+                    int a_ = 0, n = 1;
+                    if (d < k.D) {
+                        const float s = ps[d];
+                        const int l = (int)ceilf(s - k.radius);
+                        n = min((int)floorf(s + k.radius) - l + 1, kWMax);
+                        a_ = wrapmod(l - k.hw - org[d], k.mos[d]);
+                    }
+                    S.a[i][d] = a_;
+                    S.n[i][d] = n;
                     const int T = k.tile[d];
                     if (k.ntiles[d] == 1) {   // footprint may wrap inside the tile
                         lo[d] = 0;
                         hi[d] = T - 1;
                     } else {
-                        const int a_ = s_a[i][d];
                         const int st = (a_ < T) ? a_ : a_ - k.mos[d];
                         lo[d] = max(st, 0);
-                        hi[d] = min(st + s_n[i][d] - 1, T - 1);
+                        hi[d] = min(st + n - 1, T - 1);
                     }
                 }
                 for (int w = 0; w < 8; w++)
@@ -188,25 +232,39 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
                             m |= 1u << w;
                     }
             }
-            s_mask[i] = m;
+            S.mask[i] = m;
         }
-        __syncthreads();
-        uint32_t bits = __ballot_sync(0xffffffffu, lane < cnt && ((s_mask[lane] >> warp) & 1u));
+    };
+
+    int cur = 0;
+    if (it.begin < it.end) {
+        const int cnt0 = min(kChunk, it.end - it.begin);
+        prefetch(it.begin, cnt0);
+        stage_chunk(stage[0], cnt0);
+    }
+    __syncthreads();
+    for (int base = it.begin; base < it.end; base += kChunk) {
+        const int cnt = min(kChunk, it.end - base);
+        const int nbase = base + kChunk;
+        const int ncnt = nbase < it.end ? min(kChunk, it.end - nbase) : 0;
+        if (ncnt > 0) prefetch(nbase, ncnt);
+        GridStage<CG> &S = stage[cur];
+        uint32_t bits = __ballot_sync(0xffffffffu, lane < cnt && ((S.mask[lane] >> warp) & 1u));
         while (bits) {
             const int i = __ffs(bits) - 1;
             bits &= bits - 1;
-            const int a0 = s_a[i][0], a1 = s_a[i][1], a2 = s_a[i][2];
-            const int n0 = s_n[i][0], n1 = s_n[i][1], n2 = s_n[i][2];
+            const int a0 = S.a[i][0], a1 = S.a[i][1], a2 = S.a[i][2];
+            const int n0 = S.n[i][0], n1 = S.n[i][1], n2 = S.n[i][2];
 #pragma unroll
             for (int c = 0; c < CPT; c++) {
                 int o0 = lc[c][0] - a0; if (o0 < 0) o0 += k.mos[0];
                 int o1 = lc[c][1] - a1; if (o1 < 0) o1 += k.mos[1];
                 int o2 = lc[c][2] - a2; if (o2 < 0) o2 += k.mos[2];
                 if (o0 < n0 && o1 < n1 && o2 < n2) {
-                    const float w = (s_w[i][0][o0] * s_w[i][1][o1]) * s_w[i][2][o2];
+                    const float w = (S.w[i][0][o0] * S.w[i][1][o1]) * S.w[i][2][o2];
 #pragma unroll
                     for (int q = 0; q < CG; q++) {
-                        const float2 v = s_v[i][q];
+                        const float2 v = S.v[i][q];
                         if (COMP) {
                             float y0 = w * v.x - cmp[c][q][0];
                             float t0 = acc[c][q][0] + y0;
@@ -224,7 +282,9 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
                 }
             }
         }
+        if (ncnt > 0) stage_chunk(stage[cur ^ 1], ncnt);
         __syncthreads();
+        cur ^= 1;
     }
 
     const int64_t G = k.G;
@@ -357,22 +417,34 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
     float2 *tile_s = reinterpret_cast<float2 *>(smem_raw);
     Stage *stages = reinterpret_cast<Stage *>(tile_s + (((size_t)cellsR * CG + 1) & ~(size_t)1));
 
-    // Stage the region, coil fastest.
-    for (int e = threadIdx.x; e < cellsR * CG; e += kThreads) {
-        const int c = e % CG;
-        const int cell = e / CG;
-        const int rx = cell % R0, ry = (cell / R0) % R1, rz = cell / (R0 * R1);
-        const int gx = wrapmod(org[0] - h0 + rx, k.mos[0]);
-        const int gy = wrapmod(org[1] - h1 + ry, k.mos[1]);
-        const int gz = wrapmod(org[2] - h2 + rz, k.mos[2]);
-        float2 v = make_float2(0.f, 0.f);
-        if (b0 + c < a.nb)
-            v = __ldg(&grid[((int64_t)(b0 + c) * a.F + f) * k.G + ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + gx]);
-        tile_s[e] = v;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // Stage the region, coil fastest: a warp per region row, lanes over
+    // (x, coil) with coil fastest (conflict-free shared stores); the periodic
+    // wrap needs one conditional per coordinate (|offset| < mos).
+    {
+        const int rowElems = R0 * CG;
+        const int gx0 = org[0] - h0;
+        for (int row = warp; row < R1 * R2; row += 8) {
+            const int ry = row % R1, rz = row / R1;
+            int gy = org[1] - h1 + ry;
+            gy = gy < 0 ? gy + k.mos[1] : (gy >= k.mos[1] ? gy - k.mos[1] : gy);
+            int gz = org[2] - h2 + rz;
+            gz = gz < 0 ? gz + k.mos[2] : (gz >= k.mos[2] ? gz - k.mos[2] : gz);
+            const int64_t rowoff = (int64_t)f * k.G + ((int64_t)gz * k.mos[1] + gy) * k.mos[0];
+            float2 *dst = tile_s + (size_t)row * rowElems;
+            for (int e = lane; e < rowElems; e += 32) {
+                const int c = e % CG;          // CG is a power of two
+                const int rx = e / CG;
+                int gx = gx0 + rx;
+                gx = gx < 0 ? gx + k.mos[0] : (gx >= k.mos[0] ? gx - k.mos[0] : gx);
+                float2 v = make_float2(0.f, 0.f);
+                if (b0 + c < a.nb) v = __ldg(&grid[(int64_t)(b0 + c) * a.F * k.G + rowoff + gx]);
+                dst[e] = v;
+            }
+        }
     }
     __syncthreads();
 
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int sl = lane / LPS, ll = lane % LPS;
     Stage &S = stages[warp];
     const bool D3 = k.D > 2;

@@ -139,6 +139,12 @@ struct NufftPlan {
     bool prepped = false;
     uint64_t generation = 0;       // bumped by every preprocess (invalidates captured graphs)
     DevBuf<float> traj_copy;       // the preprocessed trajectory (for re-binning)
+    // preprocessing scratch, kept between calls (no allocation when sizes repeat)
+    DevBuf<float> pp_pos;
+    DevBuf<uint32_t> pp_key, pp_idx, pp_key_sorted, pp_counts, pp_pcnt, pp_poff, pp_pkey, pp_pval, pp_pkey_sorted;
+    DevBuf<unsigned char> pp_cub;
+    DevBuf<int64_t> pp_off;
+    DevBuf<int> pp_err;
     gb_prep_mode prep_mode = GB_PREP_ALL;
     bool prepped_c2nc = false, prepped_nc2c = false;
     uint32_t F = 0;
@@ -186,6 +192,9 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
 void plan_build_work(NufftPlan &p, cudaStream_t st);
 cufftHandle plan_fft(NufftPlan &p, int batches, cudaStream_t st);
 void plan_set_tiling(NufftPlan &p, const int *tile, int cg);
+// Hash of every buffer address and count the convolution kernels' launches
+// depend on: equal signatures mean a captured graph is still valid.
+uint64_t plan_layout_signature(const NufftPlan &p, int nbf);
 // Times candidate tilings on the preprocessed trajectory with `nb` batches and
 // keeps the fastest (cached per workload key for later plans).
 void plan_autotune(NufftPlan &p, int nb, cudaStream_t st);

@@ -584,7 +584,8 @@ void cg_solve(CgSolver &cg, const void *d, void *x_out, double *hist, uint32_t *
     cg_prepare(cg, st);
     if (cg.use_graph) {
         GraphKey key{d, x_out, hist, cg.iterations, cg.refinements, cg.x0, cg.precond, cg.kappa, cg.weight,
-                     cg.tol, s.csm, s.dcw, s.ncoils, s.plan.generation, cg.independent_frames};
+                     cg.tol, s.csm, s.dcw, s.ncoils, plan_layout_signature(s.plan, s.ncoils * (int)s.plan.F),
+                     cg.independent_frames};
         if (!cg.graph_exec || !(key == cg.graph_key)) {
             cudaStream_t cs;
             GB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));

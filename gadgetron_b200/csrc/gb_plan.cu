@@ -260,25 +260,21 @@ __global__ void k_write_pairs(KParams k, int64_t M, const float *__restrict__ po
 }
 
 template <class T>
-static void exclusive_scan(const T *in, T *out, int64_t n, cudaStream_t st) {
+static void exclusive_scan(const T *in, T *out, int64_t n, DevBuf<unsigned char> &tmp, cudaStream_t st) {
     size_t bytes = 0;
     GB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, st));
-    DevBuf<unsigned char> tmp;
     tmp.ensure(bytes);
     GB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, st));
-    GB_CUDA(cudaStreamSynchronize(st));
 }
 
-static void sort_pairs(uint32_t *keys_in, uint32_t *keys_out, uint32_t *vals_in,
-                       uint32_t *vals_out, int64_t n, int end_bit, cudaStream_t st) {
+static void sort_pairs(uint32_t *keys_in, uint32_t *keys_out, uint32_t *vals_in, uint32_t *vals_out, int64_t n,
+                       int end_bit, DevBuf<unsigned char> &tmp, cudaStream_t st) {
     size_t bytes = 0;
-    GB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys_in, keys_out, vals_in, vals_out,
-                                            (int)n, 0, end_bit, st));
-    DevBuf<unsigned char> tmp;
+    GB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys_in, keys_out, vals_in, vals_out, (int)n, 0,
+                                            end_bit, st));
     tmp.ensure(bytes);
-    GB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, keys_in, keys_out, vals_in, vals_out,
-                                            (int)n, 0, end_bit, st));
-    GB_CUDA(cudaStreamSynchronize(st));
+    GB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, keys_in, keys_out, vals_in, vals_out, (int)n, 0,
+                                            end_bit, st));
 }
 
 static int bits_for(uint64_t n) {
@@ -317,16 +313,16 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
         p.traj_copy.ensure((size_t)D * M);
         GB_CUDA(cudaMemcpyAsync(p.traj_copy.get(), traj, (size_t)D * M * sizeof(float), cudaMemcpyDeviceToDevice, st));
     }
-    DevBuf<int64_t> d_off;
+    DevBuf<int64_t> &d_off = p.pp_off;
     d_off.ensure(F + 1);
     GB_CUDA(cudaMemcpyAsync(d_off.get(), off.data(), (F + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-    DevBuf<float> pos;
+    DevBuf<float> &pos = p.pp_pos;
     pos.ensure((size_t)D * M);
-    DevBuf<uint32_t> key, idx, key_sorted;
+    DevBuf<uint32_t> &key = p.pp_key, &idx = p.pp_idx, &key_sorted = p.pp_key_sorted;
     key.ensure(M);
     idx.ensure(M);
     key_sorted.ensure(M);
-    DevBuf<int> err;
+    DevBuf<int> &err = p.pp_err;
     err.ensure(1);
     GB_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), st));
     const int TB = 256;
@@ -340,33 +336,34 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
 
     // Stable sort of samples by home key (frame, tile).
     p.perm.ensure(M);
-    sort_pairs(key.get(), key_sorted.get(), idx.get(), p.perm.get(), M, bits_for(nkeys), st);
+    sort_pairs(key.get(), key_sorted.get(), idx.get(), p.perm.get(), M, bits_for(nkeys), p.pp_cub, st);
     p.pos_sorted.ensure((size_t)D * M);
     k_gather_pos<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(D, M, pos.get(), p.perm.get(),
                                                                 p.pos_sorted.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 
     // Home ranges.
-    DevBuf<uint32_t> counts;
+    DevBuf<uint32_t> &counts = p.pp_counts;
     counts.ensure(nkeys + 1);
     GB_CUDA(cudaMemsetAsync(counts.get(), 0, (nkeys + 1) * sizeof(uint32_t), st));
     k_histogram<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(key_sorted.get(), M, counts.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
     p.home_off.ensure(nkeys + 1);
-    exclusive_scan(counts.get(), p.home_off.get(), (int64_t)nkeys + 1, st);
+    exclusive_scan(counts.get(), p.home_off.get(), (int64_t)nkeys + 1, p.pp_cub, st);
 
     // Gridding pair lists.
-    DevBuf<uint32_t> pcnt, poff;
+    DevBuf<uint32_t> &pcnt = p.pp_pcnt, &poff = p.pp_poff;
     pcnt.ensure(M + 1);
     poff.ensure(M + 1);
     GB_CUDA(cudaMemsetAsync(pcnt.get() + M, 0, sizeof(uint32_t), st));
     k_count_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(), pcnt.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
-    exclusive_scan(pcnt.get(), poff.get(), M + 1, st);
+    exclusive_scan(pcnt.get(), poff.get(), M + 1, p.pp_cub, st);
     uint32_t npairs = 0;
-    GB_CUDA(cudaMemcpy(&npairs, poff.get() + M, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    GB_CUDA(cudaMemcpyAsync(&npairs, poff.get() + M, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaStreamSynchronize(st));
     p.total_pairs = npairs;
-    DevBuf<uint32_t> pkey, pval, pkey_sorted;
+    DevBuf<uint32_t> &pkey = p.pp_pkey, &pval = p.pp_pval, &pkey_sorted = p.pp_pkey_sorted;
     pkey.ensure(npairs);
     pval.ensure(npairs);
     pkey_sorted.ensure(npairs);
@@ -374,12 +371,12 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     k_write_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(), key_sorted.get(),
                                                                  poff.get(), pkey.get(), pval.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
-    sort_pairs(pkey.get(), pkey_sorted.get(), pval.get(), p.grid_list.get(), npairs, bits_for(nkeys), st);
+    sort_pairs(pkey.get(), pkey_sorted.get(), pval.get(), p.grid_list.get(), npairs, bits_for(nkeys), p.pp_cub, st);
     GB_CUDA(cudaMemsetAsync(counts.get(), 0, (nkeys + 1) * sizeof(uint32_t), st));
     k_histogram<<<(unsigned)((npairs + TB - 1) / TB), TB, 0, st>>>(pkey_sorted.get(), npairs, counts.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
     p.grid_off.ensure(nkeys + 1);
-    exclusive_scan(counts.get(), p.grid_off.get(), (int64_t)nkeys + 1, st);
+    exclusive_scan(counts.get(), p.grid_off.get(), (int64_t)nkeys + 1, p.pp_cub, st);
 
     p.F = F;
     p.Mtot = M;
@@ -400,8 +397,9 @@ void plan_build_work(NufftPlan &p, cudaStream_t st) {
     const KParams &k = p.kp;
     const uint32_t nkeys = p.F * (uint32_t)k.ntiles_total;
     std::vector<uint32_t> hoff(nkeys + 1), goff(nkeys + 1);
-    GB_CUDA(cudaMemcpy(hoff.data(), p.home_off.get(), (nkeys + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    GB_CUDA(cudaMemcpy(goff.data(), p.grid_off.get(), (nkeys + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    GB_CUDA(cudaMemcpyAsync(hoff.data(), p.home_off.get(), (nkeys + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaMemcpyAsync(goff.data(), p.grid_off.get(), (nkeys + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaStreamSynchronize(st));
     p.h_home_counts.resize(nkeys);
     for (uint32_t i = 0; i < nkeys; i++) p.h_home_counts[i] = hoff[i + 1] - hoff[i];
 
@@ -471,17 +469,38 @@ void plan_build_work(NufftPlan &p, cudaStream_t st) {
     p.n_deg_items = (int)deg.size();
     p.deg_items.ensure(std::max<size_t>(1, deg.size()));
     if (!deg.empty())
-        GB_CUDA(cudaMemcpy(p.deg_items.get(), deg.data(), deg.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
+        GB_CUDA(cudaMemcpyAsync(p.deg_items.get(), deg.data(), deg.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
     p.n_grd_items = (int)grd.size();
     p.grd_items.ensure(std::max<size_t>(1, grd.size()));
-    GB_CUDA(cudaMemcpy(p.grd_items.get(), grd.data(), grd.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
+    GB_CUDA(cudaMemcpyAsync(p.grd_items.get(), grd.data(), grd.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
     p.n_splits = (int)splits.size();
     p.n_slots = slots;
     p.splits.ensure(std::max<size_t>(1, splits.size()));
     if (!splits.empty())
-        GB_CUDA(cudaMemcpy(p.splits.get(), splits.data(), splits.size() * sizeof(SplitInfo), cudaMemcpyHostToDevice));
+        GB_CUDA(cudaMemcpyAsync(p.splits.get(), splits.data(), splits.size() * sizeof(SplitInfo), cudaMemcpyHostToDevice, st));
     p.split_counter_groups = 0;   // (re)allocated by the gridding launcher
-    (void)st;
+    GB_CUDA(cudaStreamSynchronize(st));   // host vectors above go out of scope
+}
+
+uint64_t plan_layout_signature(const NufftPlan &p, int nbf) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) {
+        for (int b = 0; b < 8; b++) {
+            h ^= (v >> (8 * b)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    };
+    const void *ptrs[] = {p.pos_sorted.get(), p.perm.get(), p.grid_list.get(), p.grd_items.get(),
+                          p.deg_items.get(), p.splits.get(), p.partials.get(), p.split_counters.get(),
+                          p.img_os.get(), p.kgrid.get(), p.samp_ws.get(), p.deap_img.get(), p.deap_os.get()};
+    for (const void *q : ptrs) mix((uint64_t)(uintptr_t)q);
+    const int64_t vals[] = {p.n_deg_items, p.n_grd_items, p.n_splits, p.n_slots, p.Mtot, (int64_t)p.F,
+                            p.tiling.tile[0], p.tiling.tile[1], p.tiling.tile[2], p.tiling.cg,
+                            p.split_counter_groups, (int64_t)p.split_counters.n, (int64_t)p.partials.n, nbf};
+    for (int64_t v : vals) mix((uint64_t)v);
+    auto it = p.fft_plans.find(nbf);
+    mix(it == p.fft_plans.end() ? 0ull : (uint64_t)it->second);
+    return h;
 }
 
 // Validates and installs a tiling (tile shape and coil group).
