@@ -60,6 +60,7 @@ struct ConvArgs {
     float2 *partials;
     unsigned int *counters;
     int ncg;
+    long long part_elems;     // float2 elements of one CTA's partial tile
 };
 
 __device__ __forceinline__ float sign_of(int g) { return (g & 1) ? -1.f : 1.f; }
@@ -249,9 +250,11 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
         const int ncnt = nbase < it.end ? min(kChunk, it.end - nbase) : 0;
         if (ncnt > 0) prefetch(nbase, ncnt);
         GridStage<CG> &S = stage[cur];
-        uint32_t bits = __ballot_sync(0xffffffffu, lane < cnt && ((S.mask[lane] >> warp) & 1u));
+        for (int half = 0; half < kChunk / 32; half++) {
+        uint32_t bits = __ballot_sync(0xffffffffu, half * 32 + lane < cnt &&
+                                                       ((S.mask[half * 32 + lane] >> warp) & 1u));
         while (bits) {
-            const int i = __ffs(bits) - 1;
+            const int i = half * 32 + __ffs(bits) - 1;
             bits &= bits - 1;
             const int a0 = S.a[i][0], a1 = S.a[i][1], a2 = S.a[i][2];
             const int n0 = S.n[i][0], n1 = S.n[i][1], n2 = S.n[i][2];
@@ -281,6 +284,7 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
                     }
                 }
             }
+        }
         }
         if (ncnt > 0) stage_chunk(stage[cur ^ 1], ncnt);
         __syncthreads();
@@ -363,6 +367,292 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
     }
 }
 
+// ------------------------------------------------- NC2C, row variant -----
+//
+// Gridding for coil groups of 8 or 16 without compensation.  The tile is cut
+// into regions of ROWS x RW cells (ROWS = 64 / CG rows of RW columns, one
+// z-slice); warp w owns regions w, w + 8, ... (RPW of them).  A lane is a
+// (coil pair, row) of a region and accumulates that row's RW cells for two
+// coils in registers, so every lane of a warp works on every sample that
+// touches the region.  One visit (sample, region) costs a 16-byte value load,
+// the row's y (and z) weight, RW x-weights read as float4 from a per-sample
+// weight row laid over the tile (zero outside the footprint) and 4*RW FMAs.
+// Sample order per cell is the list order, as in k_grid_nc2c: the result is
+// bit-reproducible.
+
+// Floats per staged sample weight row: tile x + tile y (+ tile z), padded to
+// a multiple of 4 so every row starts on a 16-byte boundary.
+__host__ __device__ __forceinline__ int row_tsp(const KParams &k) {
+    const int ts = k.tile[0] + k.tile[1] + (k.D == 3 ? k.tile[2] : 0);
+    return (ts + 3) & ~3;
+}
+
+__host__ __device__ __forceinline__ int row_stage_bytes(const KParams &k, int cg) {
+    return kChunk * (row_tsp(k) * 4 + cg * 8 + 16);
+}
+
+template <int CG, int RW, int RPW, bool D3>
+__global__ void __launch_bounds__(kThreads, 2)
+k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__ grid) {
+    constexpr int CP = CG / 2;      // lanes per row: one per coil pair
+    constexpr int ROWS = 32 / CP;   // rows per region
+    constexpr int D = D3 ? 3 : 2;
+    constexpr int kWU = kChunk * D * 2;                  // weight-row units (sample, dim, half)
+    constexpr int kWP = (kWU + kThreads - 1) / kThreads;
+    constexpr int kVE = (kChunk * CG + kThreads - 1) / kThreads;
+    extern __shared__ __align__(16) unsigned char g_rows_smem[];
+    __shared__ int s_last;
+
+    const KParams &k = a.k;
+    const int grp = blockIdx.y;
+    const int b0 = grp * CG;
+    const WorkItem it = a.items[blockIdx.x];
+    const int f = it.ft / k.ntiles_total;
+    const int tile = it.ft - f * k.ntiles_total;
+    const int tx = tile % k.ntiles[0];
+    const int ty = (tile / k.ntiles[0]) % k.ntiles[1];
+    const int tz = tile / (k.ntiles[0] * k.ntiles[1]);
+    const int org0 = tx * k.tile[0], org1 = ty * k.tile[1], org2 = tz * k.tile[2];
+    const int T0 = k.tile[0], T1 = k.tile[1];
+    const int tsp = row_tsp(k);
+    const int stage_bytes = row_stage_bytes(k, CG);
+
+    auto stage_wt = [&](int s) { return reinterpret_cast<float *>(g_rows_smem + s * stage_bytes); };
+    auto stage_v = [&](int s) {
+        return reinterpret_cast<float2 *>(g_rows_smem + s * stage_bytes + kChunk * tsp * 4);
+    };
+    auto stage_rng = [&](int s) {
+        return reinterpret_cast<uint4 *>(g_rows_smem + s * stage_bytes + kChunk * tsp * 4 + kChunk * CG * 8);
+    };
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int cp = lane % CP, row = lane / CP;
+    const int nrx = T0 / RW, nry = T1 / ROWS;
+    int qx0[RPW], qy0[RPW], qz[RPW];
+#pragma unroll
+    for (int c = 0; c < RPW; c++) {
+        const int q = warp + 8 * c;
+        qx0[c] = (q % nrx) * RW;
+        qy0[c] = ((q / nrx) % nry) * ROWS;
+        qz[c] = q / (nrx * nry);
+    }
+
+    float acc[RPW][RW][4];
+#pragma unroll
+    for (int c = 0; c < RPW; c++)
+#pragma unroll
+        for (int j = 0; j < RW; j++) acc[c][j][0] = acc[c][j][1] = acc[c][j][2] = acc[c][j][3] = 0.f;
+
+    float pw[kWP];
+    float2 pv[kVE];
+    float pd[kVE];
+
+    auto prefetch = [&](int base, int cnt) {
+#pragma unroll
+        for (int q = 0; q < kWP; q++) {
+            const int u = threadIdx.x + q * kThreads;
+            const int pr = u >> 1, i = pr / D, d = pr - i * D;
+            pw[q] = 0.f;
+            if (u < kWU && i < cnt) pw[q] = a.pos[(int64_t)d * a.Mtot + a.list[base + i]];
+        }
+#pragma unroll
+        for (int q = 0; q < kVE; q++) {
+            const int e = threadIdx.x + q * kThreads;
+            const int i = e / CG, c = e % CG;
+            pv[q] = make_float2(0.f, 0.f);
+            pd[q] = 1.f;
+            if (e < kChunk * CG && i < cnt && b0 + c < a.nb) {
+                const uint32_t si = a.list[base + i];
+                const uint32_t j = a.perm[si];
+                const int64_t idx = (a.layout == LAYOUT_SORTED) ? (int64_t)si : (int64_t)j;
+                pv[q] = samples[(int64_t)(b0 + c) * a.Mtot + idx];
+                if (a.dcw) pd[q] = a.dcw[j];
+            }
+        }
+    };
+
+    // Writes the prefetched chunk into stage s: per sample and dimension a
+    // weight row over the tile (zeroed, then the footprint's taps written by
+    // the same pair of lanes after __syncwarp), the tile-local footprint
+    // range, and the values with the density weights folded in.
+    auto stage_chunk = [&](int s, int cnt) {
+        float *wt = stage_wt(s);
+        float2 *sv = stage_v(s);
+        unsigned *rng = reinterpret_cast<unsigned *>(stage_rng(s));
+#pragma unroll
+        for (int q = 0; q < kWP; q++) {
+            const int u = threadIdx.x + q * kThreads;
+            const int pr = u >> 1, i = pr / D, d = pr - i * D, sub = u & 1;
+            const bool active = u < kWU && i < cnt;
+            const int Td = k.tile[d];
+            float *rowp = wt + i * tsp + (d == 0 ? 0 : (d == 1 ? T0 : T0 + T1));
+            if (active)
+                for (int e = sub; e < Td; e += 2) rowp[e] = 0.f;
+            __syncwarp();
+            if (active) {
+                const float sp = pw[q];
+                const int lo = (int)ceilf(sp - k.radius);
+                const int n = min((int)floorf(sp + k.radius) - lo + 1, kWMax);
+                const int od = d == 0 ? org0 : (d == 1 ? org1 : org2);
+                const int a0 = wrapmod(lo - k.hw - od, k.mos[d]);   // tile-local footprint start
+                for (int t = sub; t < n; t += 2) {
+                    int e = a0 + t;
+                    if (e >= k.mos[d]) e -= k.mos[d];
+                    if (e < Td) {
+                        const int p = lo + t;
+                        float w = kb_weight_1d(fabsf(sp - (float)p), k.mos_f[d], k.one_over_W, k.beta[d], k.radius);
+                        if (a.sign_fold) w *= sign_of((p - k.hw) & 1);
+                        rowp[e] = w;
+                    }
+                }
+                if (sub == 0) {
+                    int rlo, rhi;
+                    if (k.ntiles[d] == 1) {   // the footprint may wrap inside the tile
+                        rlo = 0;
+                        rhi = Td - 1;
+                    } else {
+                        const int st = (a0 < Td) ? a0 : a0 - k.mos[d];
+                        rlo = max(st, 0);
+                        rhi = min(st + n - 1, Td - 1);
+                    }
+                    rng[i * 4 + d] = (unsigned)rlo | ((unsigned)rhi << 16);
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kVE; q++) {
+            const int e = threadIdx.x + q * kThreads;
+            if (e >= kChunk * CG) break;
+            float2 v = pv[q];
+            if (a.dcw) {
+                v.x = pd[q] * v.x;
+                v.y = pd[q] * v.y;
+            }
+            sv[e] = v;
+        }
+    };
+
+    int cur = 0;
+    if (it.begin < it.end) {
+        const int cnt0 = min(kChunk, it.end - it.begin);
+        prefetch(it.begin, cnt0);
+        stage_chunk(0, cnt0);
+    }
+    __syncthreads();
+    for (int base = it.begin; base < it.end; base += kChunk) {
+        const int cnt = min(kChunk, it.end - base);
+        const int nbase = base + kChunk;
+        const int ncnt = nbase < it.end ? min(kChunk, it.end - nbase) : 0;
+        if (ncnt > 0) prefetch(nbase, ncnt);
+        const float *wt = stage_wt(cur);
+        const float4 *sv4 = reinterpret_cast<const float4 *>(stage_v(cur));
+        const uint4 *rng = stage_rng(cur);
+#pragma unroll
+        for (int c = 0; c < RPW; c++) {
+            const int ry = qy0[c] + row;
+#pragma unroll
+            for (int half = 0; half < kChunk / 32; half++) {
+                const int il = half * 32 + lane;
+                bool hit = false;
+                if (il < cnt) {
+                    const uint4 r = rng[il];
+                    hit = (int)(r.x & 0xffffu) <= qx0[c] + RW - 1 && (int)(r.x >> 16) >= qx0[c] &&
+                          (int)(r.y & 0xffffu) <= qy0[c] + ROWS - 1 && (int)(r.y >> 16) >= qy0[c];
+                    if (D3) hit = hit && (int)(r.z & 0xffffu) <= qz[c] && (int)(r.z >> 16) >= qz[c];
+                }
+                uint32_t bits = __ballot_sync(0xffffffffu, hit);
+                while (bits) {
+                    const int i = half * 32 + __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    const float4 v = sv4[i * CP + cp];
+                    const float *wr = wt + i * tsp;
+                    float wyz = wr[T0 + ry];
+                    if (D3) wyz *= wr[T0 + T1 + qz[c]];
+#pragma unroll
+                    for (int jj = 0; jj < RW / 4; jj++) {
+                        const float4 w4 = *reinterpret_cast<const float4 *>(wr + qx0[c] + 4 * jj);
+                        const float wj[4] = {w4.x * wyz, w4.y * wyz, w4.z * wyz, w4.w * wyz};
+#pragma unroll
+                        for (int m = 0; m < 4; m++) {
+                            float *ac = acc[c][4 * jj + m];
+                            ac[0] = fmaf(wj[m], v.x, ac[0]);
+                            ac[1] = fmaf(wj[m], v.y, ac[1]);
+                            ac[2] = fmaf(wj[m], v.z, ac[2]);
+                            ac[3] = fmaf(wj[m], v.w, ac[3]);
+                        }
+                    }
+                }
+            }
+        }
+        if (ncnt > 0) stage_chunk(cur ^ 1, ncnt);
+        __syncthreads();
+        cur ^= 1;
+    }
+
+    const int64_t G = k.G;
+    auto store = [&](int c, int j, float4 v) {
+        const int gx = org0 + qx0[c] + j, gy = org1 + qy0[c] + row, gz = org2 + qz[c];
+        const int64_t g = ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + gx;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int q = 2 * cp + h;
+            if (b0 + q >= a.nb) break;
+            float2 *o = grid + ((int64_t)(b0 + q) * a.F + f) * G + g;
+            float2 w = h ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
+            if (a.accumulate) { const float2 old = *o; w.x += old.x; w.y += old.y; }
+            *o = w;
+        }
+    };
+    if (it.split < 0) {
+#pragma unroll
+        for (int c = 0; c < RPW; c++)
+#pragma unroll
+            for (int j = 0; j < RW; j++)
+                store(c, j, make_float4(acc[c][j][0], acc[c][j][1], acc[c][j][2], acc[c][j][3]));
+        return;
+    }
+    // Split tile: write this chunk's partial tile, the last CTA sums the
+    // partials in chunk order.
+    const SplitInfo si = a.splits[it.split];
+    auto part = [&](int slot) -> float4 * {
+        return reinterpret_cast<float4 *>(a.partials + ((int64_t)slot * a.ncg + grp) * a.part_elems);
+    };
+    {
+        float4 *pp = part(si.first_slot + it.chunk);
+#pragma unroll
+        for (int c = 0; c < RPW; c++)
+#pragma unroll
+            for (int j = 0; j < RW; j++)
+                pp[(c * RW + j) * kThreads + threadIdx.x] =
+                    make_float4(acc[c][j][0], acc[c][j][1], acc[c][j][2], acc[c][j][3]);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int *ctr = a.counters + (int64_t)it.split * a.ncg + grp;
+        const unsigned int old = atomicAdd(ctr, 1u);
+        s_last = (old == (unsigned int)(si.nchunks - 1));
+        if (s_last) *ctr = 0u;   // ready for the next launch
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+#pragma unroll
+    for (int c = 0; c < RPW; c++)
+#pragma unroll
+        for (int j = 0; j < RW; j++) {
+            float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int ch = 0; ch < si.nchunks; ch++) {
+                const float4 v = __ldcg(&part(si.first_slot + ch)[(c * RW + j) * kThreads + threadIdx.x]);
+                s.x += v.x;
+                s.y += v.y;
+                s.z += v.z;
+                s.w += v.w;
+            }
+            store(c, j, s);
+        }
+}
+
 // --------------------------------------------------------------- C2NC -----
 
 // Staged region of a home tile: tile + pad/2 cells on each side.
@@ -437,11 +727,18 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
                 const int rx = e / CG;
                 int gx = gx0 + rx;
                 gx = gx < 0 ? gx + k.mos[0] : (gx >= k.mos[0] ? gx - k.mos[0] : gx);
-                float2 v = make_float2(0.f, 0.f);
-                if (b0 + c < a.nb) v = __ldg(&grid[(int64_t)(b0 + c) * a.F * k.G + rowoff + gx]);
-                dst[e] = v;
+                // asynchronous 8-byte copy global -> shared (all of a thread's
+                // copies in flight at once); coils beyond nb are zero-filled
+                const bool in = b0 + c < a.nb;
+                const float2 *src = in ? &grid[(int64_t)(b0 + c) * a.F * k.G + rowoff + gx] : grid;
+                const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst + e);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(src),
+                             "r"(in ? 8 : 0)
+                             : "memory");
             }
         }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     }
     __syncthreads();
 
@@ -658,6 +955,50 @@ static int choose_cg(int requested, int nb) {
     return cg;
 }
 
+// Which gridding kernel runs for a plan and batch count, with its coil group
+// and the size of one CTA's partial tile (split tiles).
+struct GridCfg {
+    bool rows;        // k_grid_rows (else k_grid_nc2c)
+    int cg;
+    int rw, rpw;      // row variant: columns per lane, regions per warp
+    int cpt;          // cell variant: cells per thread
+    int ncg;
+    int64_t part_elems;
+    int smem;         // dynamic shared memory (row variant)
+};
+
+static GridCfg grid_config(const NufftPlan &p, int nb) {
+    const KParams &k = p.kp;
+    GridCfg c{};
+    const int cells = k.tile[0] * k.tile[1] * k.tile[2];
+    c.cpt = (cells + kThreads - 1) / kThreads;
+    const bool comp = (p.flags & GB_FLAG_COMPENSATED) != 0;
+    int cg = choose_cg(p.tiling.cg, nb);
+    if (!comp && k.D >= 2 && (cg == 8 || cg == 16)) {
+        const int rows = 64 / cg;
+        const int smem = 2 * row_stage_bytes(k, cg);
+        if (k.tile[1] % rows == 0 && smem <= 96 * 1024) {
+            for (int rw = 4; rw <= 8 && !c.rows; rw *= 2) {
+                if (k.tile[0] % rw) continue;
+                const int regions = cells / (rows * rw);
+                if (regions % 8) continue;
+                const int rpw = regions / 8;
+                if ((rpw == 1 || rpw == 2 || rpw == 4) && rpw * rw <= 16) {
+                    c.rows = true;
+                    c.rw = rw;
+                    c.rpw = rpw;
+                    c.smem = smem;
+                }
+            }
+        }
+    }
+    if (!c.rows && c.cpt * cg > (comp ? 16 : 32)) cg = std::max(1, (comp ? 16 : 32) / c.cpt);
+    c.cg = cg;
+    c.ncg = (nb + cg - 1) / cg;
+    c.part_elems = (int64_t)cg * (c.rows ? cells : kThreads * c.cpt);
+    return c;
+}
+
 template <int CG, int CPT, bool COMP>
 static void grid_dispatch(const ConvArgs &a, dim3 g, const float2 *s, float2 *o, cudaStream_t st) {
     k_grid_nc2c<CG, CPT, COMP><<<g, kThreads, 0, st>>>(a, s, o); ::gb::note_launch();
@@ -674,85 +1015,99 @@ static void grid_dispatch_cpt(int cpt, const ConvArgs &a, dim3 g, const float2 *
     }
 }
 
-static int grid_cg(NufftPlan &p, int nb, int cpt, bool comp) {
-    int cg = choose_cg(p.tiling.cg, nb);
-    if (cpt * cg > (comp ? 16 : 32)) cg = std::max(1, (comp ? 16 : 32) / cpt);
-    return cg;
+template <int CG, int RW, int RPW, bool D3>
+static void grid_rows_launch(const ConvArgs &a, dim3 g, int smem, const float2 *s, float2 *o, cudaStream_t st) {
+    auto kern = k_grid_rows<CG, RW, RPW, D3>;
+    if (smem > 48 * 1024)
+        GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    kern<<<g, kThreads, smem, st>>>(a, s, o); ::gb::note_launch();
+}
+
+template <int CG, bool D3>
+static void grid_rows_shape(const GridCfg &c, const ConvArgs &a, dim3 g, const float2 *s, float2 *o,
+                            cudaStream_t st) {
+    if (c.rw == 4 && c.rpw == 1) grid_rows_launch<CG, 4, 1, D3>(a, g, c.smem, s, o, st);
+    else if (c.rw == 4 && c.rpw == 2) grid_rows_launch<CG, 4, 2, D3>(a, g, c.smem, s, o, st);
+    else if (c.rw == 4 && c.rpw == 4) grid_rows_launch<CG, 4, 4, D3>(a, g, c.smem, s, o, st);
+    else if (c.rw == 8 && c.rpw == 1) grid_rows_launch<CG, 8, 1, D3>(a, g, c.smem, s, o, st);
+    else if (c.rw == 8 && c.rpw == 2) grid_rows_launch<CG, 8, 2, D3>(a, g, c.smem, s, o, st);
+    else fail(GB_ERR_INTERNAL, "unsupported gridding region shape");
+}
+
+// Launches the gridding kernel selected by `c` over all work items.
+static void grid_dispatch_cfg(const GridCfg &c, const NufftPlan &p, const ConvArgs &a, const float2 *samples,
+                              float2 *grid, cudaStream_t st) {
+    dim3 g(p.n_grd_items, c.ncg);
+    if (c.rows) {
+        const bool d3 = p.kp.D == 3;
+        if (c.cg == 16) {
+            if (d3) grid_rows_shape<16, true>(c, a, g, samples, grid, st);
+            else grid_rows_shape<16, false>(c, a, g, samples, grid, st);
+        } else {
+            if (d3) grid_rows_shape<8, true>(c, a, g, samples, grid, st);
+            else grid_rows_shape<8, false>(c, a, g, samples, grid, st);
+        }
+    } else if (p.flags & GB_FLAG_COMPENSATED) {
+        switch (c.cg) {
+            case 1: grid_dispatch_cpt<1, true>(c.cpt, a, g, samples, grid, st); break;
+            case 2: grid_dispatch_cpt<2, true>(c.cpt, a, g, samples, grid, st); break;
+            case 4: grid_dispatch_cpt<4, true>(c.cpt, a, g, samples, grid, st); break;
+            case 8: grid_dispatch_cpt<8, true>(c.cpt, a, g, samples, grid, st); break;
+            default: grid_dispatch_cpt<16, true>(c.cpt, a, g, samples, grid, st); break;
+        }
+    } else {
+        switch (c.cg) {
+            case 1: grid_dispatch_cpt<1, false>(c.cpt, a, g, samples, grid, st); break;
+            case 2: grid_dispatch_cpt<2, false>(c.cpt, a, g, samples, grid, st); break;
+            case 4: grid_dispatch_cpt<4, false>(c.cpt, a, g, samples, grid, st); break;
+            case 8: grid_dispatch_cpt<8, false>(c.cpt, a, g, samples, grid, st); break;
+            default: grid_dispatch_cpt<16, false>(c.cpt, a, g, samples, grid, st); break;
+        }
+    }
+    GB_CUDA(cudaGetLastError());
 }
 
 // Allocates the split-tile counters and partial buffers for `nb` batches
 // (must run outside stream capture).
 void launch_grid_prepare(NufftPlan &p, int nb, cudaStream_t st) {
-    const KParams &k = p.kp;
-    const int cpt = (k.tile[0] * k.tile[1] * k.tile[2] + kThreads - 1) / kThreads;
-    const int cells = kThreads * cpt;
-    const bool comp = (p.flags & GB_FLAG_COMPENSATED) != 0;
-    const int cg = grid_cg(p, nb, cpt, comp);
-    const int ncg = (nb + cg - 1) / cg;
+    const GridCfg c = grid_config(p, nb);
     if (p.n_splits > 0) {
-        const size_t need_ctr = (size_t)p.n_splits * ncg;
+        const size_t need_ctr = (size_t)p.n_splits * c.ncg;
         if (p.split_counters.n < need_ctr || p.split_counter_groups == 0) {
             p.split_counters.ensure(need_ctr);
             GB_CUDA(cudaMemsetAsync(p.split_counters.get(), 0, p.split_counters.n * sizeof(unsigned int), st));
-            p.split_counter_groups = ncg;
+            p.split_counter_groups = c.ncg;
         }
-        p.partials.ensure((size_t)p.n_slots * ncg * cg * cells);
+        p.partials.ensure((size_t)p.n_slots * c.ncg * c.part_elems);
     }
 }
 
 void launch_grid(NufftPlan &p, const float2 *samples, float2 *grid, int nb, SampleLayout layout,
                  const float *dcw, bool sign_fold, bool accumulate, cudaStream_t st) {
     if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
-    const KParams &k = p.kp;
-    const int cells = k.tile[0] * k.tile[1] * k.tile[2];
-    const int cpt = (cells + kThreads - 1) / kThreads;
-    const bool comp = (p.flags & GB_FLAG_COMPENSATED) != 0;
-    const int cg = grid_cg(p, nb, cpt, comp);
-    const int ncg = (nb + cg - 1) / cg;
+    const GridCfg c = grid_config(p, nb);
     ConvArgs a = make_args(p, nb, layout, dcw, 1, sign_fold, accumulate);
     a.list = p.grid_list.get();
     a.items = p.grd_items.get();
     a.n_items = p.n_grd_items;
     a.splits = p.splits.get();
-    a.ncg = ncg;
+    a.ncg = c.ncg;
+    a.part_elems = c.part_elems;
     if (p.n_splits > 0) {
         launch_grid_prepare(p, nb, st);
         a.partials = p.partials.get();
         a.counters = p.split_counters.get();
     }
     if (p.n_grd_items == 0) return;
-    dim3 g(p.n_grd_items, ncg);
-    if (comp) {
-        switch (cg) {
-            case 1: grid_dispatch_cpt<1, true>(cpt, a, g, samples, grid, st); break;
-            case 2: grid_dispatch_cpt<2, true>(cpt, a, g, samples, grid, st); break;
-            case 4: grid_dispatch_cpt<4, true>(cpt, a, g, samples, grid, st); break;
-            case 8: grid_dispatch_cpt<8, true>(cpt, a, g, samples, grid, st); break;
-            default: grid_dispatch_cpt<16, true>(cpt, a, g, samples, grid, st); break;
-        }
-    } else {
-        switch (cg) {
-            case 1: grid_dispatch_cpt<1, false>(cpt, a, g, samples, grid, st); break;
-            case 2: grid_dispatch_cpt<2, false>(cpt, a, g, samples, grid, st); break;
-            case 4: grid_dispatch_cpt<4, false>(cpt, a, g, samples, grid, st); break;
-            case 8: grid_dispatch_cpt<8, false>(cpt, a, g, samples, grid, st); break;
-            default: grid_dispatch_cpt<16, false>(cpt, a, g, samples, grid, st); break;
-        }
-    }
-    GB_CUDA(cudaGetLastError());
+    grid_dispatch_cfg(c, p, a, samples, grid, st);
 }
 
 // Scratch (split-tile partial tiles and their counters) that launch_grid
 // needs for `nb` batches, in elements.
 void grid_scratch_need(const NufftPlan &p, int nb, size_t *partial_elems, size_t *counter_elems) {
-    const KParams &k = p.kp;
-    const int cpt = (k.tile[0] * k.tile[1] * k.tile[2] + kThreads - 1) / kThreads;
-    const bool comp = (p.flags & GB_FLAG_COMPENSATED) != 0;
-    int cg = choose_cg(p.tiling.cg, nb);
-    if (cpt * cg > (comp ? 16 : 32)) cg = std::max(1, (comp ? 16 : 32) / cpt);
-    const int ncg = (nb + cg - 1) / cg;
-    *partial_elems = p.n_splits > 0 ? (size_t)p.n_slots * ncg * cg * kThreads * cpt : 0;
-    *counter_elems = p.n_splits > 0 ? (size_t)p.n_splits * ncg : 0;
+    const GridCfg c = grid_config(p, nb);
+    *partial_elems = p.n_splits > 0 ? (size_t)p.n_slots * c.ncg * c.part_elems : 0;
+    *counter_elems = p.n_splits > 0 ? (size_t)p.n_splits * c.ncg : 0;
 }
 
 // The gridding launch of launch_grid with caller-provided scratch: no device
@@ -761,39 +1116,18 @@ void grid_scratch_need(const NufftPlan &p, int nb, size_t *partial_elems, size_t
 void launch_grid_external_scratch(NufftPlan &p, const float2 *samples, float2 *grid, int nb, bool accumulate,
                                   float2 *partials, unsigned int *counters, cudaStream_t st) {
     if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
-    const KParams &k = p.kp;
-    const int cpt = (k.tile[0] * k.tile[1] * k.tile[2] + kThreads - 1) / kThreads;
-    const bool comp = (p.flags & GB_FLAG_COMPENSATED) != 0;
-    const int cg = grid_cg(p, nb, cpt, comp);
-    const int ncg = (nb + cg - 1) / cg;
+    const GridCfg c = grid_config(p, nb);
     ConvArgs a = make_args(p, nb, LAYOUT_ORIGINAL, nullptr, 1, false, accumulate);
     a.list = p.grid_list.get();
     a.items = p.grd_items.get();
     a.n_items = p.n_grd_items;
     a.splits = p.splits.get();
-    a.ncg = ncg;
+    a.ncg = c.ncg;
+    a.part_elems = c.part_elems;
     a.partials = partials;
     a.counters = counters;
     if (p.n_grd_items == 0) return;
-    dim3 g(p.n_grd_items, ncg);
-    if (comp) {
-        switch (cg) {
-            case 1: grid_dispatch_cpt<1, true>(cpt, a, g, samples, grid, st); break;
-            case 2: grid_dispatch_cpt<2, true>(cpt, a, g, samples, grid, st); break;
-            case 4: grid_dispatch_cpt<4, true>(cpt, a, g, samples, grid, st); break;
-            case 8: grid_dispatch_cpt<8, true>(cpt, a, g, samples, grid, st); break;
-            default: grid_dispatch_cpt<16, true>(cpt, a, g, samples, grid, st); break;
-        }
-    } else {
-        switch (cg) {
-            case 1: grid_dispatch_cpt<1, false>(cpt, a, g, samples, grid, st); break;
-            case 2: grid_dispatch_cpt<2, false>(cpt, a, g, samples, grid, st); break;
-            case 4: grid_dispatch_cpt<4, false>(cpt, a, g, samples, grid, st); break;
-            case 8: grid_dispatch_cpt<8, false>(cpt, a, g, samples, grid, st); break;
-            default: grid_dispatch_cpt<16, false>(cpt, a, g, samples, grid, st); break;
-        }
-    }
-    GB_CUDA(cudaGetLastError());
+    grid_dispatch_cfg(c, p, a, samples, grid, st);
 }
 
 template <int CG, bool GRAD>

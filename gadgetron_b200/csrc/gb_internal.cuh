@@ -29,7 +29,7 @@ namespace gb {
 constexpr int kMaxD = 3;
 constexpr int kWMax = 8;          // max taps per dimension (W <= 7)
 constexpr int kThreads = 256;     // threads per CTA for the tile kernels
-constexpr int kChunk = 32;        // samples staged per pass
+constexpr int kChunk = 64;        // samples staged per pass (gridding)
 
 // ------------------------------------------------------------ errors -----
 

@@ -322,7 +322,7 @@ __global__ void k_cg_update(int64_t seg_len, float2 *__restrict__ x, float2 *__r
             x[e] = xv;
             r[e] = rv;
             float w2 = 1.f;
-            if (P) { const float w = P[e % Pn]; w2 = w * w; }
+            if (P) { const float w = P[e]; w2 = w * w; }
             acc.x += (double)rv.x * (double)(rv.x * w2) + (double)rv.y * (double)(rv.y * w2);
         }
     }
@@ -367,7 +367,7 @@ __global__ void k_cg_pupdate(int64_t seg_len, float2 *__restrict__ p, const floa
          l += (int64_t)gridDim.x * blockDim.x) {
         const int64_t e = e0 + l;
         float2 rv = r[e];
-        if (P) { const float w = P[e % Pn]; const float w2 = w * w; rv.x *= w2; rv.y *= w2; }
+        if (P) { const float w = P[e]; const float w2 = w * w; rv.x *= w2; rv.y *= w2; }
         float2 pv = p[e];
         p[e] = make_float2(b * pv.x + rv.x, b * pv.y + rv.y);
     }
@@ -390,7 +390,7 @@ __global__ void k_cg_init(int64_t seg_len, const float2 *__restrict__ rhs, const
         if (q) { const float2 qv = q[e]; rv.x -= qv.x; rv.y -= qv.y; }
         r[e] = rv;
         float w2 = 1.f;
-        if (P) { const float w = P[e % Pn]; w2 = w * w; }
+        if (P) { const float w = P[e]; w2 = w * w; }
         const float2 pv = make_float2(rv.x * w2, rv.y * w2);
         p[e] = pv;
         if (set_rq0) x[e] = x0 ? x0[e] : make_float2(0.f, 0.f);
