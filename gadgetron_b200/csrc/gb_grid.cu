@@ -34,6 +34,7 @@
 //     (sign_fold), and the density weights are folded into the sample loads
 //     (gridding) or stores (degridding).
 #include <algorithm>
+#include <cmath>
 
 #include "gb_internal.cuh"
 #include "gb_ops.hpp"
@@ -43,6 +44,7 @@ namespace gb {
 struct ConvArgs {
     KParams k;
     const float *pos;         // [D][Mtot] sorted positions
+    const float *wtab;        // [Mtot][D][kWMax] tap weights of sorted samples
     const uint32_t *perm;     // sorted -> original
     const uint32_t *list;     // gridding list (sorted positions) or unused
     const WorkItem *items;
@@ -126,7 +128,7 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
     // registers one chunk ahead so their latency overlaps the accumulation.
     constexpr int kWE = (kChunk * 3 * kWMax + kThreads - 1) / kThreads;
     constexpr int kVE = (kChunk * CG + kThreads - 1) / kThreads;
-    float pw[kWE];
+    float pw[kWE], pt[kWE];
     float2 pv[kVE];
     float pd[kVE];
     float ps[3];
@@ -137,8 +139,12 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
             const int e = threadIdx.x + q * kThreads;
             const int i = e / (3 * kWMax), d = (e / kWMax) % 3;
             pw[q] = 0.f;
-            if (e < kChunk * 3 * kWMax && i < cnt && d < k.D)
-                pw[q] = a.pos[(int64_t)d * a.Mtot + a.list[base + i]];
+            pt[q] = 0.f;
+            if (e < kChunk * 3 * kWMax && i < cnt && d < k.D) {
+                const uint32_t si = a.list[base + i];
+                pw[q] = a.pos[(int64_t)d * a.Mtot + si];
+                pt[q] = a.wtab[((int64_t)si * k.D + d) * kWMax + (e % kWMax)];
+            }
         }
 #pragma unroll
         for (int q = 0; q < kVE; q++) {
@@ -170,17 +176,9 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
             float w = 0.f;
             if (i < cnt) {
                 if (d < k.D) {
-                    const float s = pw[q];
-                    const int lo = (int)ceilf(s - k.radius);
-                    const int n = (int)floorf(s + k.radius) - lo + 1;
-                    if (t < n) {
-                        const int p = lo + t;
-                        w = kb_weight_1d(fabsf(s - (float)p), k.mos_f[d], k.one_over_W, k.beta[d], k.radius);
-                        if (a.sign_fold) {
-                            int g = p - k.hw;   // parity of (p - hw) mod mos (mos is even)
-                            w *= sign_of(g & 1);
-                        }
-                    }
+                    const int lo = (int)ceilf(pw[q] - k.radius);
+                    w = pt[q];   // zero beyond the footprint
+                    if (a.sign_fold) w *= sign_of((lo + t - k.hw) & 1);   // parity of (p - hw) mod mos (mos even)
                 } else {
                     w = (t == 0) ? 1.f : 0.f;
                 }
@@ -381,10 +379,12 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
 // bit-reproducible.
 
 // Floats per staged sample weight row: tile x + tile y (+ tile z), padded to
-// a multiple of 4 so every row starts on a 16-byte boundary.
+// an odd multiple of 4 so every row starts on a 16-byte boundary and rows of
+// consecutive samples start in different banks.
 __host__ __device__ __forceinline__ int row_tsp(const KParams &k) {
     const int ts = k.tile[0] + k.tile[1] + (k.D == 3 ? k.tile[2] : 0);
-    return (ts + 3) & ~3;
+    const int t4 = (ts + 3) >> 2;
+    return 4 * (t4 | 1);
 }
 
 __host__ __device__ __forceinline__ int row_stage_bytes(const KParams &k, int cg) {
@@ -444,6 +444,7 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
         for (int j = 0; j < RW; j++) acc[c][j][0] = acc[c][j][1] = acc[c][j][2] = acc[c][j][3] = 0.f;
 
     float pw[kWP];
+    float4 pt[kWP];
     float2 pv[kVE];
     float pd[kVE];
 
@@ -453,7 +454,13 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
             const int u = threadIdx.x + q * kThreads;
             const int pr = u >> 1, i = pr / D, d = pr - i * D;
             pw[q] = 0.f;
-            if (u < kWU && i < cnt) pw[q] = a.pos[(int64_t)d * a.Mtot + a.list[base + i]];
+            pt[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (u < kWU && i < cnt) {
+                const uint32_t si = a.list[base + i];
+                pw[q] = a.pos[(int64_t)d * a.Mtot + si];
+                // taps 4*sub .. 4*sub+3 of (sample, dim)
+                pt[q] = *reinterpret_cast<const float4 *>(a.wtab + ((int64_t)si * D + d) * kWMax + 4 * (u & 1));
+            }
         }
 #pragma unroll
         for (int q = 0; q < kVE; q++) {
@@ -463,7 +470,8 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
             pd[q] = 1.f;
             if (e < kChunk * CG && i < cnt && b0 + c < a.nb) {
                 const uint32_t si = a.list[base + i];
-                const uint32_t j = a.perm[si];
+                const bool need_j = a.layout != LAYOUT_SORTED || a.dcw;
+                const uint32_t j = need_j ? a.perm[si] : si;
                 const int64_t idx = (a.layout == LAYOUT_SORTED) ? (int64_t)si : (int64_t)j;
                 pv[q] = samples[(int64_t)(b0 + c) * a.Mtot + idx];
                 if (a.dcw) pd[q] = a.dcw[j];
@@ -486,22 +494,30 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
             const bool active = u < kWU && i < cnt;
             const int Td = k.tile[d];
             float *rowp = wt + i * tsp + (d == 0 ? 0 : (d == 1 ? T0 : T0 + T1));
-            if (active)
-                for (int e = sub; e < Td; e += 2) rowp[e] = 0.f;
+            if (active) {
+                // row offsets are multiples of 4 floats; Td is for x and y
+                for (int e4 = sub; e4 < (Td >> 2); e4 += 2)
+                    *reinterpret_cast<float4 *>(rowp + 4 * e4) = make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int e = (Td & ~3) + sub; e < Td; e += 2) rowp[e] = 0.f;
+            }
             __syncwarp();
             if (active) {
                 const float sp = pw[q];
                 const int lo = (int)ceilf(sp - k.radius);
                 const int n = min((int)floorf(sp + k.radius) - lo + 1, kWMax);
                 const int od = d == 0 ? org0 : (d == 1 ? org1 : org2);
-                const int a0 = wrapmod(lo - k.hw - od, k.mos[d]);   // tile-local footprint start
-                for (int t = sub; t < n; t += 2) {
+                // tile-local footprint start (lo - hw - od) mod mos; |lo - hw - od| < 2 mos
+                int a0 = lo - k.hw - od;
+                a0 = a0 < 0 ? a0 + k.mos[d] : (a0 >= k.mos[d] ? a0 - k.mos[d] : a0);
+                const float tw[4] = {pt[q].x, pt[q].y, pt[q].z, pt[q].w};
+#pragma unroll
+                for (int m = 0; m < 4; m++) {
+                    const int t = 4 * sub + m;
                     int e = a0 + t;
                     if (e >= k.mos[d]) e -= k.mos[d];
-                    if (e < Td) {
-                        const int p = lo + t;
-                        float w = kb_weight_1d(fabsf(sp - (float)p), k.mos_f[d], k.one_over_W, k.beta[d], k.radius);
-                        if (a.sign_fold) w *= sign_of((p - k.hw) & 1);
+                    if (t < n && e >= 0 && e < Td) {
+                        float w = tw[m];
+                        if (a.sign_fold) w *= sign_of((lo + t - k.hw) & 1);
                         rowp[e] = w;
                     }
                 }
@@ -759,7 +775,10 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
                 if (t < n) {
                     const int g = lo + t;
                     const float diff = sp - (float)g;
-                    w = kb_weight_1d(fabsf(diff), k.mos_f[d], k.one_over_W, k.beta[d], k.radius);
+                    // tap t of the sample's table row is the weight of |diff|
+                    // (both differences are exact in float)
+                    w = GRAD ? kb_weight_1d(fabsf(diff), k.mos_f[d], k.one_over_W, k.beta[d], k.radius)
+                             : a.wtab[((int64_t)i * k.D + d) * kWMax + t];
                     if (GRAD) {
                         dw = kb_deriv_1d(fabsf(diff), k.mos_f[d], k.one_over_W, k.beta[d], k.radius);
                         dw = (diff < 0.f) ? -dw : dw;
@@ -771,7 +790,8 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
                     }
                 }
                 if (t == 0) {
-                    S.rs[s][d] = wrapmod(lo - org[d] + k.hw, k.mos[d]);
+                    const int od = d == 0 ? org[0] : (d == 1 ? org[1] : org[2]);
+                    S.rs[s][d] = wrapmod(lo - od + k.hw, k.mos[d]);
                     S.n[s][d] = n;
                 }
             } else if (i < it.end) {
@@ -920,6 +940,162 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
     }
 }
 
+// Degridding, table variant (plain accumulation, no gradient): the same
+// region staging and lane layout as k_degrid_c2nc, but each lane reads its
+// sample's tap weights straight from the per-trajectory weight table into
+// registers (no per-warp staging, no kernel evaluation) and runs a fully
+// unrolled NT x NT (x NT) tap nest predicated on the sample's tap counts, so
+// the inner loop is loads and FMAs only.  NT = the largest tap count a
+// footprint can have (2*ceil(W/2), plus one when W is an even integer).
+template <int CG, int NT, bool D3>
+__global__ void __launch_bounds__(kThreads)
+k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ out) {
+    using Sh = DegridShape<CG>;
+    constexpr int CPL = Sh::CPL, LPS = Sh::LPS, SPW = Sh::SPW;
+    constexpr int D = D3 ? 3 : 2;
+    extern __shared__ float4 smem_raw[];
+    const KParams &k = a.k;
+    const WorkItem it = a.items[blockIdx.x];
+    const int grp = blockIdx.y;
+    const int b0 = grp * CG;
+    const int f = it.ft / k.ntiles_total;
+    const int tile = it.ft - f * k.ntiles_total;
+    const int tx = tile % k.ntiles[0];
+    const int ty = (tile / k.ntiles[0]) % k.ntiles[1];
+    const int tz = tile / (k.ntiles[0] * k.ntiles[1]);
+    const int org0 = tx * k.tile[0], org1 = ty * k.tile[1], org2 = tz * k.tile[2];
+    const int R0 = region_dim(k, 0), R1 = region_dim(k, 1), R2 = region_dim(k, 2);
+    const int h2 = D3 ? k.hw : 0;
+    float2 *tile_s = reinterpret_cast<float2 *>(smem_raw);
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    {
+        // Region staging, coil fastest (as in k_degrid_c2nc).  A lane's coil
+        // is fixed (32 is a multiple of CG), so its plane offset is too.
+        const int rowElems = R0 * CG;
+        const int gx0 = org0 - k.hw;
+        const int c = lane % CG;
+        const bool cin = b0 + c < a.nb;
+        const float2 *plane = grid + (cin ? (int64_t)(b0 + c) * a.F * k.G : 0) + (int64_t)f * k.G;
+        for (int row = warp; row < R1 * R2; row += 8) {
+            const int ry = row % R1, rz = row / R1;
+            int gy = org1 - k.hw + ry;
+            gy = gy < 0 ? gy + k.mos[1] : (gy >= k.mos[1] ? gy - k.mos[1] : gy);
+            int gz = org2 - h2 + rz;
+            gz = gz < 0 ? gz + k.mos[2] : (gz >= k.mos[2] ? gz - k.mos[2] : gz);
+            const float2 *src_row = plane + ((int64_t)gz * k.mos[1] + gy) * k.mos[0];
+            const unsigned dst_row = (unsigned)__cvta_generic_to_shared(tile_s + (size_t)row * rowElems);
+            for (int e = lane; e < rowElems; e += 32) {
+                int gx = gx0 + e / CG;
+                gx = gx < 0 ? gx + k.mos[0] : (gx >= k.mos[0] ? gx - k.mos[0] : gx);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst_row + 8u * (unsigned)e),
+                             "l"(src_row + gx), "r"(cin ? 8 : 0)
+                             : "memory");
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncthreads();
+
+    const int sl = lane / LPS, ll = lane % LPS;
+    for (int base = it.begin + warp * SPW; base < it.end; base += 8 * SPW) {
+        const int i = base + sl;
+        const bool valid = i < it.end;
+        const int ic = valid ? i : it.begin;   // a valid row for the loads of idle lanes
+        int rs[3] = {0, 0, 0}, n[3] = {1, 1, 1};
+        float w[3][NT];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+#pragma unroll
+            for (int t = 0; t < NT; t++) w[d][t] = (t == 0) ? 1.f : 0.f;
+        }
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+            const float sp = a.pos[(int64_t)d * a.Mtot + ic] - (float)k.hw;
+            const int lo = (int)ceilf(sp - k.radius);
+            n[d] = valid ? min((int)floorf(sp + k.radius) - lo + 1, NT) : 0;
+            const int od = d == 0 ? org0 : (d == 1 ? org1 : org2);
+            int x = lo - od + k.hw;   // region-local start, |x| < 2 mos
+            x = x < 0 ? x + k.mos[d] : (x >= k.mos[d] ? x - k.mos[d] : x);
+            rs[d] = x;
+            const int Rd = d == 0 ? R0 : (d == 1 ? R1 : R2);
+            n[d] = min(n[d], Rd - x);   // the footprint lies inside the region; keep reads there
+            const float4 *trow = reinterpret_cast<const float4 *>(a.wtab + ((int64_t)ic * D + d) * kWMax);
+            const float4 q0 = __ldg(trow);
+            const float tw[8] = {q0.x, q0.y, q0.z, q0.w, 0.f, 0.f, 0.f, 0.f};
+            float tv[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) tv[t] = tw[t];
+            if (NT > 4) {
+                const float4 q1 = __ldg(trow + 1);
+                tv[4] = q1.x; tv[5] = q1.y; tv[6] = q1.z; tv[7] = q1.w;
+            }
+            // centring checkerboard: (-1)^(cell) with cell = lo + t (mos even)
+            const float s0 = (a.sign_fold && (lo & 1)) ? -1.f : 1.f;
+#pragma unroll
+            for (int t = 0; t < NT; t++) w[d][t] = (a.sign_fold && (t & 1)) ? -s0 * tv[t] : s0 * tv[t];
+        }
+        float acc[CPL][2];
+#pragma unroll
+        for (int c = 0; c < CPL; c++) acc[c][0] = acc[c][1] = 0.f;
+        const float2 *base_s = tile_s + (((size_t)rs[2] * R1 + rs[1]) * R0 + rs[0]) * CG + ll * CPL;
+#pragma unroll
+        for (int tzi = 0; tzi < (D3 ? NT : 1); tzi++) {
+            if (tzi < n[2]) {
+#pragma unroll
+                for (int tyi = 0; tyi < NT; tyi++) {
+                    if (tyi < n[1]) {
+                        const float wyz = D3 ? w[1][tyi] * w[2][tzi] : w[1][tyi];
+                        const float2 *row = base_s + ((size_t)tzi * R1 + tyi) * R0 * CG;
+#pragma unroll
+                        for (int t = 0; t < NT; t++) {
+                            if (t < n[0]) {
+                                const float wv = w[0][t] * wyz;
+                                if (CPL == 2) {
+                                    const float4 q = *reinterpret_cast<const float4 *>(row + t * CG);
+                                    acc[0][0] = fmaf(wv, q.x, acc[0][0]);
+                                    acc[0][1] = fmaf(wv, q.y, acc[0][1]);
+                                    acc[CPL - 1][0] = fmaf(wv, q.z, acc[CPL - 1][0]);
+                                    acc[CPL - 1][1] = fmaf(wv, q.w, acc[CPL - 1][1]);
+                                } else {
+                                    const float2 q = row[t * CG];
+                                    acc[0][0] = fmaf(wv, q.x, acc[0][0]);
+                                    acc[0][1] = fmaf(wv, q.y, acc[0][1]);
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (valid) {
+            const uint32_t j = a.perm[i];
+            const int64_t idx = (a.layout == LAYOUT_SORTED) ? (int64_t)i : (int64_t)j;
+            float dw = 1.f;
+            if (a.dcw) dw = a.dcw[j];
+#pragma unroll
+            for (int c = 0; c < CPL; c++) {
+                const int coil = b0 + ll * CPL + c;
+                if (coil >= a.nb) break;
+                float2 val = make_float2(acc[c][0], acc[c][1]);
+                if (a.dcw) {
+                    if (a.dcw_pow == 2) {
+                        val.x = (val.x * dw) * dw;
+                        val.y = (val.y * dw) * dw;
+                    } else {
+                        val.x *= dw;
+                        val.y *= dw;
+                    }
+                }
+                float2 *o = out + (int64_t)coil * a.Mtot + idx;
+                if (a.accumulate) { const float2 ov = *o; val.x += ov.x; val.y += ov.y; }
+                *o = val;
+            }
+        }
+    }
+}
+
 __global__ void k_sum_groups(const float *__restrict__ part, int ngroups, int64_t n,
                              float *__restrict__ out) {
     int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -936,6 +1112,7 @@ static ConvArgs make_args(NufftPlan &p, int nb, SampleLayout layout, const float
     ConvArgs a{};
     a.k = p.kp;
     a.pos = p.pos_sorted.get();
+    a.wtab = p.wtab.get();
     a.perm = p.perm.get();
     a.Mtot = p.Mtot;
     a.F = (int)p.F;
@@ -1168,6 +1345,49 @@ static void degrid_dispatch(int cg, const ConvArgs &a, dim3 g, size_t smem, cons
     }
 }
 
+static size_t degrid_table_smem(const KParams &k, int cg) {
+    return (((size_t)region_dim(k, 0) * region_dim(k, 1) * region_dim(k, 2) * cg + 1) & ~(size_t)1) *
+           sizeof(float2);
+}
+
+template <int CG, int NT, bool D3>
+static void degrid_table_launch(const ConvArgs &a, dim3 g, size_t smem, const float2 *grid, float2 *out,
+                                cudaStream_t st) {
+    auto kern = k_degrid_table<CG, NT, D3>;
+    if (smem > 48 * 1024)
+        GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<g, kThreads, smem, st>>>(a, grid, out); ::gb::note_launch();
+}
+
+template <int CG, bool D3>
+static void degrid_table_nt(int nt, const ConvArgs &a, dim3 g, size_t smem, const float2 *grid, float2 *out,
+                            cudaStream_t st) {
+    switch (nt) {
+        case 4: degrid_table_launch<CG, 4, D3>(a, g, smem, grid, out, st); break;
+        case 5: degrid_table_launch<CG, 5, D3>(a, g, smem, grid, out, st); break;
+        case 6: degrid_table_launch<CG, 6, D3>(a, g, smem, grid, out, st); break;
+        case 7: degrid_table_launch<CG, 7, D3>(a, g, smem, grid, out, st); break;
+        default: degrid_table_launch<CG, 8, D3>(a, g, smem, grid, out, st); break;
+    }
+}
+
+static void degrid_table_dispatch(int cg, int nt, bool d3, const ConvArgs &a, dim3 g, size_t smem,
+                                  const float2 *grid, float2 *out, cudaStream_t st) {
+    if (d3) {
+        switch (cg) {
+            case 4: degrid_table_nt<4, true>(nt, a, g, smem, grid, out, st); break;
+            case 8: degrid_table_nt<8, true>(nt, a, g, smem, grid, out, st); break;
+            default: degrid_table_nt<16, true>(nt, a, g, smem, grid, out, st); break;
+        }
+    } else {
+        switch (cg) {
+            case 4: degrid_table_nt<4, false>(nt, a, g, smem, grid, out, st); break;
+            case 8: degrid_table_nt<8, false>(nt, a, g, smem, grid, out, st); break;
+            default: degrid_table_nt<16, false>(nt, a, g, smem, grid, out, st); break;
+        }
+    }
+}
+
 static int degrid_cg(NufftPlan &p, int nb, bool grad = false) {
     int cg = choose_cg(p.tiling.cg, nb);
     while (cg > 1 && degrid_smem(p.kp, cg, grad) > 200 * 1024) cg /= 2;
@@ -1185,11 +1405,16 @@ void launch_degrid(NufftPlan &p, const float2 *grid, float2 *samples, int nb, Sa
     a.n_items = p.n_deg_items;
     if (p.n_deg_items == 0) return;
     dim3 g(p.n_deg_items, ncg);
-    const size_t smem = degrid_smem(p.kp, cg);
-    if (p.flags & GB_FLAG_COMPENSATED)
-        degrid_dispatch<true, false>(cg, a, g, smem, grid, samples, nullptr, nullptr, st);
-    else
-        degrid_dispatch<false, false>(cg, a, g, smem, grid, samples, nullptr, nullptr, st);
+    const int nt = (int)std::floor(p.W) + 1;   // most taps a footprint can have per dimension
+    if (!(p.flags & GB_FLAG_COMPENSATED) && p.D >= 2 && cg >= 4 && nt >= 4 && nt <= kWMax) {
+        degrid_table_dispatch(cg, nt, p.D == 3, a, g, degrid_table_smem(p.kp, cg), grid, samples, st);
+    } else {
+        const size_t smem = degrid_smem(p.kp, cg);
+        if (p.flags & GB_FLAG_COMPENSATED)
+            degrid_dispatch<true, false>(cg, a, g, smem, grid, samples, nullptr, nullptr, st);
+        else
+            degrid_dispatch<false, false>(cg, a, g, smem, grid, samples, nullptr, nullptr, st);
+    }
     GB_CUDA(cudaGetLastError());
 }
 

@@ -151,6 +151,7 @@ struct NufftPlan {
     int64_t Mtot = 0;
     std::vector<int64_t> frame_off;
     DevBuf<float> pos_sorted;      // [D][Mtot]
+    DevBuf<float> wtab;            // [Mtot][D][kWMax] 1D kernel weights of the taps of sorted samples
     DevBuf<uint32_t> perm;         // sorted pos -> original sample index
     DevBuf<uint32_t> home_off;     // [F*ntiles + 1]
     DevBuf<uint32_t> grid_list;    // gridding pair list (sorted positions)

@@ -196,10 +196,16 @@ __global__ void k_gather_pos(int D, int64_t M, const float *__restrict__ pos,
     for (int d = 0; d < D; d++) pos_sorted[(int64_t)d * M + i] = pos[(int64_t)d * M + j];
 }
 
-__global__ void k_histogram(const uint32_t *__restrict__ keys, int64_t n, uint32_t *__restrict__ counts) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    atomicAdd(&counts[keys[i]], 1u);
+// Run offsets of a sorted key array: off[k] = first index whose key is >= k,
+// off[nkeys] = n (no atomics: every thread fills the offsets between the key
+// before it and its own).
+__global__ void k_sorted_offsets(const uint32_t *__restrict__ keys, int64_t n, uint32_t nkeys,
+                                 uint32_t *__restrict__ off) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    const int64_t prev = (i == 0) ? -1 : (int64_t)keys[i - 1];
+    const int64_t cur = (i == n) ? (int64_t)nkeys : (int64_t)keys[i];
+    for (int64_t k = prev + 1; k <= cur; k++) off[k] = (uint32_t)i;
 }
 
 // Tiles touched by the gridding footprint of sorted sample i (NC2C taps
@@ -225,6 +231,27 @@ __device__ __forceinline__ int touched_tiles(const KParams &k, const float *s, i
         total *= n;
     }
     return total;
+}
+
+// Per sorted sample and dimension, the 1D kernel weights of its taps
+// t = 0..kWMax-1 at padded-grid cells ceil(s - W/2) + t (zero beyond the
+// footprint): the values the convolution kernels would compute from the
+// position, evaluated once per trajectory.
+__global__ void k_weight_table(KParams k, int64_t M, const float *__restrict__ pos_sorted,
+                               float4 *__restrict__ wtab) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M * k.D) return;
+    const int64_t j = e / k.D;
+    const int d = (int)(e - j * k.D);
+    const float s = pos_sorted[(int64_t)d * M + j];
+    const int lo = (int)ceilf(s - k.radius);
+    const int n = (int)floorf(s + k.radius) - lo + 1;
+    float w[kWMax];
+#pragma unroll
+    for (int t = 0; t < kWMax; t++)
+        w[t] = t < n ? kb_weight_1d(fabsf(s - (float)(lo + t)), k.mos_f[d], k.one_over_W, k.beta[d], k.radius) : 0.f;
+    wtab[2 * e] = make_float4(w[0], w[1], w[2], w[3]);
+    wtab[2 * e + 1] = make_float4(w[4], w[5], w[6], w[7]);
 }
 
 __global__ void k_count_pairs(KParams k, int64_t M, const float *__restrict__ pos_sorted,
@@ -341,15 +368,16 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     k_gather_pos<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(D, M, pos.get(), p.perm.get(),
                                                                 p.pos_sorted.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
+    p.wtab.ensure((size_t)M * D * kWMax);
+    k_weight_table<<<(unsigned)((M * D + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(),
+                                                                     reinterpret_cast<float4 *>(p.wtab.get())); ::gb::note_launch();
+    GB_CUDA(cudaGetLastError());
 
     // Home ranges.
-    DevBuf<uint32_t> &counts = p.pp_counts;
-    counts.ensure(nkeys + 1);
-    GB_CUDA(cudaMemsetAsync(counts.get(), 0, (nkeys + 1) * sizeof(uint32_t), st));
-    k_histogram<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(key_sorted.get(), M, counts.get()); ::gb::note_launch();
-    GB_CUDA(cudaGetLastError());
     p.home_off.ensure(nkeys + 1);
-    exclusive_scan(counts.get(), p.home_off.get(), (int64_t)nkeys + 1, p.pp_cub, st);
+    k_sorted_offsets<<<(unsigned)((M + TB) / TB), TB, 0, st>>>(key_sorted.get(), M, (uint32_t)nkeys,
+                                                              p.home_off.get()); ::gb::note_launch();
+    GB_CUDA(cudaGetLastError());
 
     // Gridding pair lists.
     DevBuf<uint32_t> &pcnt = p.pp_pcnt, &poff = p.pp_poff;
@@ -372,11 +400,10 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
                                                                  poff.get(), pkey.get(), pval.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
     sort_pairs(pkey.get(), pkey_sorted.get(), pval.get(), p.grid_list.get(), npairs, bits_for(nkeys), p.pp_cub, st);
-    GB_CUDA(cudaMemsetAsync(counts.get(), 0, (nkeys + 1) * sizeof(uint32_t), st));
-    k_histogram<<<(unsigned)((npairs + TB - 1) / TB), TB, 0, st>>>(pkey_sorted.get(), npairs, counts.get()); ::gb::note_launch();
-    GB_CUDA(cudaGetLastError());
     p.grid_off.ensure(nkeys + 1);
-    exclusive_scan(counts.get(), p.grid_off.get(), (int64_t)nkeys + 1, p.pp_cub, st);
+    k_sorted_offsets<<<(unsigned)(((int64_t)npairs + TB) / TB), TB, 0, st>>>(pkey_sorted.get(), npairs,
+                                                                            (uint32_t)nkeys, p.grid_off.get()); ::gb::note_launch();
+    GB_CUDA(cudaGetLastError());
 
     p.F = F;
     p.Mtot = M;
@@ -490,7 +517,7 @@ uint64_t plan_layout_signature(const NufftPlan &p, int nbf) {
             h *= 1099511628211ull;
         }
     };
-    const void *ptrs[] = {p.pos_sorted.get(), p.perm.get(), p.grid_list.get(), p.grd_items.get(),
+    const void *ptrs[] = {p.pos_sorted.get(), p.wtab.get(), p.perm.get(), p.grid_list.get(), p.grd_items.get(),
                           p.deg_items.get(), p.splits.get(), p.partials.get(), p.split_counters.get(),
                           p.img_os.get(), p.kgrid.get(), p.samp_ws.get(), p.deap_img.get(), p.deap_os.get()};
     for (const void *q : ptrs) mix((uint64_t)(uintptr_t)q);
