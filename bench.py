@@ -434,7 +434,9 @@ def run_nufft(args, dims):
     """NUFFT forward (C2NC) + adjoint (NC2C, ramp dcw) throughput.
     2D: 128^2, 1 coil, 128 golden-angle spokes x 256 (32768 samples), alpha 2, W 5.5.
     3D: 128^3, 32 coils (Gaussian-bump coil images), 20000 golden-means
-    spokes x 256 (5.12M samples), alpha 1.5 (192^3), W 4."""
+    spokes x 256 (5.12M samples), alpha 1.5 (192^3), W 4.
+    --size small (profiling case, 3D only): 64^3, 16 coils, 2500 spokes x 128,
+    alpha 1.5 (96^3), W 4."""
     import torch
     import gadgetron_b200 as gb
     from gadgetron_b200 import synthetic as S
@@ -445,6 +447,11 @@ def run_nufft(args, dims):
         N, mos, W, C = (128, 128), (256, 256), 5.5, 1
         traj = S.radial_golden_angle_2d(128, 256)
         img = S.gaussian_image((C, 1, 128, 128), 11)
+    elif getattr(args, "size", "full") == "small":
+        N, mos, W, C = (64, 64, 64), (96, 96, 96), 4.0, 16
+        traj = S.kooshball_golden_means_3d(2500, 128)
+        x = S.gaussian_image((64, 64, 64), 6)
+        img = (S.gaussian_bump_csm((64, 64, 64), C) * x[None])[:, None].astype(np.complex64)
     else:
         N, mos, W, C = (128, 128, 128), (192, 192, 192), 4.0, 32
         traj = S.kooshball_golden_means_3d(20000, 256)
@@ -485,7 +492,7 @@ def run_nufft(args, dims):
         "unit": "Msample-coils/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "c64 (fp32)", "data": "synthetic",
-        "config": {"workload": "nufft-%dd" % dims, "matrix": N[0], "matrix_os": mos[0], "W": W, "coils": C,
+        "config": {"workload": "nufft-%dd" % dims + ("-small" if N[0] == 64 and dims == 3 else ""), "matrix": N[0], "matrix_os": mos[0], "W": W, "coils": C,
                    "samples": M, "l2": "flushed before every timed step"},
         "ms_forward": round(t_fwd, 4), "ms_adjoint": round(t_adj, 4), "ms_preprocess_wall": round(t_prep, 2),
         "forward_rel_l2_vs_fp64_ndft": err_ndft, "gpu_launches": int(launches),
@@ -711,6 +718,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="cg-sense-2d",
                     choices=["cg-sense-2d", "nufft-2d", "nufft-3d", "batched", "precision"])
+    ap.add_argument("--size", default="full", choices=["full", "small"],
+                    help="nufft-3d only: small = the 64^3 profiling case")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

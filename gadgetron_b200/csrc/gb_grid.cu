@@ -35,6 +35,7 @@
 //     (gridding) or stores (degridding).
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "gb_internal.cuh"
 #include "gb_ops.hpp"
@@ -948,11 +949,17 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
 // the inner loop is loads and FMAs only.  NT = the largest tap count a
 // footprint can have (2*ceil(W/2), plus one when W is an even integer).
 template <int CG, int NT, bool D3>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, D3 ? 2 : 3)
 k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ out) {
     using Sh = DegridShape<CG>;
     constexpr int CPL = Sh::CPL, LPS = Sh::LPS, SPW = Sh::SPW;
     constexpr int D = D3 ? 3 : 2;
+    // Staged cell stride in float2.  2D: padded to an odd number of 16-byte
+    // chunks (conflict-free staging stores; the region copy is a large share
+    // of a 2D item's work).  3D: unpadded (the copy is a few percent of an
+    // item's work there and the region is large).
+    constexpr int CS = D3 ? CG : CG + 2;
+    static_assert(CG >= 4, "table degridding stages coil pairs");
     extern __shared__ float4 smem_raw[];
     const KParams &k = a.k;
     const WorkItem it = a.items[blockIdx.x];
@@ -969,40 +976,82 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
     float2 *tile_s = reinterpret_cast<float2 *>(smem_raw);
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int sl = lane / LPS, ll = lane % LPS;
+
+    // Per-sample inputs of one pass, loaded a pass ahead (the first pass's
+    // loads overlap the region copy).
+    struct Raw {
+        float sp[3];
+        float4 t0[3], t1[3];
+        uint32_t j;
+        float dw;
+    };
+    auto load_raw = [&](int bs, Raw &r) {
+        const int i = bs + sl;
+        const bool valid = i < it.end;
+        const int ic = valid ? i : it.begin;   // a valid row for the loads of idle lanes
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+            r.sp[d] = a.pos[(int64_t)d * a.Mtot + ic];
+            const float4 *trow = reinterpret_cast<const float4 *>(a.wtab + ((int64_t)ic * D + d) * kWMax);
+            r.t0[d] = __ldg(trow);
+            r.t1[d] = NT > 4 ? __ldg(trow + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        const bool need_j = a.layout != LAYOUT_SORTED || a.dcw;
+        r.j = need_j ? a.perm[ic] : (uint32_t)ic;
+        r.dw = a.dcw ? a.dcw[r.j] : 1.f;
+    };
+    Raw cur, nxt;
+    int base = it.begin + warp * SPW;
+    if (base < it.end) load_raw(base, cur);
     {
-        // Region staging, coil fastest (as in k_degrid_c2nc).  A lane's coil
-        // is fixed (32 is a multiple of CG), so its plane offset is too.
-        const int rowElems = R0 * CG;
+        // Region staging through registers: lanes run along x (each load is
+        // a coalesced run of one coil plane), then every lane stores its
+        // cell's CG coils as 16-byte chunks (with padded cells, the chunks
+        // that a warp stores at once fall into different banks).
+        const int XW = R0 > 16 ? 32 : (R0 > 8 ? 16 : 8);   // lanes per row
+        const int RPS = 32 / XW;                          // rows per warp step
+        const int rsub = lane / XW, xl = lane - rsub * XW;
+        const int nrows = R1 * R2;
         const int gx0 = org0 - k.hw;
-        const int c = lane % CG;
-        const bool cin = b0 + c < a.nb;
-        const float2 *plane = grid + (cin ? (int64_t)(b0 + c) * a.F * k.G : 0) + (int64_t)f * k.G;
-        for (int row = warp; row < R1 * R2; row += 8) {
-            const int ry = row % R1, rz = row / R1;
-            int gy = org1 - k.hw + ry;
-            gy = gy < 0 ? gy + k.mos[1] : (gy >= k.mos[1] ? gy - k.mos[1] : gy);
-            int gz = org2 - h2 + rz;
-            gz = gz < 0 ? gz + k.mos[2] : (gz >= k.mos[2] ? gz - k.mos[2] : gz);
-            const float2 *src_row = plane + ((int64_t)gz * k.mos[1] + gy) * k.mos[0];
-            const unsigned dst_row = (unsigned)__cvta_generic_to_shared(tile_s + (size_t)row * rowElems);
-            for (int e = lane; e < rowElems; e += 32) {
-                int gx = gx0 + e / CG;
-                gx = gx < 0 ? gx + k.mos[0] : (gx >= k.mos[0] ? gx - k.mos[0] : gx);
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst_row + 8u * (unsigned)e),
-                             "l"(src_row + gx), "r"(cin ? 8 : 0)
-                             : "memory");
+        const int64_t pstride = (int64_t)a.F * k.G;
+        const float2 *fbase = grid + (int64_t)b0 * pstride + (int64_t)f * k.G;
+        for (int row0 = warp * RPS; row0 < nrows; row0 += 8 * RPS) {
+            const int row = row0 + rsub;
+            if (row < nrows) {
+                const int rz = row / R1, ry = row - rz * R1;
+                int gy = org1 - k.hw + ry;
+                gy = gy < 0 ? gy + k.mos[1] : (gy >= k.mos[1] ? gy - k.mos[1] : gy);
+                int gz = org2 - h2 + rz;
+                gz = gz < 0 ? gz + k.mos[2] : (gz >= k.mos[2] ? gz - k.mos[2] : gz);
+                const float2 *src_row = fbase + ((int64_t)gz * k.mos[1] + gy) * k.mos[0];
+                for (int xo = xl; xo < R0; xo += XW) {
+                    int gx = gx0 + xo;
+                    gx = gx < 0 ? gx + k.mos[0] : (gx >= k.mos[0] ? gx - k.mos[0] : gx);
+                    float4 *cell = reinterpret_cast<float4 *>(tile_s + ((size_t)row * R0 + xo) * CS);
+                    constexpr int CH = CG < 8 ? CG : 8;   // coils in flight per lane
+#pragma unroll
+                    for (int h = 0; h < CG / CH; h++) {
+                        float2 v[CH];
+#pragma unroll
+                        for (int c = 0; c < CH; c++) {
+                            const int cc = h * CH + c;
+                            v[c] = (b0 + cc < a.nb) ? __ldg(src_row + cc * pstride + gx) : make_float2(0.f, 0.f);
+                        }
+#pragma unroll
+                        for (int q = 0; q < CH / 2; q++)
+                            cell[h * CH / 2 + q] = make_float4(v[2 * q].x, v[2 * q].y, v[2 * q + 1].x, v[2 * q + 1].y);
+                    }
+                }
             }
         }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     }
     __syncthreads();
 
-    const int sl = lane / LPS, ll = lane % LPS;
-    for (int base = it.begin + warp * SPW; base < it.end; base += 8 * SPW) {
+    for (; base < it.end; base += 8 * SPW) {
         const int i = base + sl;
         const bool valid = i < it.end;
-        const int ic = valid ? i : it.begin;   // a valid row for the loads of idle lanes
+        if (base + 8 * SPW < it.end) load_raw(base + 8 * SPW, nxt);
         int rs[3] = {0, 0, 0}, n[3] = {1, 1, 1};
         float w[3][NT];
 #pragma unroll
@@ -1012,7 +1061,7 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
         }
 #pragma unroll
         for (int d = 0; d < D; d++) {
-            const float sp = a.pos[(int64_t)d * a.Mtot + ic] - (float)k.hw;
+            const float sp = cur.sp[d] - (float)k.hw;
             const int lo = (int)ceilf(sp - k.radius);
             n[d] = valid ? min((int)floorf(sp + k.radius) - lo + 1, NT) : 0;
             const int od = d == 0 ? org0 : (d == 1 ? org1 : org2);
@@ -1021,16 +1070,8 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
             rs[d] = x;
             const int Rd = d == 0 ? R0 : (d == 1 ? R1 : R2);
             n[d] = min(n[d], Rd - x);   // the footprint lies inside the region; keep reads there
-            const float4 *trow = reinterpret_cast<const float4 *>(a.wtab + ((int64_t)ic * D + d) * kWMax);
-            const float4 q0 = __ldg(trow);
-            const float tw[8] = {q0.x, q0.y, q0.z, q0.w, 0.f, 0.f, 0.f, 0.f};
-            float tv[8];
-#pragma unroll
-            for (int t = 0; t < 8; t++) tv[t] = tw[t];
-            if (NT > 4) {
-                const float4 q1 = __ldg(trow + 1);
-                tv[4] = q1.x; tv[5] = q1.y; tv[6] = q1.z; tv[7] = q1.w;
-            }
+            const float tv[8] = {cur.t0[d].x, cur.t0[d].y, cur.t0[d].z, cur.t0[d].w,
+                                 cur.t1[d].x, cur.t1[d].y, cur.t1[d].z, cur.t1[d].w};
             // centring checkerboard: (-1)^(cell) with cell = lo + t (mos even)
             const float s0 = (a.sign_fold && (lo & 1)) ? -1.f : 1.f;
 #pragma unroll
@@ -1039,41 +1080,52 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
         float acc[CPL][2];
 #pragma unroll
         for (int c = 0; c < CPL; c++) acc[c][0] = acc[c][1] = 0.f;
-        const float2 *base_s = tile_s + (((size_t)rs[2] * R1 + rs[1]) * R0 + rs[0]) * CG + ll * CPL;
+        const float2 *base_s = tile_s + (((size_t)rs[2] * R1 + rs[1]) * R0 + rs[0]) * CS + ll * CPL;
+        // Tap nest, unrolled to NTT taps per dimension and predicated on the
+        // sample's counts.  When every sample of the warp has fewer than NT
+        // taps in every dimension (the common case when W is an even integer)
+        // the NT-1 nest runs.
+        auto nest = [&](auto ntc) {
+            constexpr int NTT = decltype(ntc)::value;
 #pragma unroll
-        for (int tzi = 0; tzi < (D3 ? NT : 1); tzi++) {
-            if (tzi < n[2]) {
+            for (int tzi = 0; tzi < (D3 ? NTT : 1); tzi++) {
+                if (tzi < n[2]) {
 #pragma unroll
-                for (int tyi = 0; tyi < NT; tyi++) {
-                    if (tyi < n[1]) {
-                        const float wyz = D3 ? w[1][tyi] * w[2][tzi] : w[1][tyi];
-                        const float2 *row = base_s + ((size_t)tzi * R1 + tyi) * R0 * CG;
+                    for (int tyi = 0; tyi < NTT; tyi++) {
+                        if (tyi < n[1]) {
+                            const float wyz = D3 ? w[1][tyi] * w[2][tzi] : w[1][tyi];
+                            const float2 *row = base_s + ((size_t)tzi * R1 + tyi) * R0 * CS;
 #pragma unroll
-                        for (int t = 0; t < NT; t++) {
-                            if (t < n[0]) {
-                                const float wv = w[0][t] * wyz;
-                                if (CPL == 2) {
-                                    const float4 q = *reinterpret_cast<const float4 *>(row + t * CG);
-                                    acc[0][0] = fmaf(wv, q.x, acc[0][0]);
-                                    acc[0][1] = fmaf(wv, q.y, acc[0][1]);
-                                    acc[CPL - 1][0] = fmaf(wv, q.z, acc[CPL - 1][0]);
-                                    acc[CPL - 1][1] = fmaf(wv, q.w, acc[CPL - 1][1]);
-                                } else {
-                                    const float2 q = row[t * CG];
-                                    acc[0][0] = fmaf(wv, q.x, acc[0][0]);
-                                    acc[0][1] = fmaf(wv, q.y, acc[0][1]);
+                            for (int t = 0; t < NTT; t++) {
+                                if (t < n[0]) {
+                                    const float wv = w[0][t] * wyz;
+                                    if (CPL == 2) {
+                                        const float4 q = *reinterpret_cast<const float4 *>(row + t * CS);
+                                        acc[0][0] = fmaf(wv, q.x, acc[0][0]);
+                                        acc[0][1] = fmaf(wv, q.y, acc[0][1]);
+                                        acc[CPL - 1][0] = fmaf(wv, q.z, acc[CPL - 1][0]);
+                                        acc[CPL - 1][1] = fmaf(wv, q.w, acc[CPL - 1][1]);
+                                    } else {
+                                        const float2 q = row[t * CS];
+                                        acc[0][0] = fmaf(wv, q.x, acc[0][0]);
+                                        acc[0][1] = fmaf(wv, q.y, acc[0][1]);
+                                    }
                                 }
                             }
                         }
                     }
                 }
             }
-        }
+        };
+        const bool shorter = __all_sync(0xffffffffu, n[0] < NT && n[1] < NT && n[2] < NT);
+        if (NT > 4 && shorter)
+            nest(std::integral_constant<int, (NT > 4 ? NT - 1 : NT)>{});
+        else
+            nest(std::integral_constant<int, NT>{});
         if (valid) {
-            const uint32_t j = a.perm[i];
+            const uint32_t j = cur.j;
             const int64_t idx = (a.layout == LAYOUT_SORTED) ? (int64_t)i : (int64_t)j;
-            float dw = 1.f;
-            if (a.dcw) dw = a.dcw[j];
+            const float dw = cur.dw;
 #pragma unroll
             for (int c = 0; c < CPL; c++) {
                 const int coil = b0 + ll * CPL + c;
@@ -1093,6 +1145,7 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
                 *o = val;
             }
         }
+        cur = nxt;
     }
 }
 
@@ -1346,8 +1399,8 @@ static void degrid_dispatch(int cg, const ConvArgs &a, dim3 g, size_t smem, cons
 }
 
 static size_t degrid_table_smem(const KParams &k, int cg) {
-    return (((size_t)region_dim(k, 0) * region_dim(k, 1) * region_dim(k, 2) * cg + 1) & ~(size_t)1) *
-           sizeof(float2);
+    const int cs = k.D == 3 ? cg : cg + 2;   // cell stride of k_degrid_table
+    return (size_t)region_dim(k, 0) * region_dim(k, 1) * region_dim(k, 2) * cs * sizeof(float2);
 }
 
 template <int CG, int NT, bool D3>
@@ -1406,7 +1459,8 @@ void launch_degrid(NufftPlan &p, const float2 *grid, float2 *samples, int nb, Sa
     if (p.n_deg_items == 0) return;
     dim3 g(p.n_deg_items, ncg);
     const int nt = (int)std::floor(p.W) + 1;   // most taps a footprint can have per dimension
-    if (!(p.flags & GB_FLAG_COMPENSATED) && p.D >= 2 && cg >= 4 && nt >= 4 && nt <= kWMax) {
+    if (!(p.flags & GB_FLAG_COMPENSATED) && p.D >= 2 && cg >= 4 && nt >= 4 && nt <= kWMax &&
+        degrid_table_smem(p.kp, cg) <= 220 * 1024) {
         degrid_table_dispatch(cg, nt, p.D == 3, a, g, degrid_table_smem(p.kp, cg), grid, samples, st);
     } else {
         const size_t smem = degrid_smem(p.kp, cg);

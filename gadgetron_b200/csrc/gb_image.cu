@@ -61,29 +61,63 @@ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {   // a * conj(b)
     return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 
+// Image rows of N0 pixels spread over a block: rpb rows per block pass,
+// n0c threads per row (index math once per row, threads along x).
+struct RowIter {
+    int rpb, n0c, lr, x0;
+};
+__device__ __forceinline__ RowIter row_iter(int N0) {
+    RowIter it;
+    it.n0c = min(N0, (int)blockDim.x);
+    it.rpb = blockDim.x / it.n0c;
+    it.lr = threadIdx.x / it.n0c;
+    it.x0 = threadIdx.x - it.lr * it.n0c;
+    return it;
+}
+
+// Row R of the [F][N2][N1] row space -> frame, z, y.
+__device__ __forceinline__ void row_coords(const KParams &k, int R, int &f, int &z, int &y, int &rem) {
+    const int rpf = k.N[1] * k.N[2];
+    f = R / rpf;
+    rem = R - f * rpf;
+    z = rem / k.N[1];
+    y = rem - z * k.N[1];
+}
+
 // Forward, interior only.  csm == null: src [nb][F][NN]; else src [F][NN].
 __global__ void k_pad_forward(ImgArgs a, const float2 *__restrict__ src, const float2 *__restrict__ csm,
                               float2 *__restrict__ dst, int nb, int F) {
     const KParams &k = a.k;
-    const int64_t total = (int64_t)F * k.NN;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        const int f = (int)(e / k.NN);
-        const int64_t n = e - (int64_t)f * k.NN;
-        int x, y, z;
-        unflatten(n, k.N, x, y, z);
-        int64_t g;
-        const float fac = interior_factor(a, x, y, z, g);
-        if (csm) {
-            const float2 v = src[e];
-            for (int b = 0; b < nb; b++) {
-                const float2 c = cmul(v, csm[(int64_t)b * k.NN + n]);
-                dst[((int64_t)b * F + f) * k.G + g] = make_float2(c.x * fac, c.y * fac);
-            }
-        } else {
-            for (int b = 0; b < nb; b++) {
-                const float2 v = src[((int64_t)b * F + f) * k.NN + n];
-                dst[((int64_t)b * F + f) * k.G + g] = make_float2(v.x * fac, v.y * fac);
+    const RowIter ri = row_iter(k.N[0]);
+    if (ri.lr >= ri.rpb) return;
+    const int rows = F * k.N[1] * k.N[2];
+    const int ox = (k.mos[0] - k.N[0]) >> 1, oy = (k.mos[1] - k.N[1]) >> 1, oz = (k.mos[2] - k.N[2]) >> 1;
+    for (int R = blockIdx.x * ri.rpb + ri.lr; R < rows; R += gridDim.x * ri.rpb) {
+        int f, z, y, rem;
+        row_coords(k, R, f, z, y, rem);
+        const int gy = y + oy, gz = z + oz;
+        float fyz = a.scale;
+        if (k.D > 1) fyz *= a.deap[a.deap_stride + y];
+        if (k.D > 2) fyz *= a.deap[2 * a.deap_stride + z];
+        const int64_t grow = ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + ox;
+        const int64_t nrow = (int64_t)rem * k.N[0];
+        for (int x = ri.x0; x < k.N[0]; x += ri.n0c) {
+            float fac = a.deap[x] * fyz;
+            if ((x + ox + gy + gz) & 1) fac = -fac;
+            const int64_t g = grow + x, n = nrow + x;
+            if (csm) {
+                const float2 v = src[(int64_t)f * k.NN + n];
+#pragma unroll 8
+                for (int b = 0; b < nb; b++) {
+                    const float2 c = cmul(v, csm[(int64_t)b * k.NN + n]);
+                    dst[((int64_t)b * F + f) * k.G + g] = make_float2(c.x * fac, c.y * fac);
+                }
+            } else {
+#pragma unroll 4
+                for (int b = 0; b < nb; b++) {
+                    const float2 v = src[((int64_t)b * F + f) * k.NN + n];
+                    dst[((int64_t)b * F + f) * k.G + g] = make_float2(v.x * fac, v.y * fac);
+                }
             }
         }
     }
@@ -109,33 +143,46 @@ __global__ void k_pad_forward_os(ImgArgs a, const float2 *__restrict__ src, floa
 __global__ void k_crop_adjoint(ImgArgs a, const float2 *__restrict__ grid, const float2 *__restrict__ csm,
                                float2 *__restrict__ dst, int nb, int F, int accumulate, float weight) {
     const KParams &k = a.k;
-    const int64_t total = (int64_t)F * k.NN;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        const int f = (int)(e / k.NN);
-        const int64_t n = e - (int64_t)f * k.NN;
-        int x, y, z;
-        unflatten(n, k.N, x, y, z);
-        int64_t g;
-        const float fac = interior_factor(a, x, y, z, g) * weight;
-        if (csm) {
-            float2 s = make_float2(0.f, 0.f);
-            for (int b = 0; b < nb; b++) {
-                float2 v = grid[((int64_t)b * F + f) * k.G + g];
-                v = make_float2(v.x * fac, v.y * fac);
-                const float2 c = cmulc(v, csm[(int64_t)b * k.NN + n]);
-                s.x += c.x;
-                s.y += c.y;
-            }
-            if (accumulate) { const float2 o = dst[e]; s.x += o.x; s.y += o.y; }
-            dst[e] = s;
-        } else {
-            for (int b = 0; b < nb; b++) {
-                const float2 v = grid[((int64_t)b * F + f) * k.G + g];
-                float2 r = make_float2(v.x * fac, v.y * fac);
-                float2 *o = dst + ((int64_t)b * F + f) * k.NN + n;
-                if (accumulate) { const float2 ov = *o; r.x += ov.x; r.y += ov.y; }
-                *o = r;
+    const RowIter ri = row_iter(k.N[0]);
+    if (ri.lr >= ri.rpb) return;
+    const int rows = F * k.N[1] * k.N[2];
+    const int ox = (k.mos[0] - k.N[0]) >> 1, oy = (k.mos[1] - k.N[1]) >> 1, oz = (k.mos[2] - k.N[2]) >> 1;
+    for (int R = blockIdx.x * ri.rpb + ri.lr; R < rows; R += gridDim.x * ri.rpb) {
+        int f, z, y, rem;
+        row_coords(k, R, f, z, y, rem);
+        const int gy = y + oy, gz = z + oz;
+        float fyz = a.scale;
+        if (k.D > 1) fyz *= a.deap[a.deap_stride + y];
+        if (k.D > 2) fyz *= a.deap[2 * a.deap_stride + z];
+        const int64_t grow = ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + ox;
+        const int64_t nrow = (int64_t)rem * k.N[0];
+        for (int x = ri.x0; x < k.N[0]; x += ri.n0c) {
+            float fac = a.deap[x] * fyz;
+            if ((x + ox + gy + gz) & 1) fac = -fac;
+            fac *= weight;
+            const int64_t g = grow + x, n = nrow + x;
+            const int64_t e = (int64_t)f * k.NN + n;
+            if (csm) {
+                float2 sacc = make_float2(0.f, 0.f);
+#pragma unroll 8
+                for (int b = 0; b < nb; b++) {
+                    float2 v = grid[((int64_t)b * F + f) * k.G + g];
+                    v = make_float2(v.x * fac, v.y * fac);
+                    const float2 c = cmulc(v, csm[(int64_t)b * k.NN + n]);
+                    sacc.x += c.x;
+                    sacc.y += c.y;
+                }
+                if (accumulate) { const float2 o = dst[e]; sacc.x += o.x; sacc.y += o.y; }
+                dst[e] = sacc;
+            } else {
+#pragma unroll 4
+                for (int b = 0; b < nb; b++) {
+                    const float2 v = grid[((int64_t)b * F + f) * k.G + g];
+                    float2 r = make_float2(v.x * fac, v.y * fac);
+                    float2 *o = dst + ((int64_t)b * F + f) * k.NN + n;
+                    if (accumulate) { const float2 ov = *o; r.x += ov.x; r.y += ov.y; }
+                    *o = r;
+                }
             }
         }
     }
@@ -202,6 +249,14 @@ static unsigned grid_for(int64_t n) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16));
 }
 
+// Blocks for the row kernels: one pass over all image rows, at most 16 per SM.
+static unsigned rows_grid(const NufftPlan &p) {
+    const int64_t rows = (int64_t)p.F * p.kp.N[1] * p.kp.N[2];
+    const int n0c = std::min(p.kp.N[0], 256);
+    const int64_t rpb = 256 / n0c;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((rows + rpb - 1) / rpb, 148 * 16));
+}
+
 static ImgArgs img_args(NufftPlan &p, bool oversampled) {
     ImgArgs a{};
     a.k = p.kp;
@@ -219,7 +274,7 @@ void launch_pad_forward(NufftPlan &p, const float2 *src, const float2 *csm, floa
         k_pad_forward_os<<<grid_for(nbf * p.kp.G), 256, 0, st>>>(a, src, dst, nbf); ::gb::note_launch();
     } else {
         ImgArgs a = img_args(p, false);
-        k_pad_forward<<<grid_for((int64_t)p.F * p.kp.NN), 256, 0, st>>>(a, src, csm, dst, nb, (int)p.F); ::gb::note_launch();
+        k_pad_forward<<<rows_grid(p), 256, 0, st>>>(a, src, csm, dst, nb, (int)p.F); ::gb::note_launch();
     }
     GB_CUDA(cudaGetLastError());
 }
@@ -235,7 +290,7 @@ void launch_crop_adjoint(NufftPlan &p, const float2 *grid, const float2 *csm, fl
         k_crop_adjoint_os<<<grid_for(nbf * p.kp.G), 256, 0, st>>>(a, grid, dst, nbf, accumulate ? 1 : 0); ::gb::note_launch();
     } else {
         ImgArgs a = img_args(p, false);
-        k_crop_adjoint<<<grid_for((int64_t)p.F * p.kp.NN), 256, 0, st>>>(a, grid, csm, dst, nb, (int)p.F,
+        k_crop_adjoint<<<rows_grid(p), 256, 0, st>>>(a, grid, csm, dst, nb, (int)p.F,
                                                                          accumulate ? 1 : 0, weight); ::gb::note_launch();
     }
     GB_CUDA(cudaGetLastError());

@@ -256,38 +256,47 @@ __global__ void k_cg_crop_dot(KParams k, const float *deap, int deap_stride, flo
     CgSeg &S = segs[blockIdx.y];
     if (S.done) return;
     const int ox = (k.mos[0] - k.N[0]) >> 1, oy = (k.mos[1] - k.N[1]) >> 1, oz = (k.mos[2] - k.N[2]) >> 1;
-    const int64_t e0 = (int64_t)blockIdx.y * seg_len;
+    // Rows of N0 pixels: a block takes whole rows (index math once per row,
+    // threads along x).
+    const int rows_per_frame = k.N[1] * k.N[2];
+    const int seg_rows = (int)(seg_len / k.N[0]);
+    const int row0 = (int)blockIdx.y * seg_rows;
     double2 acc = make_double2(0.0, 0.0);
-    for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < seg_len;
-         l += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t e = e0 + l;
-        const int f = (int)(e / k.NN);
-        const int64_t n = e - (int64_t)f * k.NN;
-        const int x = (int)(n % k.N[0]);
-        const int y = (int)((n / k.N[0]) % k.N[1]);
-        const int z = (int)(n / ((int64_t)k.N[0] * k.N[1]));
-        const int gx = x + ox, gy = y + oy, gz = z + oz;
-        const int64_t g = ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + gx;
-        float fac = deap[x];
-        if (k.D > 1) fac *= deap[deap_stride + y];
-        if (k.D > 2) fac *= deap[2 * deap_stride + z];
-        if ((gx + gy + gz) & 1) fac = -fac;
-        fac *= scale * weight;
-        float2 s = make_float2(0.f, 0.f);
-        for (int b = 0; b < nb; b++) {
-            const float2 v = grid[((int64_t)b * F + f) * k.G + g];
-            const float2 c = csm[(int64_t)b * k.NN + n];
-            const float vr = v.x * fac, vi = v.y * fac;
-            s.x += vr * c.x + vi * c.y;
-            s.y += vi * c.x - vr * c.y;
+    for (int r = blockIdx.x; r < seg_rows; r += gridDim.x) {
+        const int R = row0 + r;
+        const int f = R / rows_per_frame;
+        const int rem = R - f * rows_per_frame;
+        const int z = rem / k.N[1], y = rem - (rem / k.N[1]) * k.N[1];
+        const int gy = y + oy, gz = z + oz;
+        float fyz = 1.f;
+        if (k.D > 1) fyz = deap[deap_stride + y];
+        if (k.D > 2) fyz *= deap[2 * deap_stride + z];
+        const int64_t grow = ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + ox;   // grid cell of x = 0
+        const int64_t nrow = (int64_t)rem * k.N[0];                            // pixel of x = 0 in a frame
+        const int64_t erow = (int64_t)R * k.N[0];
+        for (int x = threadIdx.x; x < k.N[0]; x += blockDim.x) {
+            const int gx = x + ox;
+            float fac = deap[x] * fyz;
+            if ((gx + gy + gz) & 1) fac = -fac;
+            fac *= scale * weight;
+            const int64_t g = grow + x, n = nrow + x, e = erow + x;
+            float2 s = make_float2(0.f, 0.f);
+#pragma unroll 8
+            for (int b = 0; b < nb; b++) {
+                const float2 v = grid[((int64_t)b * F + f) * k.G + g];
+                const float2 c = csm[(int64_t)b * k.NN + n];
+                const float vr = v.x * fac, vi = v.y * fac;
+                s.x += vr * c.x + vi * c.y;
+                s.y += vi * c.x - vr * c.y;
+            }
+            const float2 pv = p[e];
+            s.x += kappa * pv.x;
+            s.y += kappa * pv.y;
+            q[e] = s;
+            // conj(p) * q
+            acc.x += (double)pv.x * s.x + (double)pv.y * s.y;
+            acc.y += (double)pv.x * s.y - (double)pv.y * s.x;
         }
-        const float2 pv = p[e];
-        s.x += kappa * pv.x;
-        s.y += kappa * pv.y;
-        q[e] = s;
-        // conj(p) * q
-        acc.x += (double)pv.x * s.x + (double)pv.y * s.y;
-        acc.y += (double)pv.x * s.y - (double)pv.y * s.x;
     }
     double2 tot;
     if (last_block_sum(acc, partials, &S.ctr_dot, &tot) && threadIdx.x == 0) {
