@@ -76,47 +76,87 @@ def synth_data_gpu(wl, dev):
 # ------------------------------------------------------------------ clocks ---
 
 class ClockSampler:
-    def __init__(self, index: int, path: str):
+    """SM clock, max clock, power and clock-event reasons of this rank's GPU,
+    polled through NVML every ~2 ms while the timed region runs (the timed
+    region is tens of milliseconds, too short for nvidia-smi's sampling).
+    Read-only: nothing is set on the GPU.  Samples go to `path` as CSV."""
+
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("sw_power_cap", 0x4))
+
+    def __init__(self, device_index: int, path, period_s: float = 0.002):
+        import threading
         self.path = path
-        self.proc = None
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.samples = []
+        self.h = None
+        self._stop = threading.Event()
+        self._thread = None
         try:
-            self.f = open(path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            try:   # match the CUDA device by PCI address (CUDA_VISIBLE_DEVICES may renumber)
+                pr = torch.cuda.get_device_properties(device_index)
+                bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+                self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
         except Exception:
-            self.proc = None
+            self.h = None
+            return
+
+        def poll():
+            nv = self.nv
+            while not self._stop.is_set():
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                    try:
+                        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                    except Exception:
+                        rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                    pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                    self.samples.append((time.perf_counter(), float(sm), int(rs), pw))
+                except Exception:
+                    pass
+                self._stop.wait(period_s)
+
+        self._thread = threading.Thread(target=poll, daemon=True)
+        self._thread.start()
 
     def stop(self):
-        if self.proc is None:
+        if self._thread is None:
             return None
-        self.proc.terminate()
+        self._stop.set()
+        self._thread.join(timeout=5)
         try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.f.close()
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx.append(float(parts[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
+            if self.path is None:
+                raise OSError("no sample file")
+            with open(self.path, "w") as f:
+                f.write("t_s,sm_mhz,max_mhz,reasons_mask,power_w\n")
+                for t, sm, rs, pw in self.samples:
+                    f.write("%.6f,%.0f,%.0f,0x%x,%.1f\n" % (t, sm, self.max_mhz, rs, pw))
+        except OSError:
+            pass
+        if not self.samples:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = sorted({nm for _, _, rs, _ in self.samples for nm, bit in self.REASONS if rs & bit})
+        return {"sm_mhz": float(np.median([sm for _, sm, _, _ in self.samples])), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples), "source": "NVML, 2 ms polling"}
+
+
+def reduce_max_over_ranks(vals, device):
+    """Element-wise max of a float64 vector over all ranks (timings: the job
+    is as slow as its slowest replica).  Identity when not distributed."""
+    import torch
+    import torch.distributed as dist
+    vals = np.asarray(vals, np.float64)
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return vals
+    t = torch.from_numpy(vals.copy()).to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.cpu().numpy()
 
 
 # ------------------------------------------------------------ our arm -------
@@ -162,8 +202,8 @@ def run_ours(args, rank, world, local_rank):
             import torch.distributed as dist
             dist.barrier()
 
-    clk = ClockSampler(local_rank, os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % rank)) \
-        if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else None
+    clk = ClockSampler(local_rank, os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % rank)
+                       if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else None)
     launches0 = lib.gb_kernel_launch_count()
     barrier()
     torch.cuda.synchronize()
@@ -259,12 +299,7 @@ def run_ours(args, rank, world, local_rank):
     bytes_degrid = C * (8 * G + 8 * M) + 4 * 2 * M        # C2NC: grid in, samples out, coordinates
 
     # Reduce timings over ranks (max).
-    vals = np.array([total_ms, e2e_ms, t_grid, t_degrid], np.float64)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.from_numpy(vals).to(dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        vals = t.cpu().numpy()
+    vals = reduce_max_over_ranks([total_ms, e2e_ms, t_grid, t_degrid], dev)
     total_ms, e2e_ms, t_grid, t_degrid = [float(v) for v in vals]
     if rank != 0:
         return None
@@ -277,9 +312,9 @@ def run_ours(args, rank, world, local_rank):
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     if t_grid >= t_degrid:
-        kname, kms, kbytes = "k_grid_nc2c (gridding, 16 coils)", t_grid, bytes_grid
+        kname, kms, kbytes = "k_grid_rows (gridding, 16 coils)", t_grid, bytes_grid
     else:
-        kname, kms, kbytes = "k_degrid_c2nc (degridding, 16 coils)", t_degrid, bytes_degrid
+        kname, kms, kbytes = "k_degrid_table (degridding, 16 coils)", t_degrid, bytes_degrid
     achieved = kbytes / (kms * 1e-3) / 1e9
 
     ms_per_step = total_ms / args.steps
@@ -569,7 +604,7 @@ def run_batched(args):
     384 samples; 12 coils; alpha 2, W 5.5 (not stated by the workload; chosen);
     15 CG iterations.  Batched: one operator over all frames (uneven sample
     counts), per-frame CG scalars, one CUDA graph for the whole solve.  Plain:
-    one operator + solve per frame, no graph."""
+    one operator + solve per frame, no graph, default tiling."""
     import torch
     import gadgetron_b200 as gb
     from gadgetron_b200 import synthetic as S
@@ -592,6 +627,7 @@ def run_batched(args):
     sq_d = torch.from_numpy(sq).to(dev)
     E.set_dcw(sq_d)
     E.preprocess(torch.from_numpy(traj).to(dev), frame_offsets=offs)
+    E.autotune()   # tile shape and coil group for this trajectory set
     y = torch.empty((C, offs[-1]), dtype=torch.complex64, device=dev)
     E.mult_M(torch.from_numpy(ph).to(dev), y)
     rms = float(y.abs().pow(2).mean().sqrt())

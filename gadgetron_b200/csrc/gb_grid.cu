@@ -379,6 +379,8 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
 // Sample order per cell is the list order, as in k_grid_nc2c: the result is
 // bit-reproducible.
 
+constexpr int kChunkR = 64;   // samples staged per pass (row variant)
+
 // Floats per staged sample weight row: tile x + tile y (+ tile z), padded to
 // an odd multiple of 4 so every row starts on a 16-byte boundary and rows of
 // consecutive samples start in different banks.
@@ -388,19 +390,22 @@ __host__ __device__ __forceinline__ int row_tsp(const KParams &k) {
     return 4 * (t4 | 1);
 }
 
+// Per stage: weight rows, values (sample stride cg + 2 float2: an odd
+// number of 16-byte chunks) and footprint ranges.
 __host__ __device__ __forceinline__ int row_stage_bytes(const KParams &k, int cg) {
-    return kChunk * (row_tsp(k) * 4 + cg * 8 + 16);
+    return kChunkR * (row_tsp(k) * 4 + (cg + 2) * 8 + 16);
 }
 
 template <int CG, int RW, int RPW, bool D3>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, (RPW * RW <= 8) ? 3 : 2)
 k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__ grid) {
     constexpr int CP = CG / 2;      // lanes per row: one per coil pair
     constexpr int ROWS = 32 / CP;   // rows per region
+    constexpr int SVS = CG + 2;     // staged values: float2 per sample (padded)
     constexpr int D = D3 ? 3 : 2;
-    constexpr int kWU = kChunk * D * 2;                  // weight-row units (sample, dim, half)
+    constexpr int kWU = kChunkR * D * 2;                  // weight-row units (sample, dim, half)
     constexpr int kWP = (kWU + kThreads - 1) / kThreads;
-    constexpr int kVE = (kChunk * CG + kThreads - 1) / kThreads;
+    constexpr int kVE = (kChunkR * CG + kThreads - 1) / kThreads;
     extern __shared__ __align__(16) unsigned char g_rows_smem[];
     __shared__ int s_last;
 
@@ -420,10 +425,10 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
 
     auto stage_wt = [&](int s) { return reinterpret_cast<float *>(g_rows_smem + s * stage_bytes); };
     auto stage_v = [&](int s) {
-        return reinterpret_cast<float2 *>(g_rows_smem + s * stage_bytes + kChunk * tsp * 4);
+        return reinterpret_cast<float2 *>(g_rows_smem + s * stage_bytes + kChunkR * tsp * 4);
     };
     auto stage_rng = [&](int s) {
-        return reinterpret_cast<uint4 *>(g_rows_smem + s * stage_bytes + kChunk * tsp * 4 + kChunk * CG * 8);
+        return reinterpret_cast<uint4 *>(g_rows_smem + s * stage_bytes + kChunkR * tsp * 4 + kChunkR * SVS * 8);
     };
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -463,13 +468,14 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
                 pt[q] = *reinterpret_cast<const float4 *>(a.wtab + ((int64_t)si * D + d) * kWMax + 4 * (u & 1));
             }
         }
+        // values: lanes run along samples (one coil per load instruction)
 #pragma unroll
         for (int q = 0; q < kVE; q++) {
             const int e = threadIdx.x + q * kThreads;
-            const int i = e / CG, c = e % CG;
+            const int i = e % kChunkR, c = e / kChunkR;
             pv[q] = make_float2(0.f, 0.f);
             pd[q] = 1.f;
-            if (e < kChunk * CG && i < cnt && b0 + c < a.nb) {
+            if (e < kChunkR * CG && i < cnt && b0 + c < a.nb) {
                 const uint32_t si = a.list[base + i];
                 const bool need_j = a.layout != LAYOUT_SORTED || a.dcw;
                 const uint32_t j = need_j ? a.perm[si] : si;
@@ -539,27 +545,27 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
 #pragma unroll
         for (int q = 0; q < kVE; q++) {
             const int e = threadIdx.x + q * kThreads;
-            if (e >= kChunk * CG) break;
+            if (e >= kChunkR * CG) break;
             float2 v = pv[q];
             if (a.dcw) {
                 v.x = pd[q] * v.x;
                 v.y = pd[q] * v.y;
             }
-            sv[e] = v;
+            sv[(e % kChunkR) * SVS + e / kChunkR] = v;
         }
     };
 
     int cur = 0;
     if (it.begin < it.end) {
-        const int cnt0 = min(kChunk, it.end - it.begin);
+        const int cnt0 = min(kChunkR, it.end - it.begin);
         prefetch(it.begin, cnt0);
         stage_chunk(0, cnt0);
     }
     __syncthreads();
-    for (int base = it.begin; base < it.end; base += kChunk) {
-        const int cnt = min(kChunk, it.end - base);
-        const int nbase = base + kChunk;
-        const int ncnt = nbase < it.end ? min(kChunk, it.end - nbase) : 0;
+    for (int base = it.begin; base < it.end; base += kChunkR) {
+        const int cnt = min(kChunkR, it.end - base);
+        const int nbase = base + kChunkR;
+        const int ncnt = nbase < it.end ? min(kChunkR, it.end - nbase) : 0;
         if (ncnt > 0) prefetch(nbase, ncnt);
         const float *wt = stage_wt(cur);
         const float4 *sv4 = reinterpret_cast<const float4 *>(stage_v(cur));
@@ -568,7 +574,7 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
         for (int c = 0; c < RPW; c++) {
             const int ry = qy0[c] + row;
 #pragma unroll
-            for (int half = 0; half < kChunk / 32; half++) {
+            for (int half = 0; half < kChunkR / 32; half++) {
                 const int il = half * 32 + lane;
                 bool hit = false;
                 if (il < cnt) {
@@ -581,7 +587,7 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
                 while (bits) {
                     const int i = half * 32 + __ffs(bits) - 1;
                     bits &= bits - 1;
-                    const float4 v = sv4[i * CP + cp];
+                    const float4 v = sv4[i * (SVS / 2) + cp];
                     const float *wr = wt + i * tsp;
                     float wyz = wr[T0 + ry];
                     if (D3) wyz *= wr[T0 + T1 + qz[c]];
@@ -620,12 +626,51 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
             *o = w;
         }
     };
-    if (it.split < 0) {
+    // Writes the accumulators to the grid.  Through shared memory when the
+    // tile fits the stage buffers: lanes put their cells into a [coil][z][y][x]
+    // tile (rows padded by one cell, coil planes to 2 mod 8 cells: conflict-
+    // free), then threads store whole rows of one coil plane (coalesced).
+    // Every thread of the CTA calls it (it has a barrier).
+    auto epilogue = [&]() {
+        const int T2 = k.tile[2];
+        const int RS = T0 + 1, ZS = T1 * RS;
+        int PS = T2 * ZS;
+        PS += (10 - PS % 8) % 8;   // PS = 2 (mod 8)
+        if ((int64_t)CG * PS * 8 > 2 * (int64_t)stage_bytes) {
+#pragma unroll
+            for (int c = 0; c < RPW; c++)
+#pragma unroll
+                for (int j = 0; j < RW; j++)
+                    store(c, j, make_float4(acc[c][j][0], acc[c][j][1], acc[c][j][2], acc[c][j][3]));
+            return;
+        }
+        float2 *tl = reinterpret_cast<float2 *>(g_rows_smem);
 #pragma unroll
         for (int c = 0; c < RPW; c++)
 #pragma unroll
-            for (int j = 0; j < RW; j++)
-                store(c, j, make_float4(acc[c][j][0], acc[c][j][1], acc[c][j][2], acc[c][j][3]));
+            for (int j = 0; j < RW; j++) {
+                const int o = qz[c] * ZS + (qy0[c] + row) * RS + qx0[c] + j;
+                tl[(2 * cp) * PS + o] = make_float2(acc[c][j][0], acc[c][j][1]);
+                tl[(2 * cp + 1) * PS + o] = make_float2(acc[c][j][2], acc[c][j][3]);
+            }
+        __syncthreads();
+        const int x = threadIdx.x % T0, r0 = threadIdx.x / T0, rpp = kThreads / T0;
+        if (r0 >= rpp) return;
+        const int rows_c = T2 * T1;
+        for (int R = r0; R < CG * rows_c; R += rpp) {
+            const int c = R / rows_c;
+            if (b0 + c >= a.nb) break;
+            const int rem = R - c * rows_c;
+            const int z = rem / T1, y = rem - z * T1;
+            float2 v = tl[c * PS + z * ZS + y * RS + x];
+            float2 *o = grid + ((int64_t)(b0 + c) * a.F + f) * G +
+                        ((int64_t)(org2 + z) * k.mos[1] + org1 + y) * k.mos[0] + org0 + x;
+            if (a.accumulate) { const float2 old = *o; v.x += old.x; v.y += old.y; }
+            *o = v;
+        }
+    };
+    if (it.split < 0) {
+        epilogue();
         return;
     }
     // Split tile: write this chunk's partial tile, the last CTA sums the
@@ -666,8 +711,12 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
                 s.z += v.z;
                 s.w += v.w;
             }
-            store(c, j, s);
+            acc[c][j][0] = s.x;
+            acc[c][j][1] = s.y;
+            acc[c][j][2] = s.z;
+            acc[c][j][3] = s.w;
         }
+    epilogue();
 }
 
 // --------------------------------------------------------------- C2NC -----
@@ -1117,8 +1166,11 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
                 }
             }
         };
-        const bool shorter = __all_sync(0xffffffffu, n[0] < NT && n[1] < NT && n[2] < NT);
-        if (NT > 4 && shorter)
+        // only when W is an even integer can a footprint have NT = W + 1 taps
+        // (an exact-integer position); otherwise NT taps are common
+        const bool shorter = (NT > 4 && 2 * k.hw < NT) &&
+                             __all_sync(0xffffffffu, n[0] < NT && n[1] < NT && n[2] < NT);
+        if (shorter)
             nest(std::integral_constant<int, (NT > 4 ? NT - 1 : NT)>{});
         else
             nest(std::integral_constant<int, NT>{});

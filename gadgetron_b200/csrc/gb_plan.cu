@@ -432,7 +432,9 @@ void plan_build_work(NufftPlan &p, cudaStream_t st) {
 
     // Degridding items: chunks of at most `deg_chunk` home samples.
     const int64_t M = p.Mtot;
-    int deg_chunk = (int)std::max<int64_t>(64, std::min<int64_t>(1024, M / (148 * 4) + 1));
+    // (large enough that a tile is staged once or a few times; the region
+    // copy is a large share of an item's work in 2D)
+    int deg_chunk = (int)std::max<int64_t>(256, std::min<int64_t>(1024, M / (148 * 4) + 1));
     std::vector<WorkItem> deg;
     for (uint32_t key = 0; key < nkeys; key++) {
         uint32_t b = hoff[key], e = hoff[key + 1];
