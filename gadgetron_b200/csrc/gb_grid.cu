@@ -64,6 +64,7 @@ struct ConvArgs {
     unsigned int *counters;
     int ncg;
     long long part_elems;     // float2 elements of one CTA's partial tile
+    KLayout kl;               // k-space array layout
 };
 
 __device__ __forceinline__ float sign_of(int g) { return (g & 1) ? -1.f : 1.f; }
@@ -290,14 +291,13 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
         cur ^= 1;
     }
 
-    const int64_t G = k.G;
     bool cell_ok[CPT];
 #pragma unroll
     for (int c = 0; c < CPT; c++)
         cell_ok[c] = lc[c][0] < k.tile[0] && lc[c][1] < k.tile[1] && lc[c][2] < k.tile[2];
-    auto cell_index = [&](int c) -> int64_t {
+    auto cell_index = [&](int c) -> int64_t {   // address of the cell within its batch
         const int gx = org[0] + lc[c][0], gy = org[1] + lc[c][1], gz = org[2] + lc[c][2];
-        return ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + gx;
+        return (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y + gx;
     };
     if (it.split < 0) {
 #pragma unroll
@@ -307,7 +307,7 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
 #pragma unroll
             for (int q = 0; q < CG; q++) {
                 if (b0 + q >= a.nb) break;
-                float2 *o = grid + ((int64_t)(b0 + q) * a.F + f) * G + g;
+                float2 *o = grid + ((int64_t)(b0 + q) * a.F + f) * a.kl.s_bf + g;
                 float2 v = make_float2(acc[c][q][0], acc[c][q][1]);
                 if (a.accumulate) { float2 old = *o; v.x += old.x; v.y += old.y; }
                 *o = v;
@@ -358,7 +358,7 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
                     sim += v.y;
                 }
             }
-            float2 *o = grid + ((int64_t)(b0 + q) * a.F + f) * G + g;
+            float2 *o = grid + ((int64_t)(b0 + q) * a.F + f) * a.kl.s_bf + g;
             float2 v = make_float2(sr, sim);
             if (a.accumulate) { float2 old = *o; v.x += old.x; v.y += old.y; }
             *o = v;
@@ -612,15 +612,14 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
         cur ^= 1;
     }
 
-    const int64_t G = k.G;
     auto store = [&](int c, int j, float4 v) {
         const int gx = org0 + qx0[c] + j, gy = org1 + qy0[c] + row, gz = org2 + qz[c];
-        const int64_t g = ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + gx;
+        const int64_t g = (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y + gx;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int q = 2 * cp + h;
             if (b0 + q >= a.nb) break;
-            float2 *o = grid + ((int64_t)(b0 + q) * a.F + f) * G + g;
+            float2 *o = grid + ((int64_t)(b0 + q) * a.F + f) * a.kl.s_bf + g;
             float2 w = h ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
             if (a.accumulate) { const float2 old = *o; w.x += old.x; w.y += old.y; }
             *o = w;
@@ -663,8 +662,8 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
             const int rem = R - c * rows_c;
             const int z = rem / T1, y = rem - z * T1;
             float2 v = tl[c * PS + z * ZS + y * RS + x];
-            float2 *o = grid + ((int64_t)(b0 + c) * a.F + f) * G +
-                        ((int64_t)(org2 + z) * k.mos[1] + org1 + y) * k.mos[0] + org0 + x;
+            float2 *o = grid + ((int64_t)(b0 + c) * a.F + f) * a.kl.s_bf + (int64_t)(org2 + z) * a.kl.s_z +
+                        (int64_t)(org1 + y) * a.kl.s_y + org0 + x;
             if (a.accumulate) { const float2 old = *o; v.x += old.x; v.y += old.y; }
             *o = v;
         }
@@ -786,7 +785,7 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
             gy = gy < 0 ? gy + k.mos[1] : (gy >= k.mos[1] ? gy - k.mos[1] : gy);
             int gz = org[2] - h2 + rz;
             gz = gz < 0 ? gz + k.mos[2] : (gz >= k.mos[2] ? gz - k.mos[2] : gz);
-            const int64_t rowoff = (int64_t)f * k.G + ((int64_t)gz * k.mos[1] + gy) * k.mos[0];
+            const int64_t rowoff = (int64_t)f * a.kl.s_bf + (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y;
             float2 *dst = tile_s + (size_t)row * rowElems;
             for (int e = lane; e < rowElems; e += 32) {
                 const int c = e % CG;          // CG is a power of two
@@ -796,7 +795,7 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
                 // asynchronous 8-byte copy global -> shared (all of a thread's
                 // copies in flight at once); coils beyond nb are zero-filled
                 const bool in = b0 + c < a.nb;
-                const float2 *src = in ? &grid[(int64_t)(b0 + c) * a.F * k.G + rowoff + gx] : grid;
+                const float2 *src = in ? &grid[(int64_t)(b0 + c) * a.F * a.kl.s_bf + rowoff + gx] : grid;
                 const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst + e);
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(src),
                              "r"(in ? 8 : 0)
@@ -1063,8 +1062,8 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
         const int rsub = lane / XW, xl = lane - rsub * XW;
         const int nrows = R1 * R2;
         const int gx0 = org0 - k.hw;
-        const int64_t pstride = (int64_t)a.F * k.G;
-        const float2 *fbase = grid + (int64_t)b0 * pstride + (int64_t)f * k.G;
+        const int64_t pstride = (int64_t)a.F * a.kl.s_bf;
+        const float2 *fbase = grid + (int64_t)b0 * pstride + (int64_t)f * a.kl.s_bf;
         for (int row0 = warp * RPS; row0 < nrows; row0 += 8 * RPS) {
             const int row = row0 + rsub;
             if (row < nrows) {
@@ -1073,7 +1072,7 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
                 gy = gy < 0 ? gy + k.mos[1] : (gy >= k.mos[1] ? gy - k.mos[1] : gy);
                 int gz = org2 - h2 + rz;
                 gz = gz < 0 ? gz + k.mos[2] : (gz >= k.mos[2] ? gz - k.mos[2] : gz);
-                const float2 *src_row = fbase + ((int64_t)gz * k.mos[1] + gy) * k.mos[0];
+                const float2 *src_row = fbase + (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y;
                 for (int xo = xl; xo < R0; xo += XW) {
                     int gx = gx0 + xo;
                     gx = gx < 0 ? gx + k.mos[0] : (gx >= k.mos[0] ? gx - k.mos[0] : gx);
@@ -1218,6 +1217,7 @@ static ConvArgs make_args(NufftPlan &p, int nb, SampleLayout layout, const float
     a.k = p.kp;
     a.pos = p.pos_sorted.get();
     a.wtab = p.wtab.get();
+    a.kl = klayout_standard(p.kp);
     a.perm = p.perm.get();
     a.Mtot = p.Mtot;
     a.F = (int)p.F;
@@ -1365,10 +1365,11 @@ void launch_grid_prepare(NufftPlan &p, int nb, cudaStream_t st) {
 }
 
 void launch_grid(NufftPlan &p, const float2 *samples, float2 *grid, int nb, SampleLayout layout,
-                 const float *dcw, bool sign_fold, bool accumulate, cudaStream_t st) {
+                 const float *dcw, bool sign_fold, bool accumulate, cudaStream_t st, const KLayout *kl) {
     if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
     const GridCfg c = grid_config(p, nb);
     ConvArgs a = make_args(p, nb, layout, dcw, 1, sign_fold, accumulate);
+    if (kl) a.kl = *kl;
     a.list = p.grid_list.get();
     a.items = p.grd_items.get();
     a.n_items = p.n_grd_items;
@@ -1501,11 +1502,13 @@ static int degrid_cg(NufftPlan &p, int nb, bool grad = false) {
 }
 
 void launch_degrid(NufftPlan &p, const float2 *grid, float2 *samples, int nb, SampleLayout layout,
-                   const float *dcw, int dcw_pow, bool sign_fold, bool accumulate, cudaStream_t st) {
+                   const float *dcw, int dcw_pow, bool sign_fold, bool accumulate, cudaStream_t st,
+                   const KLayout *kl) {
     if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
     const int cg = degrid_cg(p, nb);
     const int ncg = (nb + cg - 1) / cg;
     ConvArgs a = make_args(p, nb, layout, dcw, dcw_pow, sign_fold, accumulate);
+    if (kl) a.kl = *kl;
     a.items = p.deg_items.get();
     a.n_items = p.n_deg_items;
     if (p.n_deg_items == 0) return;
@@ -1525,11 +1528,12 @@ void launch_degrid(NufftPlan &p, const float2 *grid, float2 *samples, int nb, Sa
 }
 
 void launch_traj_grad(NufftPlan &p, const float2 *grid, const float2 *weights, int nb,
-                      const float *dcw, float *grad, bool sign_fold, cudaStream_t st) {
+                      const float *dcw, float *grad, bool sign_fold, cudaStream_t st, const KLayout *kl) {
     if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
     const int cg = degrid_cg(p, nb, true);
     const int ncg = (nb + cg - 1) / cg;
     ConvArgs a = make_args(p, nb, LAYOUT_ORIGINAL, dcw, 1, sign_fold, false);
+    if (kl) a.kl = *kl;
     a.items = p.deg_items.get();
     a.n_items = p.n_deg_items;
     const int64_t n = p.Mtot * p.D;

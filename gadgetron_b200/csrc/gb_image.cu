@@ -23,6 +23,8 @@ struct ImgArgs {
     const float *deap;     // [D][stride] per-dim reciprocal transforms
     int deap_stride;
     float scale;
+    KLayout kl;            // layout of the oversampled array
+    int full_lines;        // pad: write whole lines of the interior band (outer-major workspaces)
 };
 
 __device__ __forceinline__ void unflatten(int64_t n, const int *sz, int &x, int &y, int &z) {
@@ -84,39 +86,71 @@ __device__ __forceinline__ void row_coords(const KParams &k, int R, int &f, int 
     y = rem - z * k.N[1];
 }
 
-// Forward, interior only.  csm == null: src [nb][F][NN]; else src [F][NN].
+// Forward.  csm == null: src [nb][F][NN]; else src [F][NN].  Interior only,
+// or (full_lines) every padded line of the interior band -- the rows of the
+// N1-row band in 2D, all mos1 rows of the N2 band slices in 3D -- with zeros
+// outside the interior, so that an in-place FFT pass over the band can follow.
 __global__ void k_pad_forward(ImgArgs a, const float2 *__restrict__ src, const float2 *__restrict__ csm,
-                              float2 *__restrict__ dst, int nb, int F) {
+                              float2 *__restrict__ dst, int nb, int F, PUpdate pu) {
     const KParams &k = a.k;
-    const RowIter ri = row_iter(k.N[0]);
+    const bool full = a.full_lines != 0;
+    const int width = full ? k.mos[0] : k.N[0];
+    const RowIter ri = row_iter(width);
     if (ri.lr >= ri.rpb) return;
-    const int rows = F * k.N[1] * k.N[2];
+    const int lines_y = (full && k.D == 3) ? k.mos[1] : k.N[1];   // lines per (frame, slice)
+    const int lines = F * k.N[2] * lines_y;
     const int ox = (k.mos[0] - k.N[0]) >> 1, oy = (k.mos[1] - k.N[1]) >> 1, oz = (k.mos[2] - k.N[2]) >> 1;
-    for (int R = blockIdx.x * ri.rpb + ri.lr; R < rows; R += gridDim.x * ri.rpb) {
-        int f, z, y, rem;
-        row_coords(k, R, f, z, y, rem);
-        const int gy = y + oy, gz = z + oz;
+    for (int L = blockIdx.x * ri.rpb + ri.lr; L < lines; L += gridDim.x * ri.rpb) {
+        const int fz = L / lines_y, ly = L - fz * lines_y;
+        const int f = fz / k.N[2], z = fz - f * k.N[2];
+        const int gy = (full && k.D == 3) ? ly : ly + oy, gz = z + oz;
+        const int y = gy - oy;
+        const bool yin = y >= 0 && y < k.N[1];
         float fyz = a.scale;
-        if (k.D > 1) fyz *= a.deap[a.deap_stride + y];
-        if (k.D > 2) fyz *= a.deap[2 * a.deap_stride + z];
-        const int64_t grow = ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + ox;
-        const int64_t nrow = (int64_t)rem * k.N[0];
-        for (int x = ri.x0; x < k.N[0]; x += ri.n0c) {
-            float fac = a.deap[x] * fyz;
-            if ((x + ox + gy + gz) & 1) fac = -fac;
-            const int64_t g = grow + x, n = nrow + x;
+        if (yin) {
+            if (k.D > 1) fyz *= a.deap[a.deap_stride + y];
+            if (k.D > 2) fyz *= a.deap[2 * a.deap_stride + z];
+        }
+        const int64_t gline = (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y;
+        const int64_t nrow = ((int64_t)z * k.N[1] + y) * k.N[0];
+        for (int xw = ri.x0; xw < width; xw += ri.n0c) {
+            const int gx = full ? xw : xw + ox;
+            const int x = gx - ox;
+            const bool in = yin && x >= 0 && x < k.N[0];
+            float fac = 0.f;
+            if (in) {
+                fac = a.deap[x] * fyz;
+                if ((gx + gy + gz) & 1) fac = -fac;
+            }
+            const int64_t g = gline + gx, n = nrow + x;
             if (csm) {
-                const float2 v = src[(int64_t)f * k.NN + n];
+                float2 v = make_float2(0.f, 0.f);
+                if (in) {
+                    const int64_t e = (int64_t)f * k.NN + n;
+                    if (pu.p) {   // p = beta p + P^2 r (segment still running), in place
+                        v = pu.p[e];
+                        const CgSeg &S = pu.segs[pu.seg_per_frame ? f : 0];
+                        if (!S.done) {
+                            const float b = (float)S.beta;
+                            float2 rv = pu.r[e];
+                            if (pu.P) { const float w = pu.P[e]; const float w2 = w * w; rv.x *= w2; rv.y *= w2; }
+                            v = make_float2(b * v.x + rv.x, b * v.y + rv.y);
+                            pu.p[e] = v;
+                        }
+                    } else {
+                        v = src[e];
+                    }
+                }
 #pragma unroll 8
                 for (int b = 0; b < nb; b++) {
-                    const float2 c = cmul(v, csm[(int64_t)b * k.NN + n]);
-                    dst[((int64_t)b * F + f) * k.G + g] = make_float2(c.x * fac, c.y * fac);
+                    const float2 c = in ? cmul(v, csm[(int64_t)b * k.NN + n]) : make_float2(0.f, 0.f);
+                    dst[((int64_t)b * F + f) * a.kl.s_bf + g] = make_float2(c.x * fac, c.y * fac);
                 }
             } else {
 #pragma unroll 4
                 for (int b = 0; b < nb; b++) {
-                    const float2 v = src[((int64_t)b * F + f) * k.NN + n];
-                    dst[((int64_t)b * F + f) * k.G + g] = make_float2(v.x * fac, v.y * fac);
+                    const float2 v = in ? src[((int64_t)b * F + f) * k.NN + n] : make_float2(0.f, 0.f);
+                    dst[((int64_t)b * F + f) * a.kl.s_bf + g] = make_float2(v.x * fac, v.y * fac);
                 }
             }
         }
@@ -130,12 +164,12 @@ __global__ void k_pad_forward_os(ImgArgs a, const float2 *__restrict__ src, floa
     const int64_t total = nbf * k.G;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t g = e % k.G;
+        const int64_t bf = e / k.G, g = e - bf * k.G;
         int x, y, z;
         unflatten(g, k.mos, x, y, z);
         const float fac = os_factor(a, x, y, z);
         const float2 v = src[e];
-        dst[e] = make_float2(v.x * fac, v.y * fac);
+        dst[kaddr(a.kl, bf, x, y, z)] = make_float2(v.x * fac, v.y * fac);
     }
 }
 
@@ -154,7 +188,7 @@ __global__ void k_crop_adjoint(ImgArgs a, const float2 *__restrict__ grid, const
         float fyz = a.scale;
         if (k.D > 1) fyz *= a.deap[a.deap_stride + y];
         if (k.D > 2) fyz *= a.deap[2 * a.deap_stride + z];
-        const int64_t grow = ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + ox;
+        const int64_t grow = (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y + ox;
         const int64_t nrow = (int64_t)rem * k.N[0];
         for (int x = ri.x0; x < k.N[0]; x += ri.n0c) {
             float fac = a.deap[x] * fyz;
@@ -166,7 +200,7 @@ __global__ void k_crop_adjoint(ImgArgs a, const float2 *__restrict__ grid, const
                 float2 sacc = make_float2(0.f, 0.f);
 #pragma unroll 8
                 for (int b = 0; b < nb; b++) {
-                    float2 v = grid[((int64_t)b * F + f) * k.G + g];
+                    float2 v = grid[((int64_t)b * F + f) * a.kl.s_bf + g];
                     v = make_float2(v.x * fac, v.y * fac);
                     const float2 c = cmulc(v, csm[(int64_t)b * k.NN + n]);
                     sacc.x += c.x;
@@ -177,7 +211,7 @@ __global__ void k_crop_adjoint(ImgArgs a, const float2 *__restrict__ grid, const
             } else {
 #pragma unroll 4
                 for (int b = 0; b < nb; b++) {
-                    const float2 v = grid[((int64_t)b * F + f) * k.G + g];
+                    const float2 v = grid[((int64_t)b * F + f) * a.kl.s_bf + g];
                     float2 r = make_float2(v.x * fac, v.y * fac);
                     float2 *o = dst + ((int64_t)b * F + f) * k.NN + n;
                     if (accumulate) { const float2 ov = *o; r.x += ov.x; r.y += ov.y; }
@@ -194,11 +228,11 @@ __global__ void k_crop_adjoint_os(ImgArgs a, const float2 *__restrict__ grid, fl
     const int64_t total = nbf * k.G;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t g = e % k.G;
+        const int64_t bf = e / k.G, g = e - bf * k.G;
         int x, y, z;
         unflatten(g, k.mos, x, y, z);
         const float fac = os_factor(a, x, y, z);
-        const float2 v = grid[e];
+        const float2 v = grid[kaddr(a.kl, bf, x, y, z)];
         float2 r = make_float2(v.x * fac, v.y * fac);
         if (accumulate) { const float2 o = dst[e]; r.x += o.x; r.y += o.y; }
         dst[e] = r;
@@ -250,16 +284,20 @@ static unsigned grid_for(int64_t n) {
 }
 
 // Blocks for the row kernels: one pass over all image rows, at most 16 per SM.
-static unsigned rows_grid(const NufftPlan &p) {
-    const int64_t rows = (int64_t)p.F * p.kp.N[1] * p.kp.N[2];
-    const int n0c = std::min(p.kp.N[0], 256);
+static unsigned rows_grid(int64_t rows, int width) {
+    const int n0c = std::min(width, 256);
     const int64_t rpb = 256 / n0c;
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>((rows + rpb - 1) / rpb, 148 * 16));
 }
 
-static ImgArgs img_args(NufftPlan &p, bool oversampled) {
+static unsigned rows_grid(const NufftPlan &p) {
+    return rows_grid((int64_t)p.F * p.kp.N[1] * p.kp.N[2], p.kp.N[0]);
+}
+
+static ImgArgs img_args(NufftPlan &p, bool oversampled, const KLayout *kl) {
     ImgArgs a{};
     a.k = p.kp;
+    a.kl = kl ? *kl : klayout_standard(p.kp);
     a.deap = oversampled ? p.deap_os.get() : p.deap_img.get();
     a.deap_stride = oversampled ? p.maxmos : p.maxN;
     a.scale = (float)(1.0 / std::sqrt((double)p.kp.G));
@@ -267,29 +305,37 @@ static ImgArgs img_args(NufftPlan &p, bool oversampled) {
 }
 
 void launch_pad_forward(NufftPlan &p, const float2 *src, const float2 *csm, float2 *dst, int nb,
-                        bool src_oversampled, cudaStream_t st) {
+                        bool src_oversampled, cudaStream_t st, const KLayout *kl, const PUpdate *pu) {
+    PUpdate pun{};
+    if (pu) {
+        if (!csm || src_oversampled || pu->p != src) fail(GB_ERR_INTERNAL, "direction update needs the csm pad of p");
+        pun = *pu;
+    }
     if (src_oversampled) {
-        ImgArgs a = img_args(p, true);
+        ImgArgs a = img_args(p, true, kl);
         const int64_t nbf = (int64_t)nb * p.F;
         k_pad_forward_os<<<grid_for(nbf * p.kp.G), 256, 0, st>>>(a, src, dst, nbf); ::gb::note_launch();
     } else {
-        ImgArgs a = img_args(p, false);
-        k_pad_forward<<<rows_grid(p), 256, 0, st>>>(a, src, csm, dst, nb, (int)p.F); ::gb::note_launch();
+        ImgArgs a = img_args(p, false, kl);
+        a.full_lines = (kl != nullptr && p.D >= 2) ? 1 : 0;   // outer-major workspace: whole band lines
+        const int64_t lines = (int64_t)p.F * p.kp.N[2] * ((a.full_lines && p.D == 3) ? p.kp.mos[1] : p.kp.N[1]);
+        const int width = a.full_lines ? p.kp.mos[0] : p.kp.N[0];
+        k_pad_forward<<<rows_grid(lines, width), 256, 0, st>>>(a, src, csm, dst, nb, (int)p.F, pun); ::gb::note_launch();
     }
     GB_CUDA(cudaGetLastError());
 }
 
 void launch_crop_adjoint(NufftPlan &p, const float2 *grid, const float2 *csm, float2 *dst, int nb,
                          bool dst_oversampled, bool accumulate, float weight, bool fourier_deapod,
-                         cudaStream_t st) {
+                         cudaStream_t st, const KLayout *kl) {
     (void)fourier_deapod;   // both deapodization filters have the same (real) values
     if (dst_oversampled) {
-        ImgArgs a = img_args(p, true);
+        ImgArgs a = img_args(p, true, kl);
         a.scale *= weight;
         const int64_t nbf = (int64_t)nb * p.F;
         k_crop_adjoint_os<<<grid_for(nbf * p.kp.G), 256, 0, st>>>(a, grid, dst, nbf, accumulate ? 1 : 0); ::gb::note_launch();
     } else {
-        ImgArgs a = img_args(p, false);
+        ImgArgs a = img_args(p, false, kl);
         k_crop_adjoint<<<rows_grid(p), 256, 0, st>>>(a, grid, csm, dst, nb, (int)p.F,
                                                                          accumulate ? 1 : 0, weight); ::gb::note_launch();
     }
@@ -302,7 +348,7 @@ void launch_timeswitch_scale(NufftPlan &p, float2 *data, int nbf, float scale, c
 }
 
 void launch_deapodize_os(NufftPlan &p, float2 *data, int nbf, cudaStream_t st) {
-    ImgArgs a = img_args(p, true);
+    ImgArgs a = img_args(p, true, nullptr);
     k_deapodize_os<<<grid_for((int64_t)nbf * p.kp.G), 256, 0, st>>>(a, data, nbf); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 }

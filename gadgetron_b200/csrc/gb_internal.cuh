@@ -101,6 +101,18 @@ struct KParams {
     int ntiles_total;
 };
 
+// Address of cell (x, y, z) of batch bf = b*F + f in a k-space array:
+//   bf*s_bf + z*s_z + y*s_y + x.
+// Standard layout (every array a caller passes in): [bf][z][y][x].
+// Outer-major layout (the plan's own oversampled workspaces, D >= 2): the
+// outermost dimension (y in 2D, z in 3D) is moved in front of the batch,
+// [y][bf][x] or [z][bf][y][x], so that the rows (2D) or slices (3D) of the
+// N-wide interior band form one contiguous run over all batches and the FFT
+// pass over the inner dimensions can skip the zero rows/slices.
+struct KLayout {
+    long long s_bf, s_y, s_z;
+};
+
 // One unit of tile work: frame*ntiles + tile, a range of a sample list and,
 // for gridding tiles split across CTAs, the split bookkeeping.
 struct WorkItem {
@@ -110,6 +122,52 @@ struct WorkItem {
     int split;     // -1: not split; else index into split table
     int chunk;     // chunk index within the split
     int pad0, pad1, pad2;
+};
+
+__host__ __device__ inline KLayout klayout_standard(const KParams &k) {
+    KLayout l;
+    l.s_bf = k.G;
+    l.s_y = k.mos[0];
+    l.s_z = (long long)k.mos[1] * k.mos[0];
+    return l;
+}
+
+__host__ __device__ inline KLayout klayout_outer(const KParams &k, long long nbf) {
+    KLayout l;
+    if (k.D == 2) {
+        l.s_bf = k.mos[0];
+        l.s_y = nbf * k.mos[0];
+        l.s_z = 0;
+    } else if (k.D == 3) {
+        l.s_bf = (long long)k.mos[1] * k.mos[0];
+        l.s_y = k.mos[0];
+        l.s_z = nbf * k.mos[1] * k.mos[0];
+    } else {
+        l = klayout_standard(k);
+    }
+    return l;
+}
+
+__host__ __device__ inline long long kaddr(const KLayout &l, long long bf, int x, int y, int z) {
+    return bf * l.s_bf + z * l.s_z + y * l.s_y + x;
+}
+
+// Device-side scalars of one CG segment (a frame, or all frames).
+struct CgSeg {
+    double rq, rq0, alpha_re, alpha_im, beta, metric;
+    int done, pad;
+    unsigned int ctr_dot, ctr_upd, ctr_init, pad2;
+};
+
+// CG search-direction update folded into the forward pad of the normal
+// operator: p = beta p + P^2 r for segments still running, done in place on
+// the image being padded (p).  seg_per_frame: segment = frame, else one.
+struct PUpdate {
+    float2 *p;
+    const float2 *r;
+    const float *P;
+    const CgSeg *segs;
+    int seg_per_frame;
 };
 
 struct SplitInfo {
@@ -177,9 +235,11 @@ struct NufftPlan {
     DevBuf<float2> img_os;    // padded image, zero outside the interior
     size_t img_os_batches_zeroed = 0;
     bool img_os_dirty = true;
+    int64_t img_os_nbf = -1;       // batch count whose outer-major band the pad buffer holds
     DevBuf<float2> kgrid;     // k-space grid
     DevBuf<float2> samp_ws;   // samples in tile order [batches][Mtot]
-    std::map<int, cufftHandle> fft_plans;   // batch -> plan
+    std::map<int, cufftHandle> fft_plans;   // batch -> plan (standard layout, rank D)
+    std::map<std::pair<int, int>, cufftHandle> fft_plans_om;   // (batch, pass) -> plan (outer-major)
 
     ~NufftPlan();
 };
@@ -192,6 +252,15 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
                      const uint64_t *frame_offsets, gb_prep_mode mode, cudaStream_t st);
 void plan_build_work(NufftPlan &p, cudaStream_t st);
 cufftHandle plan_fft(NufftPlan &p, int batches, cudaStream_t st);
+
+// FFT passes over an outer-major workspace of nbf batches (D >= 2):
+//   FFT_PASS_A_BAND / FFT_PASS_A_FULL: the inner dimensions (x in 2D, y-x
+//     slices in 3D), over the N-wide band of the outer dimension or all of it;
+//   FFT_PASS_B: the outer dimension (y in 2D, z in 3D), every column.
+enum FftPass { FFT_PASS_A_BAND = 0, FFT_PASS_A_FULL = 1, FFT_PASS_B = 2 };
+cufftHandle plan_fft_om(NufftPlan &p, int nbf, FftPass pass, cudaStream_t st);
+// Element offset of the band start for FFT_PASS_A_BAND.
+int64_t fft_band_offset(const NufftPlan &p, int nbf);
 void plan_set_tiling(NufftPlan &p, const int *tile, int cg);
 // Hash of every buffer address and count the convolution kernels' launches
 // depend on: equal signatures mean a captured graph is still valid.
@@ -209,30 +278,36 @@ enum SampleLayout { LAYOUT_ORIGINAL = 0, LAYOUT_SORTED = 1 };
 // times (1 or 2).
 void launch_degrid(NufftPlan &p, const float2 *grid, float2 *samples, int nb,
                    SampleLayout layout, const float *dcw, int dcw_pow, bool sign_fold,
-                   bool accumulate, cudaStream_t st);
+                   bool accumulate, cudaStream_t st, const KLayout *kl = nullptr);
 
 // Gridding: samples -> grid [nb][F][G] (overwritten unless accumulate).
 // dcw multiplies the input samples (may be null).
 void launch_grid(NufftPlan &p, const float2 *samples, float2 *grid, int nb,
                  SampleLayout layout, const float *dcw, bool sign_fold, bool accumulate,
-                 cudaStream_t st);
+                 cudaStream_t st, const KLayout *kl = nullptr);
 
 // Trajectory gradient from a k-space grid (sign folded like the degridder).
 void launch_traj_grad(NufftPlan &p, const float2 *grid, const float2 *weights, int nb,
-                      const float *dcw, float *grad, bool sign_fold, cudaStream_t st);
+                      const float *dcw, float *grad, bool sign_fold, cudaStream_t st,
+                      const KLayout *kl = nullptr);
 
 // Image-side fused kernels.
 // Forward: dst_os[b][f][interior] = src[...] * (csm) * deap * sign * scale.
 //   csm == null: src [nb][F][NN] -> dst [nb][F][G]
 //   csm != null: src [F][NN], csm [C][NN] -> dst [C][F][G] (nb = C)
+// With an outer-major dst (D >= 2) the whole rows/slices of the interior band
+// are written (zeros outside the interior), so an in-place FFT pass over the
+// band may follow; the rest of dst must already be zero.
+// pu (optional, csm path only): the CG direction update applied to src first.
 void launch_pad_forward(NufftPlan &p, const float2 *src, const float2 *csm, float2 *dst,
-                        int nb, bool src_oversampled, cudaStream_t st);
+                        int nb, bool src_oversampled, cudaStream_t st, const KLayout *kl = nullptr,
+                        const PUpdate *pu = nullptr);
 // Adjoint: dst[...] (+)= crop(grid) * deap * sign * scale (* conj(csm) summed over coils)
 //   csm == null: grid [nb][F][G] -> dst [nb][F][NN] (or [nb][F][G] when dst_oversampled)
 //   csm != null: grid [C][F][G] -> dst [F][NN]
 void launch_crop_adjoint(NufftPlan &p, const float2 *grid, const float2 *csm, float2 *dst,
                          int nb, bool dst_oversampled, bool accumulate, float weight,
-                         bool fourier_deapod, cudaStream_t st);
+                         bool fourier_deapod, cudaStream_t st, const KLayout *kl = nullptr);
 
 // Reference-form utilities (NFFT_plan::fft / deapodize on oversampled arrays).
 void launch_timeswitch_scale(NufftPlan &p, float2 *data, int nbf, float scale, cudaStream_t st);

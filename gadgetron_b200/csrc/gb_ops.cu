@@ -27,10 +27,13 @@ namespace gb {
 float2 *ensure_img_os(NufftPlan &p, int64_t nbf, cudaStream_t st) {
     const size_t need = (size_t)nbf * p.kp.G;
     const bool re = p.img_os.ensure(need);
-    if (re || p.img_os_dirty || p.img_os_batches_zeroed < (size_t)nbf) {
+    // The zeros outside the interior band must hold for this batch count's
+    // outer-major layout (the band's address range depends on nbf).
+    if (re || p.img_os_dirty || p.img_os_batches_zeroed < (size_t)nbf || (p.D >= 2 && p.img_os_nbf != nbf)) {
         GB_CUDA(cudaMemsetAsync(p.img_os.get(), 0, p.img_os.n * sizeof(float2), st));
         p.img_os_batches_zeroed = p.img_os.n / p.kp.G;
         p.img_os_dirty = false;
+        p.img_os_nbf = nbf;
     }
     return p.img_os.get();
 }
@@ -50,18 +53,65 @@ static void exec_fft(NufftPlan &p, float2 *in, float2 *out, int nbf, int dir, cu
     GB_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex *>(in), reinterpret_cast<cufftComplex *>(out), dir));
 }
 
+static void exec_pass(NufftPlan &p, FftPass pass, float2 *in, float2 *out, int nbf, int dir, cudaStream_t st) {
+    cufftHandle h = plan_fft_om(p, nbf, pass, st);
+    GB_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex *>(in), reinterpret_cast<cufftComplex *>(out), dir));
+}
+
+// Layout of the plan's oversampled workspaces for nbf batches.
+KLayout ws_layout(const NufftPlan &p, int64_t nbf) {
+    return p.D >= 2 ? klayout_outer(p.kp, nbf) : klayout_standard(p.kp);
+}
+
+// Forward FFT of the padded workspace `pad` into `kg`.  D >= 2: the inner
+// pass runs in place over the interior band only (band_only; every other
+// row/slice of `pad` is zero), then the outer pass writes `kg`.  D == 1: one
+// out-of-place transform (pad's zero exterior is kept).
+static void fft_forward_ws(NufftPlan &p, float2 *pad, float2 *kg, int nbf, int dir, bool band_only,
+                           cudaStream_t st) {
+    if (p.D < 2) {
+        exec_fft(p, pad, kg, nbf, dir, st);
+        return;
+    }
+    if (band_only) {
+        float2 *band = pad + fft_band_offset(p, nbf);
+        exec_pass(p, FFT_PASS_A_BAND, band, band, nbf, dir, st);
+    } else {
+        exec_pass(p, FFT_PASS_A_FULL, pad, pad, nbf, dir, st);
+    }
+    exec_pass(p, FFT_PASS_B, pad, kg, nbf, dir, st);
+}
+
+// In-place FFT of the gridded workspace `kg` for the crop: the outer pass over
+// every column, then the inner pass over the interior band only (band_only)
+// or everything.
+static void fft_adjoint_ws(NufftPlan &p, float2 *kg, int nbf, int dir, bool band_only, cudaStream_t st) {
+    if (p.D < 2) {
+        exec_fft(p, kg, kg, nbf, dir, st);
+        return;
+    }
+    exec_pass(p, FFT_PASS_B, kg, kg, nbf, dir, st);
+    if (band_only) {
+        float2 *band = kg + fft_band_offset(p, nbf);
+        exec_pass(p, FFT_PASS_A_BAND, band, band, nbf, dir, st);
+    } else {
+        exec_pass(p, FFT_PASS_A_FULL, kg, kg, nbf, dir, st);
+    }
+}
+
 // Forward NUFFT into device sample buffer (layout chosen by caller).
 // csm != null: image [F][NN] and nb = coils.
 void nufft_forward(NufftPlan &p, const float2 *img, const float2 *csm, int nb, bool img_os,
                    float2 *samples, SampleLayout layout, const float *dcw, int dcw_pow,
-                   bool accumulate, cudaStream_t st) {
+                   bool accumulate, cudaStream_t st, const PUpdate *pu) {
     const int64_t nbf = (int64_t)nb * p.F;
+    const KLayout kl = ws_layout(p, nbf);
     float2 *pad = ensure_img_os(p, nbf, st);
     float2 *kg = ensure_kgrid(p, nbf);
-    launch_pad_forward(p, img, csm, pad, nb, img_os, st);
+    launch_pad_forward(p, img, csm, pad, nb, img_os, st, &kl, pu);
     if (img_os) p.img_os_dirty = true;
-    exec_fft(p, pad, kg, (int)nbf, CUFFT_FORWARD, st);
-    launch_degrid(p, kg, samples, nb, layout, dcw, dcw_pow, true, accumulate, st);
+    fft_forward_ws(p, pad, kg, (int)nbf, CUFFT_FORWARD, !img_os, st);
+    launch_degrid(p, kg, samples, nb, layout, dcw, dcw_pow, true, accumulate, st, &kl);
 }
 
 // Adjoint NUFFT from samples.  csm != null: out image [F][NN], nb = coils.
@@ -69,10 +119,11 @@ void nufft_adjoint(NufftPlan &p, const float2 *samples, SampleLayout layout, con
                    const float2 *csm, int nb, float2 *img, bool img_os, bool accumulate, float weight,
                    int fft_dir, cudaStream_t st) {
     const int64_t nbf = (int64_t)nb * p.F;
+    const KLayout kl = ws_layout(p, nbf);
     float2 *kg = ensure_kgrid(p, nbf);
-    launch_grid(p, samples, kg, nb, layout, dcw, true, false, st);
-    exec_fft(p, kg, kg, (int)nbf, fft_dir, st);
-    launch_crop_adjoint(p, kg, csm, img, nb, img_os, accumulate, weight, fft_dir == CUFFT_FORWARD, st);
+    launch_grid(p, samples, kg, nb, layout, dcw, true, false, st, &kl);
+    fft_adjoint_ws(p, kg, (int)nbf, fft_dir, !img_os, st);
+    launch_crop_adjoint(p, kg, csm, img, nb, img_os, accumulate, weight, fft_dir == CUFFT_FORWARD, st, &kl);
 }
 
 // Normal operator A^H W^2 A on images (csm optional), samples stay in tile order.
@@ -140,11 +191,12 @@ void nufft_traj_grad(NufftPlan &p, const float2 *img, const float2 *weights, con
                      int nb, cudaStream_t st) {
     if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
     const int64_t nbf = (int64_t)nb * p.F;
+    const KLayout kl = ws_layout(p, nbf);
     float2 *pad = ensure_img_os(p, nbf, st);
     float2 *kg = ensure_kgrid(p, nbf);
-    launch_pad_forward(p, img, nullptr, pad, nb, false, st);
-    exec_fft(p, pad, kg, (int)nbf, CUFFT_FORWARD, st);
-    launch_traj_grad(p, kg, weights, nb, dcw, grad, true, st);
+    launch_pad_forward(p, img, nullptr, pad, nb, false, st, &kl);
+    fft_forward_ws(p, pad, kg, (int)nbf, CUFFT_FORWARD, true, st);
+    launch_traj_grad(p, kg, weights, nb, dcw, grad, true, st, &kl);
 }
 
 void nufft_traj_grad_from_grid(NufftPlan &p, const float2 *grid, const float2 *weights, float *grad, int nb,
@@ -185,12 +237,6 @@ void sense_mult_MH_M(SenseOp &s, const void *in, void *out, bool accumulate, cud
 // independently (one per frame when frames are solved independently, a
 // single segment for the reference's coupled solve): each segment has its own
 // rq, rq0, alpha, beta and stop flag.
-struct CgSeg {
-    double rq, rq0, alpha_re, alpha_im, beta, metric;
-    int done, pad;
-    unsigned int ctr_dot, ctr_upd, ctr_init, pad2;
-};
-
 struct CgGlobal {
     double tol;
     int iters, hist_base, all_done, pad;
@@ -249,7 +295,7 @@ __device__ bool last_block_sum(double2 mine, double2 *partials, unsigned int *ct
 }
 
 // q = weight * crop(...) + kappa * p, then <p, q> per segment -> alpha = rq / <p, q>.
-__global__ void k_cg_crop_dot(KParams k, const float *deap, int deap_stride, float scale,
+__global__ void k_cg_crop_dot(KParams k, KLayout kl, const float *deap, int deap_stride, float scale,
                               const float2 *__restrict__ grid, const float2 *__restrict__ csm, int nb, int F,
                               const float2 *__restrict__ p, float2 *__restrict__ q, float weight, float kappa,
                               CgSeg *segs, int64_t seg_len, double2 *partials) {
@@ -271,7 +317,7 @@ __global__ void k_cg_crop_dot(KParams k, const float *deap, int deap_stride, flo
         float fyz = 1.f;
         if (k.D > 1) fyz = deap[deap_stride + y];
         if (k.D > 2) fyz *= deap[2 * deap_stride + z];
-        const int64_t grow = ((int64_t)gz * k.mos[1] + gy) * k.mos[0] + ox;   // grid cell of x = 0
+        const int64_t grow = (int64_t)gz * kl.s_z + (int64_t)gy * kl.s_y + ox;   // grid cell of x = 0
         const int64_t nrow = (int64_t)rem * k.N[0];                            // pixel of x = 0 in a frame
         const int64_t erow = (int64_t)R * k.N[0];
         for (int x = threadIdx.x; x < k.N[0]; x += blockDim.x) {
@@ -283,7 +329,7 @@ __global__ void k_cg_crop_dot(KParams k, const float *deap, int deap_stride, flo
             float2 s = make_float2(0.f, 0.f);
 #pragma unroll 8
             for (int b = 0; b < nb; b++) {
-                const float2 v = grid[((int64_t)b * F + f) * k.G + g];
+                const float2 v = grid[((int64_t)b * F + f) * kl.s_bf + g];
                 const float2 c = csm[(int64_t)b * k.NN + n];
                 const float vr = v.x * fac, vi = v.y * fac;
                 s.x += vr * c.x + vi * c.y;
@@ -362,23 +408,6 @@ __global__ void k_cg_update(int64_t seg_len, float2 *__restrict__ x, float2 *__r
                 if (all) G->all_done = 1;
             }
         }
-    }
-}
-
-// p = beta p + P^2 r (per segment)
-__global__ void k_cg_pupdate(int64_t seg_len, float2 *__restrict__ p, const float2 *__restrict__ r,
-                             const float *__restrict__ P, int64_t Pn, const CgSeg *segs) {
-    const CgSeg &S = segs[blockIdx.y];
-    if (S.done) return;
-    const float b = (float)S.beta;
-    const int64_t e0 = (int64_t)blockIdx.y * seg_len;
-    for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < seg_len;
-         l += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t e = e0 + l;
-        float2 rv = r[e];
-        if (P) { const float w = P[e]; const float w2 = w * w; rv.x *= w2; rv.y *= w2; }
-        float2 pv = p[e];
-        p[e] = make_float2(b * pv.x + rv.x, b * pv.y + rv.y);
     }
 }
 
@@ -465,31 +494,36 @@ CgSolver::~CgSolver() {
 }
 
 // E^H E p -> q with the fused crop/dot kernel (used inside the iteration).
-static void cg_normal_dot(CgSolver &cg, cudaStream_t st) {
+// update_p: first apply the previous iteration's direction update
+// p = beta p + P^2 r (folded into the forward pad).
+static void cg_normal_dot(CgSolver &cg, cudaStream_t st, bool update_p) {
     SenseOp &s = *cg.E;
     NufftPlan &p = s.plan;
     const int nb = s.ncoils;
     const int64_t nbf = (int64_t)nb * p.F;
     float2 *samp = ensure_samp(p, nb);
-    nufft_forward(p, cg.p.get(), s.csm, nb, false, samp, LAYOUT_SORTED, s.dcw, 2, false, st);
+    PUpdate pu{cg.p.get(), cg.r.get(), cg.precond, cg.segs.get(), cg.nseg > 1 ? 1 : 0};
+    nufft_forward(p, cg.p.get(), s.csm, nb, false, samp, LAYOUT_SORTED, s.dcw, 2, false, st,
+                  update_p ? &pu : nullptr);
     float2 *kg = ensure_kgrid(p, nbf);
-    launch_grid(p, samp, kg, nb, LAYOUT_SORTED, nullptr, true, false, st);
-    exec_fft(p, kg, kg, (int)nbf, CUFFT_INVERSE, st);
-    k_cg_crop_dot<<<seg_grid(cg), 256, 0, st>>>(p.kp, p.deap_img.get(), p.maxN,
+    const KLayout kl = ws_layout(p, nbf);
+    launch_grid(p, samp, kg, nb, LAYOUT_SORTED, nullptr, true, false, st, &kl);
+    fft_adjoint_ws(p, kg, (int)nbf, CUFFT_INVERSE, true, st);
+    k_cg_crop_dot<<<seg_grid(cg), 256, 0, st>>>(p.kp, kl, p.deap_img.get(), p.maxN,
                                                 (float)(1.0 / std::sqrt((double)p.kp.G)), kg, s.csm, nb,
                                                 (int)p.F, cg.p.get(), cg.q.get(), cg.weight, cg.kappa, cg.segs.get(),
                                                 cg.seg_len, cg.partials.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 }
 
-static void cg_iteration(CgSolver &cg, cudaStream_t st, double *hist) {
+// One iteration.  The direction update p = beta p + P^2 r of the previous
+// iteration runs inside this iteration's forward pad (none after the last).
+static void cg_iteration(CgSolver &cg, cudaStream_t st, double *hist, bool first) {
     NufftPlan &p = cg.E->plan;
     const int64_t n = (int64_t)p.F * p.kp.NN;
-    cg_normal_dot(cg, st);
+    cg_normal_dot(cg, st, !first);
     k_cg_update<<<seg_grid(cg), 256, 0, st>>>(cg.seg_len, cg.x.get(), cg.r.get(), cg.p.get(), cg.q.get(),
                                               cg.precond, n, cg.segs.get(), cg.G.get(), cg.partials.get(), hist); ::gb::note_launch();
-    GB_CUDA(cudaGetLastError());
-    k_cg_pupdate<<<seg_grid(cg), 256, 0, st>>>(cg.seg_len, cg.p.get(), cg.r.get(), cg.precond, n, cg.segs.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 }
 
@@ -515,7 +549,7 @@ static void cg_solve_once(CgSolver &cg, const float2 *rhs, const float2 *x0, dou
                                                 cg.partials.get(), 0, (double)cg.tol, hist_base); ::gb::note_launch();
         GB_CUDA(cudaGetLastError());
     }
-    for (uint32_t it = 0; it < cg.iterations; it++) cg_iteration(cg, st, hist);
+    for (uint32_t it = 0; it < cg.iterations; it++) cg_iteration(cg, st, hist, it == 0);
 }
 
 static void cg_prepare(CgSolver &cg, cudaStream_t st) {
@@ -541,6 +575,8 @@ static void cg_prepare(CgSolver &cg, cudaStream_t st) {
     ensure_kgrid(p, (int64_t)nb * p.F);
     ensure_samp(p, nb);
     plan_fft(p, nb * (int)p.F, st);
+    if (p.D >= 2)   // plans are made outside stream capture
+        for (FftPass pass : {FFT_PASS_A_BAND, FFT_PASS_A_FULL, FFT_PASS_B}) plan_fft_om(p, nb * (int)p.F, pass, st);
     // Split-tile counters/partials for the gridding kernel.
     launch_grid_prepare(p, nb, st);
 }

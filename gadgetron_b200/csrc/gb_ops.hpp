@@ -65,7 +65,8 @@ float2 *ensure_kgrid(NufftPlan &p, int64_t nbf);
 float2 *ensure_samp(NufftPlan &p, int nb);
 void launch_grid_prepare(NufftPlan &p, int nb, cudaStream_t st);
 void nufft_forward(NufftPlan &p, const float2 *img, const float2 *csm, int nb, bool img_os, float2 *samples,
-                   SampleLayout layout, const float *dcw, int dcw_pow, bool accumulate, cudaStream_t st);
+                   SampleLayout layout, const float *dcw, int dcw_pow, bool accumulate, cudaStream_t st,
+                   const PUpdate *pu = nullptr);
 void nufft_adjoint(NufftPlan &p, const float2 *samples, SampleLayout layout, const float *dcw, const float2 *csm,
                    int nb, float2 *img, bool img_os, bool accumulate, float weight, int fft_dir, cudaStream_t st);
 void nufft_normal(NufftPlan &p, const float2 *img, const float2 *csm, int nb, const float *dcw, float2 *out,

@@ -29,6 +29,7 @@ namespace gb {
 
 NufftPlan::~NufftPlan() {
     for (auto &kv : fft_plans) cufftDestroy(kv.second);
+    for (auto &kv : fft_plans_om) cufftDestroy(kv.second);
 }
 
 static double host_kb1(float delta, const NufftPlan &p, int d) {
@@ -529,6 +530,10 @@ uint64_t plan_layout_signature(const NufftPlan &p, int nbf) {
     for (int64_t v : vals) mix((uint64_t)v);
     auto it = p.fft_plans.find(nbf);
     mix(it == p.fft_plans.end() ? 0ull : (uint64_t)it->second);
+    for (int pass = 0; pass < 3; pass++) {
+        auto jt = p.fft_plans_om.find(std::make_pair(nbf, pass));
+        mix(jt == p.fft_plans_om.end() ? 0ull : (uint64_t)jt->second);
+    }
     return h;
 }
 
@@ -574,6 +579,45 @@ cufftHandle plan_fft(NufftPlan &p, int batches, cudaStream_t st) {
         int dist = (int)p.kp.G;
         GB_CUFFT(cufftPlanMany(&h, p.D, n, n, 1, dist, n, 1, dist, CUFFT_C2C, batches));
         p.fft_plans[batches] = h;
+    } else {
+        h = it->second;
+    }
+    GB_CUFFT(cufftSetStream(h, st));
+    return h;
+}
+
+int64_t fft_band_offset(const NufftPlan &p, int nbf) {
+    const KParams &k = p.kp;
+    if (p.D == 2) return (int64_t)((k.mos[1] - k.N[1]) / 2) * nbf * k.mos[0];
+    return (int64_t)((k.mos[2] - k.N[2]) / 2) * nbf * k.mos[1] * k.mos[0];
+}
+
+cufftHandle plan_fft_om(NufftPlan &p, int nbf, FftPass pass, cudaStream_t st) {
+    if (p.D < 2) fail(GB_ERR_INTERNAL, "outer-major FFT passes need D >= 2");
+    const auto key = std::make_pair(nbf, (int)pass);
+    auto it = p.fft_plans_om.find(key);
+    cufftHandle h;
+    if (it == p.fft_plans_om.end()) {
+        const KParams &k = p.kp;
+        if (pass == FFT_PASS_B) {
+            // the outer dimension: stride = one outer step (all batches' inner planes)
+            const int inner = p.D == 2 ? k.mos[0] : k.mos[1] * k.mos[0];
+            int n[1] = {p.D == 2 ? k.mos[1] : k.mos[2]};
+            const long long stride = (long long)nbf * inner;
+            if (stride > INT32_MAX) fail(GB_ERR_INVALID_ARGUMENT, "k-space workspace too large for the FFT plan");
+            GB_CUFFT(cufftPlanMany(&h, 1, n, n, (int)stride, 1, n, (int)stride, 1, CUFFT_C2C, nbf * inner));
+        } else {
+            const int outer = pass == FFT_PASS_A_BAND ? (p.D == 2 ? k.N[1] : k.N[2]) : (p.D == 2 ? k.mos[1] : k.mos[2]);
+            if (p.D == 2) {
+                int n[1] = {k.mos[0]};
+                GB_CUFFT(cufftPlanMany(&h, 1, n, n, 1, k.mos[0], n, 1, k.mos[0], CUFFT_C2C, outer * nbf));
+            } else {
+                int n[2] = {k.mos[1], k.mos[0]};
+                const int dist = k.mos[1] * k.mos[0];
+                GB_CUFFT(cufftPlanMany(&h, 2, n, n, 1, dist, n, 1, dist, CUFFT_C2C, outer * nbf));
+            }
+        }
+        p.fft_plans_om[key] = h;
     } else {
         h = it->second;
     }
