@@ -65,6 +65,9 @@ struct ConvArgs {
     int ncg;
     long long part_elems;     // float2 elements of one CTA's partial tile
     KLayout kl;               // k-space array layout
+    const float *prows;       // gridding pair rows (row variant)
+    int prow_floats;
+    unsigned int *err;        // bounded-wait failure flag
 };
 
 __device__ __forceinline__ float sign_of(int g) { return (g & 1) ? -1.f : 1.f; }
@@ -381,19 +384,53 @@ k_grid_nc2c(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
 
 constexpr int kChunkR = 64;   // samples staged per pass (row variant)
 
-// Floats per staged sample weight row: tile x + tile y (+ tile z), padded to
-// an odd multiple of 4 so every row starts on a 16-byte boundary and rows of
-// consecutive samples start in different banks.
-__host__ __device__ __forceinline__ int row_tsp(const KParams &k) {
-    const int ts = k.tile[0] + k.tile[1] + (k.D == 3 ? k.tile[2] : 0);
-    const int t4 = (ts + 3) >> 2;
-    return 4 * (t4 | 1);
+// Per stage: the chunk's pair rows (one bulk copy) and its values (sample
+// stride cg + 2 float2: an odd number of 16-byte chunks).
+__host__ __device__ __forceinline__ int row_stage_bytes(const KParams &k, int cg) {
+    return kChunkR * (pair_row_floats(k) * 4 + (cg + 2) * 8);
 }
 
-// Per stage: weight rows, values (sample stride cg + 2 float2: an odd
-// number of 16-byte chunks) and footprint ranges.
-__host__ __device__ __forceinline__ int row_stage_bytes(const KParams &k, int cg) {
-    return kChunkR * (row_tsp(k) * 4 + (cg + 2) * 8 + 16);
+// mbarrier + bulk-copy (TMA) helpers.  Waits are bounded: after ~1 s a wait
+// records the failure in *err and waits once more (also bounded) for the copy
+// still in flight, then gives up; the results are then wrong but no thread
+// spins forever.
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void mbar_wait_bounded(uint32_t bar, uint32_t parity, unsigned int *err) {
+    for (int round = 0; round < 2; round++) {
+        for (uint32_t i = 0; i < (1u << 22); i++) {
+            if (mbar_try_wait(bar, parity)) return;
+            if (i >= 16) __nanosleep(256);
+        }
+        if (round == 0 && err) atomicOr(err, 1u);
+    }
 }
 
 template <int CG, int RW, int RPW, bool D3>
@@ -402,11 +439,8 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
     constexpr int CP = CG / 2;      // lanes per row: one per coil pair
     constexpr int ROWS = 32 / CP;   // rows per region
     constexpr int SVS = CG + 2;     // staged values: float2 per sample (padded)
-    constexpr int D = D3 ? 3 : 2;
-    constexpr int kWU = kChunkR * D * 2;                  // weight-row units (sample, dim, half)
-    constexpr int kWP = (kWU + kThreads - 1) / kThreads;
     constexpr int kVE = (kChunkR * CG + kThreads - 1) / kThreads;
-    extern __shared__ __align__(16) unsigned char g_rows_smem[];
+    extern __shared__ __align__(128) unsigned char g_rows_smem[];
     __shared__ int s_last;
 
     const KParams &k = a.k;
@@ -420,15 +454,14 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
     const int tz = tile / (k.ntiles[0] * k.ntiles[1]);
     const int org0 = tx * k.tile[0], org1 = ty * k.tile[1], org2 = tz * k.tile[2];
     const int T0 = k.tile[0], T1 = k.tile[1];
-    const int tsp = row_tsp(k);
+    const int PRF = a.prow_floats;   // floats per pair row
+    const int PRW = PRF - 4;         // weight part; the last 4 words are the footprint ranges
     const int stage_bytes = row_stage_bytes(k, CG);
+    __shared__ __align__(8) unsigned long long s_bar[2];   // one mbarrier per stage
 
     auto stage_wt = [&](int s) { return reinterpret_cast<float *>(g_rows_smem + s * stage_bytes); };
     auto stage_v = [&](int s) {
-        return reinterpret_cast<float2 *>(g_rows_smem + s * stage_bytes + kChunkR * tsp * 4);
-    };
-    auto stage_rng = [&](int s) {
-        return reinterpret_cast<uint4 *>(g_rows_smem + s * stage_bytes + kChunkR * tsp * 4 + kChunkR * SVS * 8);
+        return reinterpret_cast<float2 *>(g_rows_smem + s * stage_bytes + kChunkR * PRF * 4);
     };
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -449,26 +482,32 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
 #pragma unroll
         for (int j = 0; j < RW; j++) acc[c][j][0] = acc[c][j][1] = acc[c][j][2] = acc[c][j][3] = 0.f;
 
-    float pw[kWP];
-    float4 pt[kWP];
+    const uint32_t bar[2] = {smem_u32(&s_bar[0]), smem_u32(&s_bar[1])};
+    if (threadIdx.x == 0) {
+        mbar_init(bar[0], 1);
+        mbar_init(bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    uint32_t phase = 0;   // bit s: parity of stage s's next barrier completion
+
+    // The pair rows of a chunk are contiguous (list order): thread 0 starts
+    // one bulk copy (TMA) of them into stage s.  Stage s was last read before
+    // the preceding __syncthreads; the proxy fence orders those reads before
+    // the asynchronous write.
+    auto issue_rows = [&](int s, int base, int cnt) {
+        if (threadIdx.x == 0) {
+            fence_proxy_async_smem();
+            const uint32_t bytes = (uint32_t)cnt * (uint32_t)PRF * 4u;
+            mbar_expect_tx(bar[s], bytes);
+            bulk_copy_g2s(smem_u32(stage_wt(s)), a.prows + (int64_t)base * PRF, bytes, bar[s]);
+        }
+    };
+
     float2 pv[kVE];
     float pd[kVE];
-
+    // values: lanes run along samples (one coil per load instruction)
     auto prefetch = [&](int base, int cnt) {
-#pragma unroll
-        for (int q = 0; q < kWP; q++) {
-            const int u = threadIdx.x + q * kThreads;
-            const int pr = u >> 1, i = pr / D, d = pr - i * D;
-            pw[q] = 0.f;
-            pt[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (u < kWU && i < cnt) {
-                const uint32_t si = a.list[base + i];
-                pw[q] = a.pos[(int64_t)d * a.Mtot + si];
-                // taps 4*sub .. 4*sub+3 of (sample, dim)
-                pt[q] = *reinterpret_cast<const float4 *>(a.wtab + ((int64_t)si * D + d) * kWMax + 4 * (u & 1));
-            }
-        }
-        // values: lanes run along samples (one coil per load instruction)
 #pragma unroll
         for (int q = 0; q < kVE; q++) {
             const int e = threadIdx.x + q * kThreads;
@@ -485,63 +524,9 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
             }
         }
     };
-
-    // Writes the prefetched chunk into stage s: per sample and dimension a
-    // weight row over the tile (zeroed, then the footprint's taps written by
-    // the same pair of lanes after __syncwarp), the tile-local footprint
-    // range, and the values with the density weights folded in.
-    auto stage_chunk = [&](int s, int cnt) {
-        float *wt = stage_wt(s);
+    // Values of the prefetched chunk into stage s, density weights folded in.
+    auto stage_values = [&](int s) {
         float2 *sv = stage_v(s);
-        unsigned *rng = reinterpret_cast<unsigned *>(stage_rng(s));
-#pragma unroll
-        for (int q = 0; q < kWP; q++) {
-            const int u = threadIdx.x + q * kThreads;
-            const int pr = u >> 1, i = pr / D, d = pr - i * D, sub = u & 1;
-            const bool active = u < kWU && i < cnt;
-            const int Td = k.tile[d];
-            float *rowp = wt + i * tsp + (d == 0 ? 0 : (d == 1 ? T0 : T0 + T1));
-            if (active) {
-                // row offsets are multiples of 4 floats; Td is for x and y
-                for (int e4 = sub; e4 < (Td >> 2); e4 += 2)
-                    *reinterpret_cast<float4 *>(rowp + 4 * e4) = make_float4(0.f, 0.f, 0.f, 0.f);
-                for (int e = (Td & ~3) + sub; e < Td; e += 2) rowp[e] = 0.f;
-            }
-            __syncwarp();
-            if (active) {
-                const float sp = pw[q];
-                const int lo = (int)ceilf(sp - k.radius);
-                const int n = min((int)floorf(sp + k.radius) - lo + 1, kWMax);
-                const int od = d == 0 ? org0 : (d == 1 ? org1 : org2);
-                // tile-local footprint start (lo - hw - od) mod mos; |lo - hw - od| < 2 mos
-                int a0 = lo - k.hw - od;
-                a0 = a0 < 0 ? a0 + k.mos[d] : (a0 >= k.mos[d] ? a0 - k.mos[d] : a0);
-                const float tw[4] = {pt[q].x, pt[q].y, pt[q].z, pt[q].w};
-#pragma unroll
-                for (int m = 0; m < 4; m++) {
-                    const int t = 4 * sub + m;
-                    int e = a0 + t;
-                    if (e >= k.mos[d]) e -= k.mos[d];
-                    if (t < n && e >= 0 && e < Td) {
-                        float w = tw[m];
-                        if (a.sign_fold) w *= sign_of((lo + t - k.hw) & 1);
-                        rowp[e] = w;
-                    }
-                }
-                if (sub == 0) {
-                    int rlo, rhi;
-                    if (k.ntiles[d] == 1) {   // the footprint may wrap inside the tile
-                        rlo = 0;
-                        rhi = Td - 1;
-                    } else {
-                        const int st = (a0 < Td) ? a0 : a0 - k.mos[d];
-                        rlo = max(st, 0);
-                        rhi = min(st + n - 1, Td - 1);
-                    }
-                    rng[i * 4 + d] = (unsigned)rlo | ((unsigned)rhi << 16);
-                }
-            }
-        }
 #pragma unroll
         for (int q = 0; q < kVE; q++) {
             const int e = threadIdx.x + q * kThreads;
@@ -558,18 +543,23 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
     int cur = 0;
     if (it.begin < it.end) {
         const int cnt0 = min(kChunkR, it.end - it.begin);
+        issue_rows(0, it.begin, cnt0);
         prefetch(it.begin, cnt0);
-        stage_chunk(0, cnt0);
+        stage_values(0);
     }
     __syncthreads();
     for (int base = it.begin; base < it.end; base += kChunkR) {
         const int cnt = min(kChunkR, it.end - base);
         const int nbase = base + kChunkR;
         const int ncnt = nbase < it.end ? min(kChunkR, it.end - nbase) : 0;
-        if (ncnt > 0) prefetch(nbase, ncnt);
+        if (ncnt > 0) {
+            issue_rows(cur ^ 1, nbase, ncnt);
+            prefetch(nbase, ncnt);
+        }
+        mbar_wait_bounded(bar[cur], (phase >> cur) & 1u, a.err);
+        phase ^= 1u << cur;
         const float *wt = stage_wt(cur);
         const float4 *sv4 = reinterpret_cast<const float4 *>(stage_v(cur));
-        const uint4 *rng = stage_rng(cur);
 #pragma unroll
         for (int c = 0; c < RPW; c++) {
             const int ry = qy0[c] + row;
@@ -578,7 +568,7 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
                 const int il = half * 32 + lane;
                 bool hit = false;
                 if (il < cnt) {
-                    const uint4 r = rng[il];
+                    const uint4 r = *reinterpret_cast<const uint4 *>(wt + il * PRF + PRW);
                     hit = (int)(r.x & 0xffffu) <= qx0[c] + RW - 1 && (int)(r.x >> 16) >= qx0[c] &&
                           (int)(r.y & 0xffffu) <= qy0[c] + ROWS - 1 && (int)(r.y >> 16) >= qy0[c];
                     if (D3) hit = hit && (int)(r.z & 0xffffu) <= qz[c] && (int)(r.z >> 16) >= qz[c];
@@ -588,7 +578,7 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
                     const int i = half * 32 + __ffs(bits) - 1;
                     bits &= bits - 1;
                     const float4 v = sv4[i * (SVS / 2) + cp];
-                    const float *wr = wt + i * tsp;
+                    const float *wr = wt + i * PRF;
                     float wyz = wr[T0 + ry];
                     if (D3) wyz *= wr[T0 + T1 + qz[c]];
 #pragma unroll
@@ -607,20 +597,23 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
                 }
             }
         }
-        if (ncnt > 0) stage_chunk(cur ^ 1, ncnt);
+        if (ncnt > 0) stage_values(cur ^ 1);
         __syncthreads();
         cur ^= 1;
     }
 
+    // The centring checkerboard (-1)^(gx+gy+gz) is a property of the output
+    // cell, so it is applied here rather than to every weight.
     auto store = [&](int c, int j, float4 v) {
         const int gx = org0 + qx0[c] + j, gy = org1 + qy0[c] + row, gz = org2 + qz[c];
         const int64_t g = (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y + gx;
+        const float sgn = (a.sign_fold && ((gx + gy + gz) & 1)) ? -1.f : 1.f;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int q = 2 * cp + h;
             if (b0 + q >= a.nb) break;
             float2 *o = grid + ((int64_t)(b0 + q) * a.F + f) * a.kl.s_bf + g;
-            float2 w = h ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
+            float2 w = h ? make_float2(sgn * v.z, sgn * v.w) : make_float2(sgn * v.x, sgn * v.y);
             if (a.accumulate) { const float2 old = *o; w.x += old.x; w.y += old.y; }
             *o = w;
         }
@@ -656,16 +649,23 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
         const int x = threadIdx.x % T0, r0 = threadIdx.x / T0, rpp = kThreads / T0;
         if (r0 >= rpp) return;
         const int rows_c = T2 * T1;
-        for (int R = r0; R < CG * rows_c; R += rpp) {
-            const int c = R / rows_c;
-            if (b0 + c >= a.nb) break;
-            const int rem = R - c * rows_c;
-            const int z = rem / T1, y = rem - z * T1;
-            float2 v = tl[c * PS + z * ZS + y * RS + x];
-            float2 *o = grid + ((int64_t)(b0 + c) * a.F + f) * a.kl.s_bf + (int64_t)(org2 + z) * a.kl.s_z +
-                        (int64_t)(org1 + y) * a.kl.s_y + org0 + x;
-            if (a.accumulate) { const float2 old = *o; v.x += old.x; v.y += old.y; }
-            *o = v;
+        const int gx = org0 + x;
+        for (int r = r0; r < rows_c; r += rpp) {
+            const int z = r / T1, y = r - z * T1;
+            const int gy = org1 + y, gz = org2 + z;
+            const float sgn = (a.sign_fold && ((gx + gy + gz) & 1)) ? -1.f : 1.f;
+            const int64_t cell = (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y + gx;
+            const float2 *src = tl + z * ZS + y * RS + x;
+            float2 *o = grid + ((int64_t)b0 * a.F + f) * a.kl.s_bf + cell;
+            const int64_t ostep = (int64_t)a.F * a.kl.s_bf;
+            for (int c = 0; c < CG && b0 + c < a.nb; c++) {
+                float2 v = src[c * PS];
+                v.x *= sgn;
+                v.y *= sgn;
+                if (a.accumulate) { const float2 old = *o; v.x += old.x; v.y += old.y; }
+                *o = v;
+                o += ostep;
+            }
         }
     };
     if (it.split < 0) {
@@ -1218,6 +1218,9 @@ static ConvArgs make_args(NufftPlan &p, int nb, SampleLayout layout, const float
     a.pos = p.pos_sorted.get();
     a.wtab = p.wtab.get();
     a.kl = klayout_standard(p.kp);
+    a.prows = p.pair_rows.get();
+    a.prow_floats = p.pair_row_stride;
+    a.err = p.err_flag.get();
     a.perm = p.perm.get();
     a.Mtot = p.Mtot;
     a.F = (int)p.F;
@@ -1256,7 +1259,8 @@ static GridCfg grid_config(const NufftPlan &p, int nb) {
     c.cpt = (cells + kThreads - 1) / kThreads;
     const bool comp = (p.flags & GB_FLAG_COMPENSATED) != 0;
     int cg = choose_cg(p.tiling.cg, nb);
-    if (!comp && k.D >= 2 && (cg == 8 || cg == 16)) {
+    if (!comp && k.D >= 2 && (cg == 8 || cg == 16) && p.pair_row_stride > 0 &&
+        p.pair_row_stride == pair_row_floats(k)) {
         const int rows = 64 / cg;
         const int smem = 2 * row_stage_bytes(k, cg);
         if (k.tile[1] % rows == 0 && smem <= 96 * 1024) {

@@ -152,6 +152,12 @@ __host__ __device__ inline long long kaddr(const KLayout &l, long long bf, int x
     return bf * l.s_bf + z * l.s_z + y * l.s_y + x;
 }
 
+// Floats of the weight part of a pair row and of a whole pair row.
+__host__ __device__ inline int pair_row_weights(const KParams &k) {
+    return (k.tile[0] + k.tile[1] + (k.D == 3 ? k.tile[2] : 0) + 3) & ~3;
+}
+__host__ __device__ inline int pair_row_floats(const KParams &k) { return pair_row_weights(k) + 4; }
+
 // Device-side scalars of one CG segment (a frame, or all frames).
 struct CgSeg {
     double rq, rq0, alpha_re, alpha_im, beta, metric;
@@ -213,6 +219,14 @@ struct NufftPlan {
     DevBuf<uint32_t> perm;         // sorted pos -> original sample index
     DevBuf<uint32_t> home_off;     // [F*ntiles + 1]
     DevBuf<uint32_t> grid_list;    // gridding pair list (sorted positions)
+    // Per gridding pair, the sample's 1D weights laid over the tile: rows of
+    // pair_row_stride floats = x weights (tile x), y weights (tile y), z
+    // weights (tile z, 3D), padding to a multiple of 4, then 4 words of the
+    // tile-local footprint ranges (lo | hi << 16 per dimension).  Built at
+    // preprocess for D >= 2 (pair_row_stride = 0 when not built).
+    DevBuf<float> pair_rows;
+    int pair_row_stride = 0;
+    DevBuf<unsigned int> err_flag;   // set by kernels whose bounded waits ran out
     DevBuf<uint32_t> grid_off;     // [F*ntiles + 1]
     DevBuf<WorkItem> deg_items;
     int n_deg_items = 0;

@@ -287,6 +287,54 @@ __global__ void k_write_pairs(KParams k, int64_t M, const float *__restrict__ po
             }
 }
 
+// Pair rows for the row-variant gridding kernel: one thread per (pair,
+// dimension) lays the sample's tap weights (from the weight table, unsigned)
+// over the tile's extent in that dimension -- tap t at tile-local cell
+// (ceil(s - W/2) + t - pad/2 - tile origin) mod mos when that falls inside the
+// tile, zero elsewhere -- and records the tile-local footprint range.
+__global__ void k_pair_rows(KParams k, int64_t M, int64_t npairs, const float *__restrict__ pos_sorted,
+                            const float *__restrict__ wtab, const uint32_t *__restrict__ pair_key,
+                            const uint32_t *__restrict__ pair_sample, float *__restrict__ rows, int row_floats,
+                            int row_weights) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= npairs * k.D) return;
+    const int64_t q = e / k.D;
+    const int d = (int)(e - q * k.D);
+    const uint32_t si = pair_sample[q];
+    const uint32_t tile = pair_key[q] % (uint32_t)k.ntiles_total;
+    const int tc = d == 0 ? (int)(tile % k.ntiles[0])
+                          : (d == 1 ? (int)((tile / k.ntiles[0]) % k.ntiles[1])
+                                    : (int)(tile / (k.ntiles[0] * k.ntiles[1])));
+    const int Td = k.tile[d];
+    const int org = tc * Td;
+    const float sp = pos_sorted[(int64_t)d * M + si];
+    const int lo = (int)ceilf(sp - k.radius);
+    const int n = min((int)floorf(sp + k.radius) - lo + 1, kWMax);
+    int a0 = lo - k.hw - org;   // tile-local footprint start, mod mos
+    a0 = a0 < 0 ? a0 + k.mos[d] : (a0 >= k.mos[d] ? a0 - k.mos[d] : a0);
+    float *row = rows + q * row_floats;
+    float *wr = row + (d == 0 ? 0 : (d == 1 ? k.tile[0] : k.tile[0] + k.tile[1]));
+    const float *taps = wtab + ((int64_t)si * k.D + d) * kWMax;
+    for (int c = 0; c < Td; c++) {
+        int t = c - a0;
+        if (t < 0) t += k.mos[d];
+        wr[c] = t < n ? taps[t] : 0.f;
+    }
+    if (d == 0)
+        for (int c = k.tile[0] + k.tile[1] + (k.D == 3 ? k.tile[2] : 0); c < row_weights; c++) row[c] = 0.f;
+    int rlo, rhi;
+    if (k.ntiles[d] == 1) {   // the footprint may wrap inside the tile
+        rlo = 0;
+        rhi = Td - 1;
+    } else {
+        const int st = (a0 < Td) ? a0 : a0 - k.mos[d];
+        rlo = max(st, 0);
+        rhi = min(st + n - 1, Td - 1);
+    }
+    reinterpret_cast<uint32_t *>(row + row_weights)[d] = (uint32_t)rlo | ((uint32_t)rhi << 16);
+    if (d == 0 && k.D == 2) reinterpret_cast<uint32_t *>(row + row_weights)[2] = 0u;
+}
+
 template <class T>
 static void exclusive_scan(const T *in, T *out, int64_t n, DevBuf<unsigned char> &tmp, cudaStream_t st) {
     size_t bytes = 0;
@@ -405,6 +453,18 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     k_sorted_offsets<<<(unsigned)(((int64_t)npairs + TB) / TB), TB, 0, st>>>(pkey_sorted.get(), npairs,
                                                                             (uint32_t)nkeys, p.grid_off.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
+    // Pair rows for the row-variant gridding kernel (2D/3D tiles up to 96 cells of extent sum).
+    p.pair_row_stride = 0;
+    if (D >= 2 && pair_row_weights(k) <= 96 && npairs > 0) {
+        const int rf = pair_row_floats(k);
+        p.pair_rows.ensure((size_t)npairs * rf);
+        k_pair_rows<<<(unsigned)(((int64_t)npairs * D + TB - 1) / TB), TB, 0, st>>>(
+            k, M, npairs, p.pos_sorted.get(), p.wtab.get(), pkey_sorted.get(), p.grid_list.get(), p.pair_rows.get(),
+            rf, pair_row_weights(k)); ::gb::note_launch();
+        GB_CUDA(cudaGetLastError());
+        p.pair_row_stride = rf;
+    }
+    if (p.err_flag.ensure(1)) GB_CUDA(cudaMemsetAsync(p.err_flag.get(), 0, sizeof(unsigned int), st));
 
     p.F = F;
     p.Mtot = M;
@@ -520,7 +580,7 @@ uint64_t plan_layout_signature(const NufftPlan &p, int nbf) {
             h *= 1099511628211ull;
         }
     };
-    const void *ptrs[] = {p.pos_sorted.get(), p.wtab.get(), p.perm.get(), p.grid_list.get(), p.grd_items.get(),
+    const void *ptrs[] = {p.pos_sorted.get(), p.wtab.get(), p.pair_rows.get(), p.perm.get(), p.grid_list.get(), p.grd_items.get(),
                           p.deg_items.get(), p.splits.get(), p.partials.get(), p.split_counters.get(),
                           p.img_os.get(), p.kgrid.get(), p.samp_ws.get(), p.deap_img.get(), p.deap_os.get()};
     for (const void *q : ptrs) mix((uint64_t)(uintptr_t)q);
