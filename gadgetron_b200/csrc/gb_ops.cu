@@ -411,6 +411,270 @@ __global__ void k_cg_update(int64_t seg_len, float2 *__restrict__ x, float2 *__r
     }
 }
 
+__device__ __forceinline__ float2 cmul2(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// ------------------------------------------------ fused CG iteration tail ---
+//
+// One cooperative launch per iteration replaces crop/<p,q>, the x/r update +
+// <r,P^2 r> and the next iteration's direction update + forward pad.  Blocks
+// keep the same image rows through all phases, so the only exchange between
+// blocks is the two segment sums, taken through a grid barrier; every block
+// of a segment sums the segment's block partials in the same order, so all
+// of them hold bit-identical scalars.  Arithmetic is that of k_cg_crop_dot,
+// k_cg_update and the pad kernel with the direction update.
+
+struct TailArgs {
+    KParams k;
+    KLayout kl;
+    const float *deap;       // [D][deap_stride] image-domain deapodization
+    int deap_stride;
+    float scale;             // 1/sqrt(G)
+    const float2 *kg;        // k-space workspace after the inverse FFT (band rows transformed)
+    const float2 *csm;
+    int nb, F;
+    float2 *x, *r, *p, *q;
+    const float *P;
+    float weight, kappa;
+    CgSeg *segs;
+    CgGlobal *G;
+    double2 *part1, *part2;  // [nseg][gridDim.x]
+    double *hist;
+    unsigned int *bar;       // grid barrier: arrival count, generation
+    unsigned int *err;
+    float2 *pad;             // next iteration's padded image (outer-major), or null after the last iteration
+    int seg_rows;            // image rows (of N0 pixels) per segment
+};
+
+// Grid-wide barrier for a cooperative launch (all blocks resident).  The
+// wait is bounded: past ~4 s it records the failure in *err and returns.
+__device__ void tail_grid_barrier(unsigned int *bar, unsigned int nblocks, unsigned int *err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int *vb = bar;
+        const unsigned int gen = vb[1];
+        __threadfence();
+        const unsigned int arrived = atomicAdd(&bar[0], 1u) + 1u;
+        if (arrived == nblocks) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        } else {
+            for (uint32_t i = 0; vb[1] == gen; i++) {
+                if (i >= (1u << 26)) {
+                    atomicOr(err, 2u);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// Sum of a segment's block partials in a fixed order (same result in every block).
+__device__ double2 tail_segment_sum(const double2 *part, int nparts, double2 *sh) {
+    double2 v = make_double2(0.0, 0.0);
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) {
+        const double2 t = __ldcg(&part[b]);
+        v.x += t.x;
+        v.y += t.y;
+    }
+    v = block_reduce_d2(v, sh);
+    __shared__ double2 s_tot;
+    if (threadIdx.x == 0) s_tot = v;
+    __syncthreads();
+    const double2 tot = s_tot;
+    __syncthreads();
+    return tot;
+}
+
+__global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
+    __shared__ double2 sh[32];
+    const KParams &k = t.k;
+    const int seg = blockIdx.y, nbx = gridDim.x;
+    const unsigned int nblocks = gridDim.x * gridDim.y;
+    CgSeg &S = t.segs[seg];
+    const bool was_done = S.done != 0;
+    const double rq = S.rq, rq0 = S.rq0;
+    const int ox = (k.mos[0] - k.N[0]) >> 1, oy = (k.mos[1] - k.N[1]) >> 1, oz = (k.mos[2] - k.N[2]) >> 1;
+    const int rows_per_frame = k.N[1] * k.N[2];
+    const int row0 = seg * t.seg_rows;
+    auto row_coords = [&](int R, int &f, int &z, int &y, int &rem) {
+        f = R / rows_per_frame;
+        rem = R - f * rows_per_frame;
+        z = rem / k.N[1];
+        y = rem - z * k.N[1];
+    };
+
+    // Phase 1: q = weight * crop(kg) * conj(csm) summed + kappa p ; <p, q>.
+    double2 acc = make_double2(0.0, 0.0);
+    if (!was_done) {
+        for (int rr = blockIdx.x; rr < t.seg_rows; rr += nbx) {
+            int f, z, y, rem;
+            row_coords(row0 + rr, f, z, y, rem);
+            const int gy = y + oy, gz = z + oz;
+            float fyz = 1.f;
+            if (k.D > 1) fyz = t.deap[t.deap_stride + y];
+            if (k.D > 2) fyz *= t.deap[2 * t.deap_stride + z];
+            const int64_t grow = (int64_t)gz * t.kl.s_z + (int64_t)gy * t.kl.s_y + ox;
+            const int64_t nrow = (int64_t)rem * k.N[0];
+            const int64_t erow = (int64_t)(row0 + rr) * k.N[0];
+            for (int x = threadIdx.x; x < k.N[0]; x += blockDim.x) {
+                const int gx = x + ox;
+                float fac = t.deap[x] * fyz;
+                if ((gx + gy + gz) & 1) fac = -fac;
+                fac *= t.scale * t.weight;
+                const int64_t g = grow + x, n = nrow + x, e = erow + x;
+                float2 s = make_float2(0.f, 0.f);
+#pragma unroll 8
+                for (int b = 0; b < t.nb; b++) {
+                    const float2 v = t.kg[((int64_t)b * t.F + f) * t.kl.s_bf + g];
+                    const float2 c = t.csm[(int64_t)b * k.NN + n];
+                    const float vr = v.x * fac, vi = v.y * fac;
+                    s.x += vr * c.x + vi * c.y;
+                    s.y += vi * c.x - vr * c.y;
+                }
+                const float2 pv = t.p[e];
+                s.x += t.kappa * pv.x;
+                s.y += t.kappa * pv.y;
+                t.q[e] = s;
+                acc.x += (double)pv.x * s.x + (double)pv.y * s.y;
+                acc.y += (double)pv.x * s.y - (double)pv.y * s.x;
+            }
+        }
+    }
+    acc = block_reduce_d2(acc, sh);
+    if (threadIdx.x == 0) t.part1[(size_t)seg * nbx + blockIdx.x] = acc;
+    tail_grid_barrier(t.bar, nblocks, t.err);
+
+    // Phase 2: alpha = rq / <p,q> ; x += alpha p ; r -= alpha q ; <r, P^2 r>.
+    const double2 pq = tail_segment_sum(t.part1 + (size_t)seg * nbx, nbx, sh);
+    double alpha_re = 0.0, alpha_im = 0.0;
+    acc = make_double2(0.0, 0.0);
+    if (!was_done) {
+        const double den = pq.x * pq.x + pq.y * pq.y;
+        alpha_re = rq * pq.x / den;
+        alpha_im = -rq * pq.y / den;
+        const float ar = (float)alpha_re, ai = (float)alpha_im;
+        for (int rr = blockIdx.x; rr < t.seg_rows; rr += nbx) {
+            const int64_t erow = (int64_t)(row0 + rr) * k.N[0];
+            for (int x = threadIdx.x; x < k.N[0]; x += blockDim.x) {
+                const int64_t e = erow + x;
+                const float2 pv = t.p[e], qv = t.q[e];
+                float2 xv = t.x[e], rv = t.r[e];
+                xv.x += ar * pv.x - ai * pv.y;
+                xv.y += ar * pv.y + ai * pv.x;
+                rv.x -= ar * qv.x - ai * qv.y;
+                rv.y -= ar * qv.y + ai * qv.x;
+                t.x[e] = xv;
+                t.r[e] = rv;
+                float w2 = 1.f;
+                if (t.P) { const float w = t.P[e]; w2 = w * w; }
+                acc.x += (double)rv.x * (double)(rv.x * w2) + (double)rv.y * (double)(rv.y * w2);
+            }
+        }
+    }
+    acc = block_reduce_d2(acc, sh);
+    if (threadIdx.x == 0) t.part2[(size_t)seg * nbx + blockIdx.x] = acc;
+    tail_grid_barrier(t.bar, nblocks, t.err);
+
+    // Phase 3: segment scalars, stop rule, history; then the direction update
+    // p = beta p + P^2 r and the forward pad of p for the next iteration.
+    const double2 rr2 = tail_segment_sum(t.part2 + (size_t)seg * nbx, nbx, sh);
+    bool done_now = was_done;
+    float beta = 0.f;
+    if (!was_done) {
+        const double rq_new = rr2.x;
+        beta = (float)(rq_new / rq);
+        done_now = (rq_new / rq0) < t.G->tol;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (!was_done) {
+            const double rq_new = rr2.x;
+            S.alpha_re = alpha_re;
+            S.alpha_im = alpha_im;
+            S.beta = rq_new / rq;
+            S.rq = rq_new;
+            S.metric = rq_new / rq0;
+            if (S.metric < t.G->tol) S.done = 1;
+        }
+        __threadfence();
+        const unsigned int old = atomicAdd(&t.G->seg_ctr, 1u);
+        if (old == gridDim.y - 1) {   // last segment of this iteration
+            __threadfence();
+            t.G->seg_ctr = 0u;
+            if (!t.G->all_done) {
+                double mx = 0.0;
+                int all = 1;
+                for (unsigned s = 0; s < gridDim.y; s++) {
+                    const double m = *((volatile double *)&t.segs[s].metric);
+                    mx = m > mx ? m : mx;
+                    all &= (*((volatile int *)&t.segs[s].done) != 0);
+                }
+                if (t.hist) t.hist[t.G->hist_base + t.G->iters] = mx;
+                t.G->iters += 1;
+                if (all) t.G->all_done = 1;
+            }
+        }
+    }
+    if (!t.pad) return;
+    for (int rr = blockIdx.x; rr < t.seg_rows; rr += nbx) {
+        int f, z, y, rem;
+        row_coords(row0 + rr, f, z, y, rem);
+        const int gy = y + oy, gz = z + oz;
+        float fyz = t.scale;
+        if (k.D > 1) fyz *= t.deap[t.deap_stride + y];
+        if (k.D > 2) fyz *= t.deap[2 * t.deap_stride + z];
+        const int64_t gline = (int64_t)gz * t.kl.s_z + (int64_t)gy * t.kl.s_y;
+        const int64_t nrow = (int64_t)rem * k.N[0];
+        const int64_t erow = (int64_t)(row0 + rr) * k.N[0];
+        for (int gx = threadIdx.x; gx < k.mos[0]; gx += blockDim.x) {
+            const int x = gx - ox;
+            const bool in = x >= 0 && x < k.N[0];
+            float fac = 0.f;
+            float2 v = make_float2(0.f, 0.f);
+            if (in) {
+                const int64_t e = erow + x;
+                v = t.p[e];
+                if (!done_now) {
+                    float2 rv = t.r[e];
+                    if (t.P) { const float w = t.P[e]; const float w2 = w * w; rv.x *= w2; rv.y *= w2; }
+                    v = make_float2(beta * v.x + rv.x, beta * v.y + rv.y);
+                    t.p[e] = v;
+                }
+                fac = t.deap[x] * fyz;
+                if ((gx + gy + gz) & 1) fac = -fac;
+            }
+            const int64_t g = gline + gx, n = nrow + x;
+#pragma unroll 8
+            for (int b = 0; b < t.nb; b++) {
+                const float2 c = in ? cmul2(v, t.csm[(int64_t)b * k.NN + n]) : make_float2(0.f, 0.f);
+                t.pad[((int64_t)b * t.F + f) * t.kl.s_bf + g] = make_float2(c.x * fac, c.y * fac);
+            }
+        }
+    }
+    if (k.D == 3) {
+        // rows of the band slices outside the interior rows: zero (the band
+        // FFT pass overwrote them)
+        const int zrows = k.mos[1] - k.N[1];
+        const int64_t lines = (int64_t)t.F * k.N[2] * zrows;
+        const int64_t nblk = (int64_t)gridDim.x * gridDim.y, bid = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+        for (int64_t L = bid; L < lines; L += nblk) {
+            const int j = (int)(L % zrows);
+            const int64_t fz = L / zrows;
+            const int z = (int)(fz % k.N[2]), f = (int)(fz / k.N[2]);
+            const int gy = j < oy ? j : j + k.N[1], gz = z + oz;
+            const int64_t gline = (int64_t)gz * t.kl.s_z + (int64_t)gy * t.kl.s_y;
+            for (int b = 0; b < t.nb; b++)
+                for (int gx = threadIdx.x; gx < k.mos[0]; gx += blockDim.x)
+                    t.pad[((int64_t)b * t.F + f) * t.kl.s_bf + gline + gx] = make_float2(0.f, 0.f);
+        }
+    }
+}
+
 // Initialisation per segment: r = rhs - q (q optional), p = P^2 r,
 // rq = Re<r, p>; set_rq0 also records rq0 and clears the iteration state
 // (cgSolver.h:219-288).
@@ -527,6 +791,52 @@ static void cg_iteration(CgSolver &cg, cudaStream_t st, double *hist, bool first
     GB_CUDA(cudaGetLastError());
 }
 
+// Iteration with the fused tail: the padded p is already in the pad buffer
+// (written by the previous iteration's tail, or by the solve's first pad).
+static void cg_iteration_fused(CgSolver &cg, cudaStream_t st, double *hist, bool last) {
+    SenseOp &s = *cg.E;
+    NufftPlan &p = s.plan;
+    const int nb = s.ncoils;
+    const int64_t nbf = (int64_t)nb * p.F;
+    const KLayout kl = ws_layout(p, nbf);
+    float2 *pad = p.img_os.get();
+    float2 *kg = ensure_kgrid(p, nbf);
+    float2 *samp = ensure_samp(p, nb);
+    fft_forward_ws(p, pad, kg, (int)nbf, CUFFT_FORWARD, true, st);
+    launch_degrid(p, kg, samp, nb, LAYOUT_SORTED, s.dcw, 2, true, false, st, &kl);
+    launch_grid(p, samp, kg, nb, LAYOUT_SORTED, nullptr, true, false, st, &kl);
+    fft_adjoint_ws(p, kg, (int)nbf, CUFFT_INVERSE, true, st);
+    TailArgs ta{};
+    ta.k = p.kp;
+    ta.kl = kl;
+    ta.deap = p.deap_img.get();
+    ta.deap_stride = p.maxN;
+    ta.scale = (float)(1.0 / std::sqrt((double)p.kp.G));
+    ta.kg = kg;
+    ta.csm = s.csm;
+    ta.nb = nb;
+    ta.F = (int)p.F;
+    ta.x = cg.x.get();
+    ta.r = cg.r.get();
+    ta.p = cg.p.get();
+    ta.q = cg.q.get();
+    ta.P = cg.precond;
+    ta.weight = cg.weight;
+    ta.kappa = cg.kappa;
+    ta.segs = cg.segs.get();
+    ta.G = cg.G.get();
+    ta.part1 = cg.partials.get();
+    ta.part2 = cg.partials2.get();
+    ta.hist = hist;
+    ta.bar = cg.tail_bar.get();
+    ta.err = p.err_flag.get();
+    ta.pad = last ? nullptr : pad;
+    ta.seg_rows = (int)(cg.seg_len / p.kp.N[0]);
+    void *args[] = {&ta};
+    GB_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg_tail, cg.tail_grid, dim3(256), args, 0, st));
+    ::gb::note_launch();
+}
+
 // Applies E^H E (with weight and kappa) to `in` into `out` without the dot.
 static void cg_apply_normal(CgSolver &cg, const float2 *in, float2 *out, cudaStream_t st) {
     SenseOp &s = *cg.E;
@@ -549,6 +859,15 @@ static void cg_solve_once(CgSolver &cg, const float2 *rhs, const float2 *x0, dou
                                                 cg.partials.get(), 0, (double)cg.tol, hist_base); ::gb::note_launch();
         GB_CUDA(cudaGetLastError());
     }
+    if (cg.use_tail && cg.iterations > 0) {
+        SenseOp &s = *cg.E;
+        const int64_t nbf = (int64_t)s.ncoils * p.F;
+        const KLayout kl = ws_layout(p, nbf);
+        float2 *pad = ensure_img_os(p, nbf, st);
+        launch_pad_forward(p, cg.p.get(), s.csm, pad, s.ncoils, false, st, &kl);
+        for (uint32_t it = 0; it < cg.iterations; it++) cg_iteration_fused(cg, st, hist, it + 1 == cg.iterations);
+        return;
+    }
     for (uint32_t it = 0; it < cg.iterations; it++) cg_iteration(cg, st, hist, it == 0);
 }
 
@@ -567,6 +886,28 @@ static void cg_prepare(CgSolver &cg, cudaStream_t st) {
     cg.seg_len = n / cg.nseg;
     const dim3 sg = seg_grid(cg);
     cg.partials.ensure((size_t)sg.x * sg.y);
+    cg.partials2.ensure((size_t)sg.x * sg.y);
+    if (cg.tail_bar.ensure(2)) GB_CUDA(cudaMemsetAsync(cg.tail_bar.get(), 0, 2 * sizeof(unsigned int), st));
+    // The fused iteration tail needs the outer-major pad buffer (D >= 2) and
+    // all of its blocks resident at once (cooperative launch).
+    cg.use_tail = false;
+    if (p.D >= 2 && cg.seg_len % p.kp.N[0] == 0) {
+        int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+        GB_CUDA(cudaGetDevice(&dev));
+        GB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        GB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_tail, 256, 0));
+        // blocks per segment: up to the resident capacity, at most one per image row
+        const int64_t cap = (int64_t)per_sm * nsm;
+        const int64_t seg_rows = cg.seg_len / p.kp.N[0];
+        const int64_t bx = std::min<int64_t>(seg_rows, cap / cg.nseg);
+        cg.use_tail = coop != 0 && bx >= 1;
+        if (cg.use_tail) {
+            cg.tail_grid = dim3((unsigned)bx, (unsigned)cg.nseg);
+            cg.partials.ensure((size_t)bx * cg.nseg);
+            cg.partials2.ensure((size_t)bx * cg.nseg);
+        }
+    }
     if (cg.segs.ensure(cg.nseg)) GB_CUDA(cudaMemsetAsync(cg.segs.get(), 0, cg.segs.n * sizeof(CgSeg), st));
     if (cg.G.ensure(1)) GB_CUDA(cudaMemsetAsync(cg.G.get(), 0, sizeof(CgGlobal), st));
     if (cg.refinements > 1) cg.x64.ensure(n);

@@ -50,7 +50,10 @@ struct CgSolver {
     int64_t seg_len = 0;
 
     DevBuf<float2> x, r, p, q, rhs0, rhs;
-    DevBuf<double2> x64, partials;
+    DevBuf<double2> x64, partials, partials2;
+    DevBuf<unsigned int> tail_bar;   // grid barrier of the fused iteration tail
+    bool use_tail = false;           // fused tail (cooperative launch) available for this shape
+    dim3 tail_grid;                  // its launch grid (blocks per segment, segments)
     DevBuf<CgSeg> segs;
     DevBuf<CgGlobal> G;
     cudaGraphExec_t graph_exec = nullptr;
