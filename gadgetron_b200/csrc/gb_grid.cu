@@ -1034,9 +1034,10 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
         uint32_t j;
         float dw;
     };
+    const bool lane_ok = sl < SPW;   // false only for the 2 spare lanes of coil group 12
     auto load_raw = [&](int bs, Raw &r) {
         const int i = bs + sl;
-        const bool valid = i < it.end;
+        const bool valid = lane_ok && i < it.end;
         const int ic = valid ? i : it.begin;   // a valid row for the loads of idle lanes
 #pragma unroll
         for (int d = 0; d < D; d++) {
@@ -1077,7 +1078,7 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
                     int gx = gx0 + xo;
                     gx = gx < 0 ? gx + k.mos[0] : (gx >= k.mos[0] ? gx - k.mos[0] : gx);
                     float4 *cell = reinterpret_cast<float4 *>(tile_s + ((size_t)row * R0 + xo) * CS);
-                    constexpr int CH = CG < 8 ? CG : 8;   // coils in flight per lane
+                    constexpr int CH = (CG % 8 == 0) ? 8 : 4;   // coils in flight per lane
 #pragma unroll
                     for (int h = 0; h < CG / CH; h++) {
                         float2 v[CH];
@@ -1098,7 +1099,7 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
 
     for (; base < it.end; base += 8 * SPW) {
         const int i = base + sl;
-        const bool valid = i < it.end;
+        const bool valid = lane_ok && i < it.end;
         if (base + 8 * SPW < it.end) load_raw(base + 8 * SPW, nxt);
         int rs[3] = {0, 0, 0}, n[3] = {1, 1, 1};
         float w[3][NT];
@@ -1487,12 +1488,14 @@ static void degrid_table_dispatch(int cg, int nt, bool d3, const ConvArgs &a, di
         switch (cg) {
             case 4: degrid_table_nt<4, true>(nt, a, g, smem, grid, out, st); break;
             case 8: degrid_table_nt<8, true>(nt, a, g, smem, grid, out, st); break;
+            case 12: degrid_table_nt<12, true>(nt, a, g, smem, grid, out, st); break;
             default: degrid_table_nt<16, true>(nt, a, g, smem, grid, out, st); break;
         }
     } else {
         switch (cg) {
             case 4: degrid_table_nt<4, false>(nt, a, g, smem, grid, out, st); break;
             case 8: degrid_table_nt<8, false>(nt, a, g, smem, grid, out, st); break;
+            case 12: degrid_table_nt<12, false>(nt, a, g, smem, grid, out, st); break;
             default: degrid_table_nt<16, false>(nt, a, g, smem, grid, out, st); break;
         }
     }
@@ -1509,7 +1512,13 @@ void launch_degrid(NufftPlan &p, const float2 *grid, float2 *samples, int nb, Sa
                    const float *dcw, int dcw_pow, bool sign_fold, bool accumulate, cudaStream_t st,
                    const KLayout *kl) {
     if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
-    const int cg = degrid_cg(p, nb);
+    int cg = degrid_cg(p, nb);
+    // 12 coils (or a multiple of 12): one group of 12 for the table kernel
+    // instead of a group of 16 with 4 empty coil slots
+    const int nt12 = (int)std::floor(p.W) + 1;
+    if (nb % 12 == 0 && nb % 16 != 0 && cg >= 8 && !(p.flags & GB_FLAG_COMPENSATED) && p.D >= 2 &&
+        nt12 >= 4 && nt12 <= kWMax && degrid_table_smem(p.kp, 12) <= 220 * 1024)
+        cg = 12;
     const int ncg = (nb + cg - 1) / cg;
     ConvArgs a = make_args(p, nb, layout, dcw, dcw_pow, sign_fold, accumulate);
     if (kl) a.kl = *kl;

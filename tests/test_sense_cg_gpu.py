@@ -58,6 +58,21 @@ def test_sense_mult_M_MH(cuda):
     assert rel_l2(xn.cpu().numpy(), orc.mult_MH_M(case["phantom"])) <= PARITY_TOL
 
 
+@pytest.mark.parametrize("coils", [12, 24])
+def test_sense_coil_groups_of_12(cuda, coils):
+    """Coil counts that are multiples of 12 degrid in groups of 12 (no empty
+    coil slots); forward and normal operator against the oracle."""
+    case = sense_case(N=32, spokes=24, samples=64, coils=coils, seed=11)
+    E, orc = make_ops(case, cuda)
+    x = torch.from_numpy(case["phantom"]).to(cuda)
+    y = torch.empty((coils, case["M"]), dtype=torch.complex64, device=cuda)
+    E.mult_M(x, y)
+    assert rel_l2(y.cpu().numpy(), orc.mult_M(case["phantom"])) <= PARITY_TOL
+    xn = torch.empty_like(x)
+    E.mult_MH_M(x, xn)
+    assert rel_l2(xn.cpu().numpy(), orc.mult_MH_M(case["phantom"])) <= PARITY_TOL
+
+
 def test_sense_multiframe(cuda):
     case = sense_case(N=32, spokes=16, samples=64, coils=4, frames=3, seed=2)
     E, orc = make_ops(case, cuda)
