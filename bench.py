@@ -146,6 +146,17 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples), "source": "NVML, 2 ms polling"}
 
 
+def traffic_for(kname):
+    """DRAM bytes (read + write) per launch of the named kernel from the ncu
+    capture summarised in profiles/roofline_traffic.json (same workload, caches
+    flushed before the launch as in the timed loop), or None."""
+    try:
+        t = json.load(open(os.path.join(ROOT, "profiles", "roofline_traffic.json")))
+        return int(t["kernels"][kname.split()[0]]["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
 def reduce_max_over_ranks(vals, device):
     """Element-wise max of a float64 vector over all ranks (timings: the job
     is as slow as its slowest replica).  Identity when not distributed."""
@@ -341,7 +352,7 @@ def run_ours(args, rank, world, local_rank):
                 "includes": "H2D (pinned) of data/trajectory/dcw/csm, preprocess, CG solve, D2H image"},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": hbm_peak,
                      "unit": "GB/s", "frac": round(achieved / hbm_peak, 4), "peak_source": peak_src,
-                     "traffic": None, "algorithmic_bytes": int(kbytes), "ms_per_launch": round(kms, 5),
+                     "traffic": traffic_for(kname), "algorithmic_bytes": int(kbytes), "ms_per_launch": round(kms, 5),
                      "other_kernel_ms": {"grid": round(t_grid, 5), "degrid": round(t_degrid, 5)}},
         "gpu_launches": int(launches),
         "clocks": clocks,

@@ -262,6 +262,21 @@ GB_API gb_status gb_nufft_get_info(gb_nufft_plan plan, int *D, uint64_t *matrix_
     });
 }
 
+GB_API gb_status gb_nufft_device_errors(gb_nufft_plan plan, uint32_t *error_bits, void *stream) {
+    return guarded([&] {
+        if (!plan || !error_bits) fail(GB_ERR_INVALID_ARGUMENT, "NULL argument");
+        NufftPlan &p = *plan->p;
+        DeviceGuard g(p.device);
+        uint32_t bits = 0;
+        if (p.err_flag.get()) {
+            GB_CUDA(cudaMemcpyAsync(&bits, p.err_flag.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, S(stream)));
+            GB_CUDA(cudaMemsetAsync(p.err_flag.get(), 0, sizeof(uint32_t), S(stream)));
+            GB_CUDA(cudaStreamSynchronize(S(stream)));
+        }
+        *error_bits = bits;
+    });
+}
+
 GB_API gb_status gb_nufft_autotune(gb_nufft_plan plan, uint32_t num_batches, void *stream) {
     return guarded([&] {
         if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");

@@ -405,10 +405,9 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     k_scale_bin<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, traj, M, d_off.get(), F, pos.get(),
                                                                key.get(), idx.get(), err.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
-    int h_err = 0;
-    GB_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
-    GB_CUDA(cudaStreamSynchronize(st));
-    if (h_err) fail(GB_ERR_TRAJECTORY_RANGE, "trajectory out of range [-1/2, 1/2]");
+    // The range flag is read together with the pair count below (one host
+    // synchronisation); until then out-of-range samples sit in tile 0 and
+    // every kernel in between stays in bounds for any position value.
 
     // Stable sort of samples by home key (frame, tile).
     p.perm.ensure(M);
@@ -437,8 +436,11 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     GB_CUDA(cudaGetLastError());
     exclusive_scan(pcnt.get(), poff.get(), M + 1, p.pp_cub, st);
     uint32_t npairs = 0;
+    int h_err = 0;
     GB_CUDA(cudaMemcpyAsync(&npairs, poff.get() + M, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
     GB_CUDA(cudaStreamSynchronize(st));
+    if (h_err) fail(GB_ERR_TRAJECTORY_RANGE, "trajectory out of range [-1/2, 1/2]");
     p.total_pairs = npairs;
     DevBuf<uint32_t> &pkey = p.pp_pkey, &pval = p.pp_pval, &pkey_sorted = p.pp_pkey_sorted;
     pkey.ensure(npairs);

@@ -134,6 +134,13 @@ class cuNFFT_plan:
         check(lib.gb_nufft_get_tiling(self._h, tile, ctypes.byref(cg)))
         return tuple(tile[: self.D]), cg.value
 
+    def device_errors(self) -> int:
+        """Error bits set on the device by kernels whose bounded waits ran out
+        (0: none); reading clears them."""
+        bits = ctypes.c_uint32()
+        check(lib.gb_nufft_device_errors(self._h, ctypes.byref(bits), _stream()))
+        return bits.value
+
     def autotune(self, num_batches: int = 1):
         """Time candidate tilings on this trajectory and keep the fastest."""
         check(lib.gb_nufft_autotune(self._h, int(num_batches), _stream()))

@@ -197,6 +197,13 @@ GB_API gb_status gb_nufft_get_info(gb_nufft_plan plan, int *D, uint64_t *matrix_
                                    uint64_t *matrix_size_os, float *W,
                                    uint64_t *num_samples_total, uint32_t *num_frames);
 
+/* Device-side error word of the plan: kernels whose bounded waits ran out
+ * (a bulk copy that did not complete, a grid barrier not reached by every
+ * block) set a bit instead of spinning forever.  Synchronises the stream,
+ * writes the word to *error_bits (0: none) and clears it.  No reference
+ * counterpart. */
+GB_API gb_status gb_nufft_device_errors(gb_nufft_plan plan, uint32_t *error_bits, void *stream);
+
 /* Autotuner: on a preprocessed plan, times candidate tile shapes and coil
  * groups for num_batches batches (one gridding + one degridding pass each on
  * this trajectory) and keeps the fastest; the choice is cached per

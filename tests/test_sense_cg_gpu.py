@@ -110,6 +110,8 @@ def test_cg_sense_matches_oracle(cuda, use_graph):
     if use_graph:
         x2 = cg.solve(torch.from_numpy(d.reshape(8, -1)).to(cuda))
         assert torch.equal(x, x2)
+    # no bounded wait (bulk-copy mbarrier, fused-tail grid barrier) ran out
+    assert E.get_plan().device_errors() == 0
 
 
 def test_cg_early_stop_and_x0(cuda):
