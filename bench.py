@@ -615,13 +615,16 @@ def run_batched(args):
     384 samples; 12 coils; alpha 2, W 5.5 (not stated by the workload; chosen);
     15 CG iterations.  Batched: one operator over all frames (uneven sample
     counts), per-frame CG scalars, one CUDA graph for the whole solve.  Plain:
-    one operator + solve per frame, no graph, default tiling."""
+    one operator + solve per frame, no graph, default tiling.
+    --size small (profiling case): the first 16 frames."""
     import torch
     import gadgetron_b200 as gb
     from gadgetron_b200 import synthetic as S
     from gadgetron_b200._lib import lib
     dev = torch.device("cuda:0")
     F, N, mos, W, C, S_per, iters = 64, 192, 384, 5.5, 12, 384, 15
+    if getattr(args, "size", "full") == "small":
+        F = 16
     spokes = S.uneven_frame_spokes(F)
     trajs = [S.radial_golden_angle_2d(s, S_per, profile_offset=sum(spokes[:f])) for f, s in enumerate(spokes)]
     offs = np.cumsum([0] + [t.shape[0] for t in trajs]).tolist()
@@ -683,7 +686,7 @@ def run_batched(args):
     xp = torch.cat(xs, 0)
     err = float((xb - xp).abs().pow(2).sum().sqrt() / xp.abs().pow(2).sum().sqrt())
     return {
-        "metric": "batched CG-SENSE ms/batch (64 uneven frames, 192^2, 12 coils, 15 it)",
+        "metric": "batched CG-SENSE ms/batch (%d uneven frames, 192^2, 12 coils, 15 it)" % F,
         "value": round(ms_b, 3), "unit": "ms/batch", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_b, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "c64 (fp32), fp64 CG reductions", "data": "synthetic",
@@ -766,7 +769,7 @@ def main():
     ap.add_argument("--workload", default="cg-sense-2d",
                     choices=["cg-sense-2d", "nufft-2d", "nufft-3d", "batched", "precision"])
     ap.add_argument("--size", default="full", choices=["full", "small"],
-                    help="nufft-3d only: small = the 64^3 profiling case")
+                    help="profiling cases: nufft-3d small = 64^3; batched small = 16 frames")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

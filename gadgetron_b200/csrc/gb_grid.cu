@@ -1054,43 +1054,43 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
     int base = it.begin + warp * SPW;
     if (base < it.end) load_raw(base, cur);
     {
-        // Region staging through registers: lanes run along x (each load is
-        // a coalesced run of one coil plane), then every lane stores its
-        // cell's CG coils as 16-byte chunks (with padded cells, the chunks
-        // that a warp stores at once fall into different banks).
-        const int XW = R0 > 16 ? 32 : (R0 > 8 ? 16 : 8);   // lanes per row
-        const int RPS = 32 / XW;                          // rows per warp step
-        const int rsub = lane / XW, xl = lane - rsub * XW;
-        const int nrows = R1 * R2;
-        const int gx0 = org0 - k.hw;
+        // Region staging through registers.  Thread e of the CTA takes cells
+        // e, e + kThreads, ... of the region in x-fastest order (every load
+        // instruction is a coalesced run of one coil plane, no idle lanes at
+        // row ends), loads all CG coils of UC cells before storing any (the
+        // loads in flight cover the memory latency), then stores each cell's
+        // coils as 16-byte chunks (with padded cells, the chunks that a warp
+        // stores at once fall into different banks).
+        constexpr int UC = CG <= 4 ? 2 : 1;   // cells in flight per thread
+        const int ncell = R0 * R1 * R2;
+        const int gx0 = org0 - k.hw, gy0 = org1 - k.hw, gz0 = org2 - h2;
         const int64_t pstride = (int64_t)a.F * a.kl.s_bf;
         const float2 *fbase = grid + (int64_t)b0 * pstride + (int64_t)f * a.kl.s_bf;
-        for (int row0 = warp * RPS; row0 < nrows; row0 += 8 * RPS) {
-            const int row = row0 + rsub;
-            if (row < nrows) {
+        for (int e0 = threadIdx.x; e0 < ncell; e0 += UC * kThreads) {
+            float2 v[UC][CG];
+#pragma unroll
+            for (int u = 0; u < UC; u++) {
+                const int e = e0 + u * kThreads;
+                const int row = e / R0, xo = e - row * R0;
                 const int rz = row / R1, ry = row - rz * R1;
-                int gy = org1 - k.hw + ry;
+                int gx = gx0 + xo, gy = gy0 + ry, gz = gz0 + rz;
+                gx = gx < 0 ? gx + k.mos[0] : (gx >= k.mos[0] ? gx - k.mos[0] : gx);
                 gy = gy < 0 ? gy + k.mos[1] : (gy >= k.mos[1] ? gy - k.mos[1] : gy);
-                int gz = org2 - h2 + rz;
                 gz = gz < 0 ? gz + k.mos[2] : (gz >= k.mos[2] ? gz - k.mos[2] : gz);
-                const float2 *src_row = fbase + (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y;
-                for (int xo = xl; xo < R0; xo += XW) {
-                    int gx = gx0 + xo;
-                    gx = gx < 0 ? gx + k.mos[0] : (gx >= k.mos[0] ? gx - k.mos[0] : gx);
-                    float4 *cell = reinterpret_cast<float4 *>(tile_s + ((size_t)row * R0 + xo) * CS);
-                    constexpr int CH = (CG % 8 == 0) ? 8 : 4;   // coils in flight per lane
+                const float2 *src = fbase + (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y + gx;
+                const bool in = e < ncell;
 #pragma unroll
-                    for (int h = 0; h < CG / CH; h++) {
-                        float2 v[CH];
+                for (int c = 0; c < CG; c++)
+                    v[u][c] = (in && b0 + c < a.nb) ? __ldg(src + c * pstride) : make_float2(0.f, 0.f);
+            }
 #pragma unroll
-                        for (int c = 0; c < CH; c++) {
-                            const int cc = h * CH + c;
-                            v[c] = (b0 + cc < a.nb) ? __ldg(src_row + cc * pstride + gx) : make_float2(0.f, 0.f);
-                        }
+            for (int u = 0; u < UC; u++) {
+                const int e = e0 + u * kThreads;
+                if (e < ncell) {
+                    float4 *cell = reinterpret_cast<float4 *>(tile_s + (size_t)e * CS);
 #pragma unroll
-                        for (int q = 0; q < CH / 2; q++)
-                            cell[h * CH / 2 + q] = make_float4(v[2 * q].x, v[2 * q].y, v[2 * q + 1].x, v[2 * q + 1].y);
-                    }
+                    for (int q = 0; q < CG / 2; q++)
+                        cell[q] = make_float4(v[u][2 * q].x, v[u][2 * q].y, v[u][2 * q + 1].x, v[u][2 * q + 1].y);
                 }
             }
         }
