@@ -254,6 +254,7 @@ struct NufftPlan {
     DevBuf<float2> samp_ws;   // samples in tile order [batches][Mtot]
     std::map<int, cufftHandle> fft_plans;   // batch -> plan (standard layout, rank D)
     std::map<std::pair<int, int>, cufftHandle> fft_plans_om;   // (batch, pass) -> plan (outer-major)
+    std::map<int, DevBuf<float2>> fft_tw;   // transform length -> W_N^e table (project-written passes)
 
     ~NufftPlan();
 };
@@ -275,6 +276,20 @@ enum FftPass { FFT_PASS_A_BAND = 0, FFT_PASS_A_FULL = 1, FFT_PASS_B = 2 };
 cufftHandle plan_fft_om(NufftPlan &p, int nbf, FftPass pass, cudaStream_t st);
 // Element offset of the band start for FFT_PASS_A_BAND.
 int64_t fft_band_offset(const NufftPlan &p, int nbf);
+
+// Project-written FFT passes (gb_fft.cu), used instead of cuFFT for D >= 2
+// when every oversampled size is 16 * n2 with n2 in {2, 4, 6, 8, 10, 12, 16,
+// 20, 24, 32, 40}.  fft_cols: `ncols` columns (col / cpp = plane at
+// plane * pstride, col % cpp = offset), points at o * ostride.  fft_rows:
+// `nrows` rows of n contiguous points (row r at (r / rpp) * pstride +
+// (row_off + r % rpp) * n).  Input points outside [in_lo, in_hi) are taken as
+// zero without being read; only points in [out_lo, out_hi) are written.
+bool fft_custom_ok(const NufftPlan &p);
+void fft_custom_prepare(NufftPlan &p, cudaStream_t st);
+void fft_cols(NufftPlan &p, int n, const float2 *in, float2 *out, int64_t ncols, int64_t cpp, int64_t pstride,
+              int64_t ostride, int in_lo, int in_hi, int out_lo, int out_hi, bool inverse, cudaStream_t st);
+void fft_rows(NufftPlan &p, int n, const float2 *in, float2 *out, int64_t nrows, int64_t rpp, int64_t row_off,
+              int64_t pstride, int in_lo, int in_hi, int out_lo, int out_hi, bool inverse, cudaStream_t st);
 void plan_set_tiling(NufftPlan &p, const int *tile, int cg);
 // Hash of every buffer address and count the convolution kernels' launches
 // depend on: equal signatures mean a captured graph is still valid.

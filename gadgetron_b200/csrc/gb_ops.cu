@@ -63,6 +63,63 @@ KLayout ws_layout(const NufftPlan &p, int64_t nbf) {
     return p.D >= 2 ? klayout_outer(p.kp, nbf) : klayout_standard(p.kp);
 }
 
+// Project-written passes (fft_custom_ok).  Forward: the padded image is
+// nonzero only inside the centred N box (band_only), so every pass reads only
+// the box's extent along its axis; the outer pass writes `kg`.  2D: x pass
+// over the band rows, y pass.  3D: x pass over the band rows of the band
+// slices, y pass within the band slices, z pass.
+static void fft_forward_custom(NufftPlan &p, float2 *pad, float2 *kg, int64_t nbf, bool inverse, bool band_only,
+                               cudaStream_t st) {
+    const KParams &k = p.kp;
+    const int m0 = k.mos[0], m1 = k.mos[1];
+    const int x0 = band_only ? (m0 - k.N[0]) / 2 : 0, nx = band_only ? k.N[0] : m0;
+    const int y0 = band_only ? (m1 - k.N[1]) / 2 : 0, ny = band_only ? k.N[1] : m1;
+    if (p.D == 2) {
+        const int64_t ncols = nbf * m0;
+        float2 *band = pad + (int64_t)y0 * ncols;   // rows y0 .. y0+ny of every batch are contiguous
+        fft_rows(p, m0, band, band, (int64_t)ny * nbf, (int64_t)ny * nbf, 0, 0, x0, x0 + nx, 0, m0, inverse, st);
+        fft_cols(p, m1, pad, kg, ncols, ncols, 0, ncols, y0, y0 + ny, 0, m1, inverse, st);
+        return;
+    }
+    const int m2 = k.mos[2];
+    const int z0 = band_only ? (m2 - k.N[2]) / 2 : 0, nz = band_only ? k.N[2] : m2;
+    const int64_t plane = (int64_t)m1 * m0;
+    const int64_t ncols = nbf * plane;
+    float2 *band = pad + (int64_t)z0 * ncols;       // slices z0 .. z0+nz of every batch
+    const int64_t nsl = (int64_t)nz * nbf;
+    fft_rows(p, m0, band, band, nsl * ny, ny, y0, plane, x0, x0 + nx, 0, m0, inverse, st);
+    fft_cols(p, m1, band, band, nsl * m0, m0, plane, m0, y0, y0 + ny, 0, m1, inverse, st);
+    fft_cols(p, m2, pad, kg, ncols, ncols, 0, ncols, z0, z0 + nz, 0, m2, inverse, st);
+}
+
+// Adjoint direction in place on `kg`: the crop reads only the centred N box
+// (band_only), so every pass writes only the box's extent along its axis.
+// 2D: y pass, x pass over the band rows.  3D: z pass, y pass within the band
+// slices, x pass over the band rows of the band slices.
+static void fft_adjoint_custom(NufftPlan &p, float2 *kg, int64_t nbf, bool inverse, bool band_only,
+                               cudaStream_t st) {
+    const KParams &k = p.kp;
+    const int m0 = k.mos[0], m1 = k.mos[1];
+    const int x0 = band_only ? (m0 - k.N[0]) / 2 : 0, nx = band_only ? k.N[0] : m0;
+    const int y0 = band_only ? (m1 - k.N[1]) / 2 : 0, ny = band_only ? k.N[1] : m1;
+    if (p.D == 2) {
+        const int64_t ncols = nbf * m0;
+        fft_cols(p, m1, kg, kg, ncols, ncols, 0, ncols, 0, m1, y0, y0 + ny, inverse, st);
+        float2 *band = kg + (int64_t)y0 * ncols;
+        fft_rows(p, m0, band, band, (int64_t)ny * nbf, (int64_t)ny * nbf, 0, 0, 0, m0, x0, x0 + nx, inverse, st);
+        return;
+    }
+    const int m2 = k.mos[2];
+    const int z0 = band_only ? (m2 - k.N[2]) / 2 : 0, nz = band_only ? k.N[2] : m2;
+    const int64_t plane = (int64_t)m1 * m0;
+    const int64_t ncols = nbf * plane;
+    fft_cols(p, m2, kg, kg, ncols, ncols, 0, ncols, 0, m2, z0, z0 + nz, inverse, st);
+    float2 *band = kg + (int64_t)z0 * ncols;
+    const int64_t nsl = (int64_t)nz * nbf;
+    fft_cols(p, m1, band, band, nsl * m0, m0, plane, m0, 0, m1, y0, y0 + ny, inverse, st);
+    fft_rows(p, m0, band, band, nsl * ny, ny, y0, plane, 0, m0, x0, x0 + nx, inverse, st);
+}
+
 // Forward FFT of the padded workspace `pad` into `kg`.  D >= 2: the inner
 // pass runs in place over the interior band only (band_only; every other
 // row/slice of `pad` is zero), then the outer pass writes `kg`.  D == 1: one
@@ -71,6 +128,10 @@ static void fft_forward_ws(NufftPlan &p, float2 *pad, float2 *kg, int nbf, int d
                            cudaStream_t st) {
     if (p.D < 2) {
         exec_fft(p, pad, kg, nbf, dir, st);
+        return;
+    }
+    if (fft_custom_ok(p)) {
+        fft_forward_custom(p, pad, kg, nbf, dir == CUFFT_INVERSE, band_only, st);
         return;
     }
     if (band_only) {
@@ -88,6 +149,10 @@ static void fft_forward_ws(NufftPlan &p, float2 *pad, float2 *kg, int nbf, int d
 static void fft_adjoint_ws(NufftPlan &p, float2 *kg, int nbf, int dir, bool band_only, cudaStream_t st) {
     if (p.D < 2) {
         exec_fft(p, kg, kg, nbf, dir, st);
+        return;
+    }
+    if (fft_custom_ok(p)) {
+        fft_adjoint_custom(p, kg, nbf, dir == CUFFT_INVERSE, band_only, st);
         return;
     }
     exec_pass(p, FFT_PASS_B, kg, kg, nbf, dir, st);
@@ -916,7 +981,9 @@ static void cg_prepare(CgSolver &cg, cudaStream_t st) {
     ensure_kgrid(p, (int64_t)nb * p.F);
     ensure_samp(p, nb);
     plan_fft(p, nb * (int)p.F, st);
-    if (p.D >= 2)   // plans are made outside stream capture
+    if (p.D >= 2 && fft_custom_ok(p))   // twiddle tables are made outside stream capture
+        fft_custom_prepare(p, st);
+    else if (p.D >= 2)                  // and so are cuFFT plans
         for (FftPass pass : {FFT_PASS_A_BAND, FFT_PASS_A_FULL, FFT_PASS_B}) plan_fft_om(p, nb * (int)p.F, pass, st);
     // Split-tile counters/partials for the gridding kernel.
     launch_grid_prepare(p, nb, st);

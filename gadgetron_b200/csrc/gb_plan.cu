@@ -478,6 +478,7 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     p.prepped_c2nc = p.prepped_nc2c = true;
     p.prep_mode = mode;
     plan_build_work(p, st);
+    fft_custom_prepare(p, st);
     p.prepped = true;
 }
 

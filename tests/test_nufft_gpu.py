@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 import torch
 
+from gadgetron_b200 import synthetic as S
 from oracle import oracle as O
 from tests.helpers import PARITY_TOL, kooshball_case, radial_case, rel_l2
 
@@ -154,6 +155,55 @@ def test_3d_forward_adjoint(cuda):
     back = torch.empty_like(x)
     plan.compute(y, back, dcw, gb.NFFT_comp_mode.BACKWARDS_NC2C)
     ref2 = orc.backwards_nc2c(ref, case["dcw"].reshape(1, -1))
+    assert rel_l2(back.cpu().numpy(), ref2) <= PARITY_TOL
+
+
+# Oversampled sizes covering every transform length of the project-written
+# FFT passes (16 * n2, n2 in 2, 4, 6, 8, 10, 12, 16, 20, 24, 32, 40) on
+# non-square grids, and one size they do not cover (224 = 16 * 14: the plan
+# then uses cuFFT for every pass).
+@pytest.mark.parametrize("N,mos", [((32, 64), (96, 160)), ((64, 32), (320, 64)), ((32, 32), (224, 128)),
+                                   ((64, 64), (384, 640)), ((32, 96), (128, 192)), ((128, 32), (256, 32)),
+                                   ((64, 128), (512, 256))])
+def test_fft_lengths_2d(cuda, N, mos):
+    W, batches = 4.0, 2
+    traj = S.radial_golden_angle_2d(24, 96)
+    dcw = S.ramp_dcw(traj)
+    img = S.gaussian_image((batches, 1, N[1], N[0]), 31)
+    dev = torch.device("cuda:0")
+    plan = gb.NFFT.make_plan(N, mos, W)
+    plan.preprocess(torch.from_numpy(traj).to(dev), gb.NFFT_prep_mode.ALL)
+    orc = O.OraclePlan(N, mos, W)
+    orc.preprocess(traj.reshape(1, -1, 2))
+    x = torch.from_numpy(img).to(dev)
+    y = torch.empty((batches, traj.shape[0]), dtype=torch.complex64, device=dev)
+    plan.compute(x, y, torch.from_numpy(dcw).to(dev), gb.NFFT_comp_mode.FORWARDS_C2NC)
+    ref = orc.forward_c2nc(img, dcw.reshape(1, -1))
+    assert rel_l2(y.cpu().numpy(), ref) <= PARITY_TOL
+    back = torch.empty_like(x)
+    plan.compute(y, back, torch.from_numpy(dcw).to(dev), gb.NFFT_comp_mode.BACKWARDS_NC2C)
+    ref2 = orc.backwards_nc2c(ref, dcw.reshape(1, -1))
+    assert rel_l2(back.cpu().numpy(), ref2) <= PARITY_TOL
+
+
+def test_fft_lengths_3d(cuda):
+    N, mos, W = (32, 32, 32), (64, 96, 160), 4.0
+    traj = S.kooshball_golden_means_3d(150, 48)
+    dcw = S.ramp_dcw(traj)
+    img = S.gaussian_image((2, 1, 32, 32, 32), 32)
+    dev = torch.device("cuda:0")
+    plan = gb.NFFT.make_plan(N, mos, W)
+    plan.preprocess(torch.from_numpy(traj).to(dev), gb.NFFT_prep_mode.ALL)
+    orc = O.OraclePlan(N, mos, W)
+    orc.preprocess(traj.reshape(1, -1, 3))
+    x = torch.from_numpy(img).to(dev)
+    y = torch.empty((2, traj.shape[0]), dtype=torch.complex64, device=dev)
+    plan.compute(x, y, torch.from_numpy(dcw).to(dev), gb.NFFT_comp_mode.FORWARDS_C2NC)
+    ref = orc.forward_c2nc(img, dcw.reshape(1, -1))
+    assert rel_l2(y.cpu().numpy(), ref) <= PARITY_TOL
+    back = torch.empty_like(x)
+    plan.compute(y, back, torch.from_numpy(dcw).to(dev), gb.NFFT_comp_mode.BACKWARDS_NC2C)
+    ref2 = orc.backwards_nc2c(ref, dcw.reshape(1, -1))
     assert rel_l2(back.cpu().numpy(), ref2) <= PARITY_TOL
 
 
