@@ -317,7 +317,9 @@ void launch_pad_forward(NufftPlan &p, const float2 *src, const float2 *csm, floa
         k_pad_forward_os<<<grid_for(nbf * p.kp.G), 256, 0, st>>>(a, src, dst, nbf); ::gb::note_launch();
     } else {
         ImgArgs a = img_args(p, false, kl);
-        a.full_lines = (kl != nullptr && p.D >= 2) ? 1 : 0;   // outer-major workspace: whole band lines
+        // outer-major workspace under cuFFT passes: whole band lines (the
+        // project-written passes read only the interior)
+        a.full_lines = (kl != nullptr && p.D >= 2 && !fft_custom_ok(p)) ? 1 : 0;
         const int64_t lines = (int64_t)p.F * p.kp.N[2] * ((a.full_lines && p.D == 3) ? p.kp.mos[1] : p.kp.N[1]);
         const int width = a.full_lines ? p.kp.mos[0] : p.kp.N[0];
         k_pad_forward<<<rows_grid(lines, width), 256, 0, st>>>(a, src, csm, dst, nb, (int)p.F, pun); ::gb::note_launch();

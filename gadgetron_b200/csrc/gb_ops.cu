@@ -509,6 +509,7 @@ struct TailArgs {
     unsigned int *bar;       // grid barrier: arrival count, generation
     unsigned int *err;
     float2 *pad;             // next iteration's padded image (outer-major), or null after the last iteration
+    int pad_full;            // 1: whole band lines with their zeros (a cuFFT pass follows); 0: interior only
     int seg_rows;            // image rows (of N0 pixels) per segment
 };
 
@@ -696,7 +697,9 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
         const int64_t gline = (int64_t)gz * t.kl.s_z + (int64_t)gy * t.kl.s_y;
         const int64_t nrow = (int64_t)rem * k.N[0];
         const int64_t erow = (int64_t)(row0 + rr) * k.N[0];
-        for (int gx = threadIdx.x; gx < k.mos[0]; gx += blockDim.x) {
+        // interior only when the FFT passes read nothing else
+        const int gx0 = t.pad_full ? 0 : ox, gx1 = t.pad_full ? k.mos[0] : ox + k.N[0];
+        for (int gx = gx0 + threadIdx.x; gx < gx1; gx += blockDim.x) {
             const int x = gx - ox;
             const bool in = x >= 0 && x < k.N[0];
             float fac = 0.f;
@@ -721,7 +724,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
             }
         }
     }
-    if (k.D == 3) {
+    if (k.D == 3 && t.pad_full) {
         // rows of the band slices outside the interior rows: zero (the band
         // FFT pass overwrote them)
         const int zrows = k.mos[1] - k.N[1];
@@ -896,6 +899,7 @@ static void cg_iteration_fused(CgSolver &cg, cudaStream_t st, double *hist, bool
     ta.bar = cg.tail_bar.get();
     ta.err = p.err_flag.get();
     ta.pad = last ? nullptr : pad;
+    ta.pad_full = fft_custom_ok(p) ? 0 : 1;
     ta.seg_rows = (int)(cg.seg_len / p.kp.N[0]);
     void *args[] = {&ta};
     GB_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg_tail, cg.tail_grid, dim3(256), args, 0, st));
