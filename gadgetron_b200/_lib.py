@@ -87,6 +87,9 @@ def _load():
         "gb_cg_set_x0": (i32, [P, P]),
         "gb_cg_set_preconditioner": (i32, [P, P]),
         "gb_cg_set_identity_regularization": (i32, [P, f32]),
+        "gb_cg_set_image_regularization": (i32, [P, P, f32]),
+        "gb_image_operator_compute": (i32, [P, u64, i32, P, P, P]),
+        "gb_sense_precond_weights": (i32, [P, P, f32, P, P]),
         "gb_cg_set_refinements": (i32, [P, u32]),
         "gb_cg_set_use_graph": (i32, [P, i32]),
         "gb_cg_set_frame_independent": (i32, [P, i32]),
@@ -108,7 +111,8 @@ EXPORTED = (
     "gb_sense_set_dcw gb_sense_mult_M gb_sense_mult_MH gb_sense_mult_MH_M gb_sense_get_nufft_plan gb_sense_autotune "
     "gb_cg_create gb_cg_destroy gb_cg_set_encoding_operator gb_cg_set_max_iterations "
     "gb_cg_set_tc_tolerance gb_cg_set_x0 gb_cg_set_preconditioner gb_cg_set_identity_regularization "
-    "gb_cg_set_refinements gb_cg_set_use_graph gb_cg_set_frame_independent gb_cg_solve").split()
+    "gb_cg_set_refinements gb_cg_set_use_graph gb_cg_set_frame_independent gb_cg_solve "
+    "gb_cg_set_image_regularization gb_image_operator_compute gb_sense_precond_weights").split()
 
 
 def check(status: int):

@@ -467,6 +467,35 @@ GB_API gb_status gb_cg_set_identity_regularization(gb_cg_solver solver, float ka
     return guarded([&] {
         if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
         solver->c.kappa = kappa;
+        solver->c.reg = nullptr;
+    });
+}
+
+GB_API gb_status gb_cg_set_image_regularization(gb_cg_solver solver, const float *image, float kappa) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
+        if (!image && kappa != 0.f) fail(GB_ERR_INVALID_ARGUMENT, "NULL regularisation image");
+        solver->c.kappa = kappa;
+        solver->c.reg = image;
+    });
+}
+
+GB_API gb_status gb_image_operator_compute(const void *reg_image, uint64_t n, int offset_estimation,
+                                           float *image, float *offset, void *stream) {
+    return guarded([&] {
+        if (!reg_image || !image || n == 0) fail(GB_ERR_INVALID_ARGUMENT, "invalid image operator arguments");
+        const float off = image_operator_compute(static_cast<const float2 *>(reg_image), (int64_t)n,
+                                                 offset_estimation != 0, image, S(stream));
+        if (offset) *offset = off;
+    });
+}
+
+GB_API gb_status gb_sense_precond_weights(gb_sense_op op, const float *reg_image, float kappa, float *weights,
+                                          void *stream) {
+    return guarded([&] {
+        if (!op || !weights) fail(GB_ERR_INVALID_ARGUMENT, "NULL operator or weights");
+        if (!op->s.csm || op->s.ncoils <= 0) fail(GB_ERR_INVALID_ARGUMENT, "set_csm before the preconditioner");
+        sense_precond_weights(op->s.csm, op->s.ncoils, op->s.plan.kp.NN, reg_image, kappa, weights, S(stream));
     });
 }
 

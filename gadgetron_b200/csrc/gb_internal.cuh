@@ -422,4 +422,12 @@ __host__ __device__ __forceinline__ int wrapmod(int x, int m) {
     return r < 0 ? r + m : r;
 }
 
+// Image regulariser and preconditioner weights (gb_reg.cu).  Returns the
+// offset; image receives 1 / (|reg n / asum(reg)| + offset).
+float image_operator_compute(const float2 *reg, int64_t n, bool offset_estimation, float *image,
+                             cudaStream_t st);
+// w = 1 / sqrt(sum_c |csm_c|^2 + kappa * reg) over nn pixels (reg may be null).
+void sense_precond_weights(const float2 *csm, int nb, int64_t nn, const float *reg, float kappa, float *w,
+                           cudaStream_t st);
+
 }  // namespace gb

@@ -359,11 +359,19 @@ __device__ bool last_block_sum(double2 mine, double2 *partials, unsigned int *ct
     return true;
 }
 
-// q = weight * crop(...) + kappa * p, then <p, q> per segment -> alpha = rq / <p, q>.
+// kappa R^H R p for the regulariser R = diag(reg) (reg null: R = I), as
+// imageOperator::mult_MH_M forms it: (p * reg) * reg.
+__device__ __forceinline__ float2 reg_term(float2 pv, const float *reg, int64_t e) {
+    if (!reg) return pv;
+    const float w = reg[e];
+    return make_float2((pv.x * w) * w, (pv.y * w) * w);
+}
+
+// q = weight * crop(...) + kappa * R^H R p, then <p, q> per segment -> alpha = rq / <p, q>.
 __global__ void k_cg_crop_dot(KParams k, KLayout kl, const float *deap, int deap_stride, float scale,
                               const float2 *__restrict__ grid, const float2 *__restrict__ csm, int nb, int F,
                               const float2 *__restrict__ p, float2 *__restrict__ q, float weight, float kappa,
-                              CgSeg *segs, int64_t seg_len, double2 *partials) {
+                              const float *__restrict__ reg, CgSeg *segs, int64_t seg_len, double2 *partials) {
     CgSeg &S = segs[blockIdx.y];
     if (S.done) return;
     const int ox = (k.mos[0] - k.N[0]) >> 1, oy = (k.mos[1] - k.N[1]) >> 1, oz = (k.mos[2] - k.N[2]) >> 1;
@@ -401,8 +409,9 @@ __global__ void k_cg_crop_dot(KParams k, KLayout kl, const float *deap, int deap
                 s.y += vi * c.x - vr * c.y;
             }
             const float2 pv = p[e];
-            s.x += kappa * pv.x;
-            s.y += kappa * pv.y;
+            const float2 rp = reg_term(pv, reg, e);
+            s.x += kappa * rp.x;
+            s.y += kappa * rp.y;
             q[e] = s;
             // conj(p) * q
             acc.x += (double)pv.x * s.x + (double)pv.y * s.y;
@@ -502,6 +511,7 @@ struct TailArgs {
     float2 *x, *r, *p, *q;
     const float *P;
     float weight, kappa;
+    const float *reg;        // image regulariser diagonal (null: identity)
     CgSeg *segs;
     CgGlobal *G;
     double2 *part1, *part2;  // [nseg][gridDim.x]
@@ -604,8 +614,9 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
                     s.y += vi * c.x - vr * c.y;
                 }
                 const float2 pv = t.p[e];
-                s.x += t.kappa * pv.x;
-                s.y += t.kappa * pv.y;
+                const float2 rp = reg_term(pv, t.reg, e);
+                s.x += t.kappa * rp.x;
+                s.y += t.kappa * rp.y;
                 t.q[e] = s;
                 acc.x += (double)pv.x * s.x + (double)pv.y * s.y;
                 acc.y += (double)pv.x * s.y - (double)pv.y * s.x;
@@ -843,7 +854,8 @@ static void cg_normal_dot(CgSolver &cg, cudaStream_t st, bool update_p) {
     fft_adjoint_ws(p, kg, (int)nbf, CUFFT_INVERSE, true, st);
     k_cg_crop_dot<<<seg_grid(cg), 256, 0, st>>>(p.kp, kl, p.deap_img.get(), p.maxN,
                                                 (float)(1.0 / std::sqrt((double)p.kp.G)), kg, s.csm, nb,
-                                                (int)p.F, cg.p.get(), cg.q.get(), cg.weight, cg.kappa, cg.segs.get(),
+                                                (int)p.F, cg.p.get(), cg.q.get(), cg.weight, cg.kappa,
+                                                cg.kappa != 0.f ? cg.reg : nullptr, cg.segs.get(),
                                                 cg.seg_len, cg.partials.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
 }
@@ -891,6 +903,7 @@ static void cg_iteration_fused(CgSolver &cg, cudaStream_t st, double *hist, bool
     ta.P = cg.precond;
     ta.weight = cg.weight;
     ta.kappa = cg.kappa;
+    ta.reg = cg.kappa != 0.f ? cg.reg : nullptr;
     ta.segs = cg.segs.get();
     ta.G = cg.G.get();
     ta.part1 = cg.partials.get();
@@ -1028,7 +1041,7 @@ void cg_solve(CgSolver &cg, const void *d, void *x_out, double *hist, uint32_t *
     if (!s.csm) fail(GB_ERR_INVALID_ARGUMENT, "csm not set");
     if (!s.plan.prepped) fail(GB_ERR_NOT_PREPROCESSED, "operator not preprocessed");
     if (cg.kappa != 0.f && (cg.refinements > 1 || cg.x0))
-        fail(GB_ERR_INVALID_ARGUMENT, "identity regularisation cannot be combined with x0 or refinement");
+        fail(GB_ERR_INVALID_ARGUMENT, "regularisation cannot be combined with x0 or refinement");
     NufftPlan &p = s.plan;
     const int64_t n = (int64_t)p.F * p.kp.NN;
     const float2 *dd = static_cast<const float2 *>(d);
@@ -1040,7 +1053,7 @@ void cg_solve(CgSolver &cg, const void *d, void *x_out, double *hist, uint32_t *
     }
     cg_prepare(cg, st);
     if (cg.use_graph) {
-        GraphKey key{d, x_out, hist, cg.iterations, cg.refinements, cg.x0, cg.precond, cg.kappa, cg.weight,
+        GraphKey key{d, x_out, hist, cg.iterations, cg.refinements, cg.x0, cg.precond, cg.reg, cg.kappa, cg.weight,
                      cg.tol, s.csm, s.dcw, s.ncoils, plan_layout_signature(s.plan, s.ncoils * (int)s.plan.F),
                      cg.independent_frames};
         if (!cg.graph_exec || !(key == cg.graph_key)) {

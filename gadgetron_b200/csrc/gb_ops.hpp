@@ -19,6 +19,7 @@ struct GraphKey {
     uint32_t iterations, refinements;
     const float2 *x0;
     const float *precond;
+    const float *reg;
     float kappa, weight, tol;
     const float2 *csm;
     const float *dcw;
@@ -27,7 +28,7 @@ struct GraphKey {
     bool independent;
     bool operator==(const GraphKey &o) const {
         return generation == o.generation && independent == o.independent && d == o.d && x == o.x && hist == o.hist && iterations == o.iterations &&
-               refinements == o.refinements && x0 == o.x0 && precond == o.precond && kappa == o.kappa &&
+               refinements == o.refinements && x0 == o.x0 && precond == o.precond && reg == o.reg && kappa == o.kappa &&
                weight == o.weight && tol == o.tol && csm == o.csm && dcw == o.dcw && ncoils == o.ncoils;
     }
 };
@@ -43,6 +44,9 @@ struct CgSolver {
     const float2 *x0 = nullptr;
     const float *precond = nullptr;
     float kappa = 0.f;
+    // Image regulariser R = diag(reg) ([frames][N], null: R = I): the
+    // operator gets kappa * R^H R = kappa * reg^2 (imageOperator::mult_MH_M).
+    const float *reg = nullptr;
     uint32_t refinements = 1;
     bool use_graph = false;
     bool independent_frames = false;   // per-frame CG scalars (frames solved independently)

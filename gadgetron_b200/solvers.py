@@ -28,6 +28,9 @@ class cuCgSolver:
         self.tc_tolerance = 1e-3
         self.x0 = None
         self.precond = None
+        self._precond_src = None
+        self.reg_ops = []
+        self._reg_image = None
         self.refinements = 1
         self.last_iterations = 0
         self.residual_history = None
@@ -61,15 +64,54 @@ class cuCgSolver:
         self.x0 = x0
         check(lib.gb_cg_set_x0(self._h, _ptr(x0)))
 
-    def set_preconditioner(self, weights: Optional[torch.Tensor]):
-        """cgPreconditioner with real diagonal weights (applied twice)."""
+    def _frames_of(self, w: torch.Tensor) -> torch.Tensor:
+        """Diagonal weights over the solution [frames, N...]: weights of one
+        frame are repeated over the frames (the reference broadcasts them)."""
+        E = self.E
+        n = 1
+        for v in E.matrix_size:
+            n *= int(v)
+        F = max(1, int(E.num_frames))
+        if w.numel() == n * F:
+            return w.contiguous()
+        if w.numel() == n:
+            return w.reshape(1, n).repeat(F, 1).contiguous()
+        raise ValueError("diagonal weights must hold N... or N... x frames elements")
+
+    def set_preconditioner(self, weights):
+        """cgSolver::set_preconditioner: a cuCgPreconditioner, or its real
+        diagonal weights directly (applied twice per iteration, as the
+        reference does); None clears."""
+        if weights is not None and hasattr(weights, "get_weights"):
+            weights = weights.get_weights()
         if weights is not None:
             _check_tensor(weights, torch.float32, "weights")
+            if self.E is None:
+                raise RuntimeError("set_encoding_operator before set_preconditioner")
+            weights = self._frames_of(weights)
         self.precond = weights
         check(lib.gb_cg_set_preconditioner(self._h, _ptr(weights)))
 
     def set_identity_regularization(self, kappa: float):
         check(lib.gb_cg_set_identity_regularization(self._h, ctypes.c_float(kappa)))
+
+    def add_regularization_operator(self, R):
+        """cgSolver::add_regularization_operator (linearOperatorSolver.h:38-41)
+        for a cuImageOperator: adds R.get_weight() * R^H R to E^H E.  One
+        regularisation operator per solver."""
+        if self.reg_ops:
+            raise RuntimeError("one regularisation operator per solver is supported")
+        if self.E is None:
+            raise RuntimeError("set_encoding_operator before add_regularization_operator")
+        img = self._frames_of(R.get())
+        self.reg_ops.append(R)
+        self._reg_image = img
+        check(lib.gb_cg_set_image_regularization(self._h, _ptr(img), ctypes.c_float(R.get_weight())))
+
+    def clear_regularization_operators(self):
+        self.reg_ops = []
+        self._reg_image = None
+        check(lib.gb_cg_set_identity_regularization(self._h, ctypes.c_float(0.0)))
 
     def set_refinements(self, n: int):
         self.refinements = int(n)

@@ -282,9 +282,29 @@ GB_API gb_status gb_cg_set_x0(gb_cg_solver solver, const void *x0);
  * real diagonal weights [N..., frames] (applied twice, as the reference does);
  * NULL clears.  Retained pointer. */
 GB_API gb_status gb_cg_set_preconditioner(gb_cg_solver solver, const float *weights);
-/* Kappa-weighted identity regulariser R = I (a stand-in for an image
- * regulariser with R^H R = I): adds kappa * x to E^H E x.  0 disables. */
+/* Kappa-weighted identity regulariser R = I: adds kappa * x to E^H E x
+ * (cgSolver::add_regularization_operator with an identityOperator,
+ * cgSolver.h:355-390).  0 disables. */
 GB_API gb_status gb_cg_set_identity_regularization(gb_cg_solver solver, float kappa);
+/* cgSolver::add_regularization_operator(R) with R a cuImageOperator of weight
+ * kappa (gadgets/pmri/gpuCgSenseGadget.cpp:71-76; cgSolver.h:380-389;
+ * imageOperator::mult_MH_M, imageOperator.h:48-67): adds
+ * kappa * image^2 * x to E^H E x.  image: device floats [N..., frames] as made
+ * by gb_image_operator_compute (retained pointer); kappa 0 disables. */
+GB_API gb_status gb_cg_set_image_regularization(gb_cg_solver solver, const float *image, float kappa);
+/* imageOperator::compute(reg_image, offset_estimation) with
+ * cuImageOperator::estimate_offset (toolboxes/operators/imageOperator.h:27-45,
+ * toolboxes/operators/gpu/cuImageOperator.h:35-62): image[i] =
+ * 1 / (|reg[i] * n / asum(reg)| + offset), offset from the 1st percentile of
+ * a 50000-bin histogram (0 without estimation).  reg: n complex64 (device);
+ * image: n floats (device); offset: host float or NULL.  Synchronises. */
+GB_API gb_status gb_image_operator_compute(const void *reg_image, uint64_t n, int offset_estimation,
+                                           float *image, float *offset, void *stream);
+/* Preconditioner weights of gpuCgSenseGadget.cpp:167-176:
+ * w = 1 / sqrt(sum_c |csm_c|^2 + kappa * reg_image) over the N... pixels of
+ * the operator (reg_image NULL: csm term only).  weights: device floats. */
+GB_API gb_status gb_sense_precond_weights(gb_sense_op op, const float *reg_image, float kappa,
+                                          float *weights, void *stream);
 /* Outer iterative refinement: solve `refinements` times, each from the FP64
  * residual of the previous solution (x <- x + CG(E^H d - E^H E x)).  1 = off. */
 GB_API gb_status gb_cg_set_refinements(gb_cg_solver solver, uint32_t refinements);

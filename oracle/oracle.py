@@ -30,7 +30,11 @@ cuNonCartesianSenseOperator and cgSolver) on the CPU:
   ``toolboxes/mri/pmri/gpu/cuNonCartesianSenseOperator.cu:14-62`` and
   ``toolboxes/mri/pmri/gpu/sense_utilities.cu:7-123``;
 * the CG solver follows ``toolboxes/solvers/cgSolver.h:105-390`` with the
-  ``relativeResidualTCB`` stop rule of ``toolboxes/solvers/cgCallback.h:56-104``.
+  ``relativeResidualTCB`` stop rule of ``toolboxes/solvers/cgCallback.h:56-104``;
+  regularisation terms w_i R_i^H R_i follow ``cgSolver.h:355-390``;
+* the image regulariser follows ``toolboxes/operators/imageOperator.h:27-67``
+  and its offset estimate ``toolboxes/operators/gpu/cuImageOperator.h:35-62``;
+  the preconditioner weights follow ``gadgets/pmri/gpuCgSenseGadget.cpp:167-176``.
 
 The direct FP64 NDFT (``ndft_forward``/``ndft_adjoint``) is the accuracy
 oracle: y_j = dcw_j / sqrt(G) * sum_n x_n exp(-2 pi i k_j.(n - N/2)), G the
@@ -371,13 +375,70 @@ class OracleSense:
         return self.mult_MH(self.mult_M(x))
 
 
+def image_operator_compute(reg_image: np.ndarray, offset_estimation: bool = True):
+    """imageOperator::compute (imageOperator.h:27-45) with the offset estimate
+    of cuImageOperator::estimate_offset (cuImageOperator.h:35-62), in float32
+    as the reference computes it.  Returns (image, offset): image =
+    1 / (|reg * n / asum(reg)| + offset), asum = sum |re| + |im| (Scasum);
+    offset = (k + 1) * max / 50000 with k the first 50000-bin histogram bin
+    of image / max at which the cumulative count reaches 1% of the elements."""
+    z = np.asarray(reg_image, np.complex64).ravel()
+    n = z.size
+    asum = float(np.sum(np.abs(z.real).astype(np.float64) + np.abs(z.imag).astype(np.float64)))
+    scale = np.float32(np.float32(n) / np.float32(asum))
+    re = (z.real * scale).astype(np.float32)
+    im = (z.imag * scale).astype(np.float32)
+    img = np.sqrt((re * re).astype(np.float32) + (im * im).astype(np.float32)).astype(np.float32)
+    offset = np.float32(0.0)
+    if offset_estimation:
+        gran = 50000
+        mx = np.float32(img.max())
+        bins = np.minimum(np.floor((img / mx) * np.float32(gran)).astype(np.int64), gran - 1)
+        hist = np.bincount(bins, minlength=gran)
+        target = int(np.float32(0.01) * np.float32(n))
+        cumsum, counter = 0, 0
+        while cumsum < target:
+            cumsum += int(hist[counter])
+            counter += 1
+        offset = np.float32(np.float32(counter + 1) * mx / np.float32(gran))
+    if offset > 0:
+        img = (img + offset).astype(np.float32)
+    img = (np.float32(1.0) / img).astype(np.float32)
+    return img.reshape(np.shape(reg_image)), float(offset)
+
+
+def sense_precond_weights(csm: np.ndarray, reg_image=None, kappa: float = 0.0) -> np.ndarray:
+    """Diagonal preconditioner of gpuCgSenseGadget.cpp:167-176:
+    1 / sqrt(sum_c |csm_c|^2 + kappa * R) with R the regularisation image."""
+    w = np.sum(np.abs(np.asarray(csm, np.complex128)) ** 2, axis=0)
+    if reg_image is not None:
+        w = w + kappa * np.asarray(reg_image, np.float64)
+    return 1.0 / np.sqrt(w)
+
+
 def cg_solve(op, d: np.ndarray, iterations: int = 10, tc_tolerance: float = 1e-3,
-             x0=None, precond_weights=None, history=None):
+             x0=None, precond_weights=None, history=None, regularization=None):
     """cgSolver::solve (cgSolver.h:105-390), complex128 throughout.
 
     Unpreconditioned: rq = ||r||^2, alpha = rq / <p, q> (complex, Cdotc),
     p <- p * (rq'/rq) + r.  Stops when rq/rq0 < tc_tolerance
-    (relativeResidualTCB)."""
+    (relativeResidualTCB).  ``regularization``: list of (weight, R) with R
+    a real diagonal (the image regulariser's image, or 1 for the identity);
+    the operator is E^H E + sum weight * R^2 (cgSolver.h:355-390)."""
+    if regularization:
+        base = op
+
+        class _Reg:
+            def mult_MH(self, y):
+                return base.mult_MH(y)
+
+            def mult_MH_M(self, x):
+                out = base.mult_MH_M(x)
+                for w, R in regularization:
+                    R = np.asarray(R, np.float64)
+                    out = out + w * (x * R * R)
+                return out
+        op = _Reg()
     rhs = op.mult_MH(d)
     if iterations == 0:
         return rhs

@@ -205,3 +205,44 @@ def test_oracle_traj_grad_matches_finite_differences():
     idx = np.nonzero(ok)[0]
     assert len(idx) > 0.5 * M
     assert np.linalg.norm(g[idx] - fd[idx]) / np.linalg.norm(fd[idx]) < 1e-3
+
+
+def test_image_operator_known_answer():
+    """imageOperator::compute + cuImageOperator::estimate_offset on a case
+    worked by hand: 99 elements 4 and one element 1 (asum 397)."""
+    z = np.full(100, 4.0, np.complex64)
+    z[37] = 1.0
+    img, off = O.image_operator_compute(z)
+    scale = np.float32(np.float32(100) / np.float32(397.0))
+    a4, a1 = np.float32(np.float32(4.0) * scale), scale
+    # a1 / a4 = 0.25 exactly: bin 12500 of 50000; 1% of 100 elements = 1, so
+    # the cumulative count first reaches 1 after bin 12500: counter = 12501
+    exp_off = np.float32(np.float32(12502) * a4 / np.float32(50000))
+    assert off == float(exp_off)
+    assert img[0] == np.float32(np.float32(1) / np.float32(a4 + exp_off))
+    assert img[37] == np.float32(np.float32(1) / np.float32(a1 + exp_off))
+    img2, off2 = O.image_operator_compute(z, offset_estimation=False)
+    assert off2 == 0.0
+    assert img2[0] == np.float32(np.float32(1) / a4) and img2[37] == np.float32(np.float32(1) / a1)
+
+
+def test_sense_precond_weights_formula():
+    """gpuCgSenseGadget.cpp:167-176: 1 / sqrt(sum_c |csm_c|^2 + kappa R)."""
+    csm = np.array([[[3.0, 0.0]], [[4.0j, 1.0]]], np.complex64)   # 2 coils, 1 x 2 pixels
+    R = np.array([[2.0, 5.0]], np.float32)
+    w = O.sense_precond_weights(csm, R, kappa=0.5)
+    np.testing.assert_allclose(w, 1.0 / np.sqrt(np.array([[9 + 16 + 1.0, 0 + 1 + 2.5]])), rtol=1e-12)
+
+
+def test_cg_regularization_term_is_kappa_R_squared():
+    """cgSolver::mult_MH_M with an image regulariser: E^H E x + kappa R^2 x."""
+    class Eye:
+        def mult_MH(self, y):
+            return y
+
+        def mult_MH_M(self, x):
+            return x
+    d = np.array([1.0 + 1.0j, 2.0, -1.0j])
+    R = np.array([1.0, 2.0, 3.0])
+    x = O.cg_solve(Eye(), d, iterations=5, tc_tolerance=0.0, regularization=[(0.5, R)])
+    np.testing.assert_allclose(x, d / (1.0 + 0.5 * R * R), rtol=1e-12)
