@@ -795,6 +795,16 @@ def run_regularized(args):
         D.set_weights(gb.sense_precond_weights(E, R.get(), kappa))
 
     setup_ms = _timed(setup, args.steps, args.warmup, None, stream)
+    # the gadget's other inputs generated on the device: golden-ratio
+    # trajectory and its Voronoi density compensation (same shape)
+    from gadgetron_b200 import radial as RU
+    gen_ms = _timed(lambda: (RU.compute_radial_trajectory_golden_ratio_2d(CFG["samples"], CFG["spokes"], device=dev),
+                             RU.compute_radial_dcw_golden_ratio_2d(CFG["samples"], CFG["spokes"], 2.0, 0.5,
+                                                                   device=dev)),
+                    args.steps, args.warmup, None, stream)
+    t0 = time.perf_counter()
+    O.radial_dcw_2d(CFG["samples"], CFG["spokes"], 2.0, 0.5)
+    gen_cpu_ms = (time.perf_counter() - t0) * 1e3
     R.set_weight(kappa)
     cg = gb.cuCgSolver()
     cg.set_encoding_operator(E)
@@ -824,6 +834,8 @@ def run_regularized(args):
         "config": {"workload": "cg-sense-2d-regularised", "kappa": kappa, "regularisation_image": "E^H d",
                    "l2_flush": "256 MB write before every timed step"},
         "setup_ms_regulariser_and_preconditioner": round(setup_ms, 4),
+        "setup_ms_trajectory_and_dcw_96x512": round(gen_ms, 4),
+        "cpu_oracle_ms_dcw_96x512": round(gen_cpu_ms, 1),
         "regulariser_offset": R.offset_, "regulariser_offset_oracle": off_o,
         "recon_rel_l2_vs_oracle_fp64_cg": O.rel_l2(x.cpu().numpy(), xr),
         "gpu_launches": int(launches),

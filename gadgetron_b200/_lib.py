@@ -90,6 +90,11 @@ def _load():
         "gb_cg_set_image_regularization": (i32, [P, P, f32]),
         "gb_image_operator_compute": (i32, [P, u64, i32, P, P, P]),
         "gb_sense_precond_weights": (i32, [P, P, f32, P, P]),
+        "gb_radial_trajectory_golden_ratio_2d": (i32, [u32, u32, u32, u32, i32, P, P]),
+        "gb_radial_trajectory_fixed_angle_2d": (i32, [u32, u32, u32, f32, P, P]),
+        "gb_radial_trajectory_variable_angle_2d": (i32, [P, u32, u32, u32, P, P]),
+        "gb_radial_dcw_golden_ratio_2d": (i32, [u32, u32, f32, f32, u32, i32, P, P]),
+        "gb_radial_dcw_fixed_angle_2d": (i32, [u32, u32, f32, f32, P, P]),
         "gb_cg_set_refinements": (i32, [P, u32]),
         "gb_cg_set_use_graph": (i32, [P, i32]),
         "gb_cg_set_frame_independent": (i32, [P, i32]),
@@ -112,7 +117,9 @@ EXPORTED = (
     "gb_cg_create gb_cg_destroy gb_cg_set_encoding_operator gb_cg_set_max_iterations "
     "gb_cg_set_tc_tolerance gb_cg_set_x0 gb_cg_set_preconditioner gb_cg_set_identity_regularization "
     "gb_cg_set_refinements gb_cg_set_use_graph gb_cg_set_frame_independent gb_cg_solve "
-    "gb_cg_set_image_regularization gb_image_operator_compute gb_sense_precond_weights").split()
+    "gb_cg_set_image_regularization gb_image_operator_compute gb_sense_precond_weights "
+    "gb_radial_trajectory_golden_ratio_2d gb_radial_trajectory_fixed_angle_2d gb_radial_trajectory_variable_angle_2d "
+    "gb_radial_dcw_golden_ratio_2d gb_radial_dcw_fixed_angle_2d").split()
 
 
 def check(status: int):

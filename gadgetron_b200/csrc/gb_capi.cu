@@ -480,6 +480,50 @@ GB_API gb_status gb_cg_set_image_regularization(gb_cg_solver solver, const float
     });
 }
 
+GB_API gb_status gb_radial_trajectory_golden_ratio_2d(uint32_t samples_per_profile, uint32_t profiles_per_frame,
+                                                     uint32_t frames, uint32_t profile_offset, int mode,
+                                                     float *trajectory, void *stream) {
+    return guarded([&] {
+        radial_traj_golden(trajectory, (int)samples_per_profile, (int)profiles_per_frame, (int)frames,
+                           (int)profile_offset, mode, S(stream));
+    });
+}
+
+GB_API gb_status gb_radial_trajectory_fixed_angle_2d(uint32_t samples_per_profile, uint32_t profiles_per_frame,
+                                                     uint32_t frames, float angular_offset, float *trajectory,
+                                                     void *stream) {
+    return guarded([&] {
+        radial_traj_fixed(trajectory, (int)samples_per_profile, (int)profiles_per_frame, (int)frames, angular_offset,
+                          S(stream));
+    });
+}
+
+GB_API gb_status gb_radial_trajectory_variable_angle_2d(const float *angles, uint32_t samples_per_profile,
+                                                        uint32_t profiles_per_frame, uint32_t frames,
+                                                        float *trajectory, void *stream) {
+    return guarded([&] {
+        radial_traj_variable(trajectory, angles, (int)samples_per_profile, (int)profiles_per_frame, (int)frames,
+                             S(stream));
+    });
+}
+
+GB_API gb_status gb_radial_dcw_golden_ratio_2d(uint32_t samples_per_profile, uint32_t profiles, float alpha,
+                                               float one_over_radial_oversampling, uint32_t profile_offset, int mode,
+                                               float *dcw, void *stream) {
+    return guarded([&] {
+        radial_dcw(dcw, (int)samples_per_profile, (int)profiles, alpha, one_over_radial_oversampling,
+                   (int)profile_offset, true, mode, S(stream));
+    });
+}
+
+GB_API gb_status gb_radial_dcw_fixed_angle_2d(uint32_t samples_per_profile, uint32_t profiles, float alpha,
+                                              float one_over_radial_oversampling, float *dcw, void *stream) {
+    return guarded([&] {
+        radial_dcw(dcw, (int)samples_per_profile, (int)profiles, alpha, one_over_radial_oversampling, 0, false, 1,
+                   S(stream));
+    });
+}
+
 GB_API gb_status gb_image_operator_compute(const void *reg_image, uint64_t n, int offset_estimation,
                                            float *image, float *offset, void *stream) {
     return guarded([&] {

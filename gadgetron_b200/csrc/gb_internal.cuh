@@ -430,4 +430,12 @@ float image_operator_compute(const float2 *reg, int64_t n, bool offset_estimatio
 void sense_precond_weights(const float2 *csm, int nb, int64_t nn, const float *reg, float kappa, float *w,
                            cudaStream_t st);
 
+// Radial trajectories [frames][profiles * S][2] and density compensation
+// weights [profiles * S] (gb_radial.cu).
+void radial_traj_golden(float *traj, int S, int P, int F, int profile_offset, int mode, cudaStream_t st);
+void radial_traj_fixed(float *traj, int S, int P, int F, float angular_offset, cudaStream_t st);
+void radial_traj_variable(float *traj, const float *angles, int S, int P, int F, cudaStream_t st);
+void radial_dcw(float *dcw, int S, int P, float alpha, float ovs, int profile_offset, bool golden, int mode,
+                cudaStream_t st);
+
 }  // namespace gb

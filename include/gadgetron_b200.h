@@ -300,6 +300,35 @@ GB_API gb_status gb_cg_set_image_regularization(gb_cg_solver solver, const float
  * image: n floats (device); offset: host float or NULL.  Synchronises. */
 GB_API gb_status gb_image_operator_compute(const void *reg_image, uint64_t n, int offset_estimation,
                                            float *image, float *offset, void *stream);
+/* ---------------------------------------------------- radial trajectories */
+
+/* compute_radial_trajectory_golden_ratio_2d (toolboxes/core/gpu/radial_utilities.cu:46-87,
+ * radial_utilities.h:16-39): trajectory [frames][profiles_per_frame *
+ * samples_per_profile][2] floats (device), profile p (counted over all frames)
+ * at angle (p + profile_offset) * step + pi, step = pi (3 - sqrt 5)/2 (mode 0,
+ * GR_SMALLEST) or pi / golden ratio (mode 1, GR_ORIGINAL); sample s at
+ * (s - S/2) / S.  samples_per_profile must be a multiple of 32. */
+GB_API gb_status gb_radial_trajectory_golden_ratio_2d(uint32_t samples_per_profile, uint32_t profiles_per_frame,
+                                                     uint32_t frames, uint32_t profile_offset, int mode,
+                                                     float *trajectory, void *stream);
+/* compute_radial_trajectory_fixed_angle_2d (radial_utilities.cu:143-199). */
+GB_API gb_status gb_radial_trajectory_fixed_angle_2d(uint32_t samples_per_profile, uint32_t profiles_per_frame,
+                                                     uint32_t frames, float angular_offset, float *trajectory,
+                                                     void *stream);
+/* compute_radial_trajectory_variable_angle_2d (radial_utilities.cu:89-140):
+ * angles: device floats [frames]. */
+GB_API gb_status gb_radial_trajectory_variable_angle_2d(const float *angles, uint32_t samples_per_profile,
+                                                        uint32_t profiles_per_frame, uint32_t frames,
+                                                        float *trajectory, void *stream);
+/* compute_radial_dcw_golden_ratio_2d / compute_radial_dcw_fixed_angle_2d
+ * (radial_utilities.cu:200-441): Voronoi-area weights of one frame,
+ * dcw [profiles * samples_per_profile] floats (device). */
+GB_API gb_status gb_radial_dcw_golden_ratio_2d(uint32_t samples_per_profile, uint32_t profiles, float alpha,
+                                               float one_over_radial_oversampling, uint32_t profile_offset, int mode,
+                                               float *dcw, void *stream);
+GB_API gb_status gb_radial_dcw_fixed_angle_2d(uint32_t samples_per_profile, uint32_t profiles, float alpha,
+                                              float one_over_radial_oversampling, float *dcw, void *stream);
+
 /* Preconditioner weights of gpuCgSenseGadget.cpp:167-176:
  * w = 1 / sqrt(sum_c |csm_c|^2 + kappa * reg_image) over the N... pixels of
  * the operator (reg_image NULL: csm term only).  weights: device floats. */

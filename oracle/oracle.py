@@ -32,6 +32,8 @@ cuNonCartesianSenseOperator and cgSolver) on the CPU:
 * the CG solver follows ``toolboxes/solvers/cgSolver.h:105-390`` with the
   ``relativeResidualTCB`` stop rule of ``toolboxes/solvers/cgCallback.h:56-104``;
   regularisation terms w_i R_i^H R_i follow ``cgSolver.h:355-390``;
+* radial trajectories and their Voronoi density compensation weights follow
+  ``toolboxes/core/gpu/radial_utilities.cu:18-441``;
 * the image regulariser follows ``toolboxes/operators/imageOperator.h:27-67``
   and its offset estimate ``toolboxes/operators/gpu/cuImageOperator.h:35-62``;
   the preconditioner weights follow ``gadgets/pmri/gpuCgSenseGadget.cpp:167-176``.
@@ -475,6 +477,129 @@ def cg_solve(op, d: np.ndarray, iterations: int = 10, tc_tolerance: float = 1e-3
         if rq / rq0 < tc_tolerance:
             break
     return x
+
+
+# ------------------------------------------------------- radial utilities ---
+
+_PI32 = np.float32(np.pi)
+
+
+def _fma32(a, b, c):
+    """float32 a * b + c with one rounding (the product of two floats is
+    exact in double; the sum is rounded to double, then to float)."""
+    return (np.asarray(a, np.float64) * np.float64(b) + np.asarray(c, np.float64)).astype(np.float32)
+
+
+def _gr_step(mode: int) -> np.float32:
+    """get_angle_step_GR<float, mode> (radial_utilities.cu:18-23)."""
+    s5 = np.sqrt(np.float32(5.0))
+    if mode == 0:
+        return np.float32(np.float32(_PI32 * (np.float32(3.0) - s5)) * np.float32(0.5))
+    return np.float32(_PI32 / np.float32((s5 + np.float32(1.0)) * np.float32(0.5)))
+
+
+def _pos(S: int, cos_a, sin_a):
+    s = np.arange(S, dtype=np.float32)
+    Sf = np.float32(S)
+    b = np.float32(Sf * np.float32(0.5))
+    d = (s - b).astype(np.float32)
+    x = (d[None, :] * cos_a[:, None]).astype(np.float32) / Sf
+    y = (d[None, :] * sin_a[:, None]).astype(np.float32) / Sf
+    return np.stack([x.astype(np.float32), y.astype(np.float32)], -1)
+
+
+def radial_trajectory_golden_ratio_2d(S: int, P: int, F: int = 1, profile_offset: int = 0, mode: int = 1):
+    """compute_radial_trajectory_golden_ratio_2d (radial_utilities.cu:25-87):
+    [F, P*S, 2] float32; profile p over all frames at
+    (p + offset) * step + pi."""
+    prof = np.arange(P * F, dtype=np.float32)
+    # (p + offset) * step + pi as one fused multiply-add (nvcc contracts it)
+    ang = _fma32((prof + np.float32(profile_offset)).astype(np.float32), _gr_step(mode), _PI32)
+    pos = _pos(S, np.cos(ang).astype(np.float32), np.sin(ang).astype(np.float32))
+    return pos.reshape(F, P * S, 2)
+
+
+def radial_trajectory_fixed_angle_2d(S: int, P: int, F: int = 1, angular_offset: float = 0.0):
+    """compute_radial_trajectory_fixed_angle_2d (radial_utilities.cu:143-199):
+    profile l of frame f at (l + f/F)/P * pi + angular_offset + pi."""
+    inv_p, inv_f = np.float32(1.0) / np.float32(P), np.float32(1.0) / np.float32(F)
+    f = np.repeat(np.arange(F, dtype=np.float32), P)
+    l = np.tile(np.arange(P, dtype=np.float32), F)
+    a = (_fma32(f, inv_f, l) * inv_p).astype(np.float32)
+    ang = (_fma32(a, _PI32, np.float32(angular_offset)) + _PI32).astype(np.float32)
+    pos = _pos(S, np.cos(ang).astype(np.float32), np.sin(ang).astype(np.float32))
+    return pos.reshape(F, P * S, 2)
+
+
+def radial_trajectory_variable_angle_2d(angles, S: int, P: int, F: int):
+    """compute_radial_trajectory_variable_angle_2d (radial_utilities.cu:89-140):
+    every profile of frame f at angles[f]."""
+    ang = np.repeat(np.asarray(angles, np.float32)[:F], P)
+    pos = _pos(S, np.cos(ang).astype(np.float32), np.sin(ang).astype(np.float32))
+    return pos.reshape(F, P * S, 2)
+
+
+def radial_dcw_2d(S: int, P: int, alpha: float, ovs: float, profile_offset: int = 0, golden: bool = True,
+                  mode: int = 1) -> np.ndarray:
+    """compute_radial_dcw_2d (radial_utilities.cu:200-396): the area of the
+    polygon through the midpoints towards the sample's two neighbours on its
+    profile and, on either side of the profile, the nearest sample of any
+    other profile (either half-line) with its two profile neighbours; the
+    centre sample gets pi (alpha ovs / 2)^2 / P.  Profile angles without + pi.
+    Returns [P*S] float32 (one frame)."""
+    f32 = np.float32
+    alpha, ovs = f32(alpha), f32(ovs)
+    if golden:
+        ang = ((np.arange(P, dtype=f32) + f32(profile_offset)) * _gr_step(mode)).astype(f32)
+    else:
+        ang = ((np.arange(P, dtype=f32) * (f32(1.0) / f32(P))).astype(f32) * _PI32).astype(f32)
+    cs, sn = np.cos(ang).astype(f32), np.sin(ang).astype(f32)
+    Sf = f32(S)
+    bias = f32(Sf * f32(0.5))
+    s = np.arange(S, dtype=f32)
+    sc = lambda v: (alpha * (v.astype(f32) * ovs).astype(f32)).astype(f32)
+    ctr, ctr_inv = sc(s - bias), sc((Sf - s).astype(f32) - bias)
+    prv, prv_inv = sc((s - bias).astype(f32) - f32(1.0)), sc((Sf - (s - f32(1.0))).astype(f32) - bias)
+    nxt, nxt_inv = sc((s - bias).astype(f32) + f32(1.0)), sc((Sf - (s + f32(1.0))).astype(f32) - bias)
+    out = np.zeros((P, S), f32)
+    r = f32(f32(alpha * ovs) * f32(0.5))
+    big = np.finfo(np.float32).max
+    for p in range(P):
+        c0, s0 = cs[p], sn[p]
+        pos = np.stack([ctr * c0, ctr * s0], -1).astype(f32)          # [S, 2]
+        nrm = np.array([-s0, c0], f32)
+        A = np.full((3, S, 2), big, f32)
+        B = np.full((3, S, 2), big, f32)
+        da = np.full(S, np.inf)
+        db = np.full(S, np.inf)
+        for i in range(P):
+            if i == p:
+                continue
+            d = np.array([cs[i], sn[i]], f32)
+            for c_s, p_s, n_s in ((ctr, prv, nxt), (ctr_inv, prv_inv, nxt_inv)):
+                cpos = (c_s[:, None] * d[None]).astype(f32)
+                side = ((cpos - pos) * nrm[None]).astype(f32).sum(-1)
+                dist = (((cpos - pos).astype(np.float64)) ** 2).sum(-1)
+                pa = side > 0
+                upd_a = pa & (dist < da)
+                upd_b = (~pa) & (dist < db)
+                for tgt, upd, dd in ((A, upd_a, da), (B, upd_b, db)):
+                    tgt[0][upd] = (p_s[upd, None] * d[None]).astype(f32)
+                    tgt[1][upd] = cpos[upd]
+                    tgt[2][upd] = (n_s[upd, None] * d[None]).astype(f32)
+                    dd[upd] = dist[upd]
+        own_p = np.stack([prv * c0, prv * s0], -1).astype(f32)
+        own_n = np.stack([nxt * c0, nxt * s0], -1).astype(f32)
+        verts = [own_p, A[0], A[1], A[2], own_n, B[2], B[1], B[0]]
+        m = [(f32(0.5) * (pos + v).astype(f32)).astype(np.float64) for v in verts]
+        area = np.zeros(S)
+        for k in range(8):
+            u, t = m[k], m[(k + 1) % 8]
+            area += u[:, 0] * t[:, 1] - t[:, 0] * u[:, 1]
+        w = np.abs(0.5 * area).astype(f32)
+        w[S // 2] = f32(f32(r * r) * _PI32) / f32(P)
+        out[p] = w
+    return out.reshape(-1)
 
 
 # ---------------------------------------------------------------- NDFT ------

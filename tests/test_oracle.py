@@ -246,3 +246,33 @@ def test_cg_regularization_term_is_kappa_R_squared():
     R = np.array([1.0, 2.0, 3.0])
     x = O.cg_solve(Eye(), d, iterations=5, tc_tolerance=0.0, regularization=[(0.5, R)])
     np.testing.assert_allclose(x, d / (1.0 + 0.5 * R * R), rtol=1e-12)
+
+
+def test_radial_trajectory_conventions():
+    """The golden-ratio trajectory of radial_utilities.cu:25-44 is the one the
+    synthetic workloads use (FP64 there, float32 here); fixed angles cover a
+    half turn."""
+    t = O.radial_trajectory_golden_ratio_2d(256, 64)
+    np.testing.assert_allclose(t.reshape(-1, 2), S.radial_golden_angle_2d(64, 256), atol=1e-5)
+    f = O.radial_trajectory_fixed_angle_2d(64, 8, 2)
+    ang = np.arctan2(f[0, 0::64, 1], f[0, 0::64, 0])     # first sample of every profile of frame 0
+    steps = np.diff(np.unwrap(ang))
+    np.testing.assert_allclose(steps, np.pi / 8, atol=1e-5)
+    f1 = np.arctan2(f[1, 0, 1], f[1, 0, 0])               # frame 1 is shifted by pi / (8 * 2)
+    assert abs(np.angle(np.exp(1j * (f1 - ang[0]))) - np.pi / 16) < 1e-5
+
+
+def test_radial_dcw_geometry():
+    """Voronoi weights (radial_utilities.cu:200-396): with equally spaced
+    profiles they are the same on every profile, symmetric about the centre,
+    grow linearly away from it, and tile the disc they cover."""
+    P, Sn = 64, 128
+    w = O.radial_dcw_2d(Sn, P, 1.0, 1.0, golden=False).reshape(P, Sn)
+    np.testing.assert_allclose(w, np.broadcast_to(w[:1], w.shape), rtol=1e-4)
+    np.testing.assert_allclose(w[0, 1:Sn // 2], w[0, Sn - 1:Sn // 2:-1], rtol=1e-4)
+    # ring of radius r at unit radial spacing: 2 pi r / (2 P) per sample
+    r = np.abs(np.arange(Sn) - Sn // 2)[Sn // 2 + 1:Sn - 1]
+    np.testing.assert_allclose(w[0, Sn // 2 + 1:Sn - 1], np.pi * r / P, rtol=2e-3)
+    assert abs(w[0, Sn // 2] - np.pi * 0.25 / P) < 1e-7
+    total = w.sum()
+    assert abs(total - np.pi * (Sn / 2) ** 2) / (np.pi * (Sn / 2) ** 2) < 0.02
