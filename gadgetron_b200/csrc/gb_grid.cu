@@ -993,9 +993,9 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
 // region staging and lane layout as k_degrid_c2nc, but each lane reads its
 // sample's tap weights straight from the per-trajectory weight table into
 // registers (no per-warp staging, no kernel evaluation) and runs a fully
-// unrolled NT x NT (x NT) tap nest (2D: unpredicated over zero weights; 3D:
-// predicated on the sample's tap counts), so the inner loop is loads and
-// FMAs only.  NT = the largest tap count a
+// unrolled NT x NT (x NT) tap nest (unpredicated in x and y over the zero
+// weights beyond the footprint; 3D slices predicated on the sample's z
+// count), so the inner loop is loads and FMAs only.  NT = the largest tap count a
 // footprint can have (2*ceil(W/2), plus one when W is an even integer).
 template <int CG, int NT, bool D3>
 __global__ void __launch_bounds__(kThreads, D3 ? 2 : 3)
@@ -1095,7 +1095,7 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
                 }
             }
         }
-        if (!D3) {
+        {
             // zero pad after the region: a tap with zero weight beyond the
             // footprint may read up to one row and one cell past it
             const int npad = (R0 + 1) * CS;
@@ -1138,13 +1138,14 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
 #pragma unroll
         for (int c = 0; c < CPL; c++) acc[c][0] = acc[c][1] = 0.f;
         const float2 *base_s = tile_s + (((size_t)rs[2] * R1 + rs[1]) * R0 + rs[0]) * CS + ll * CPL;
-        // Tap nest, unrolled to NTT taps per dimension.  2D: no per-tap
-        // predicates -- the table weights beyond a footprint are zero and the
-        // footprint starts at most NT-1 cells before the region's end, so the
-        // extra taps read at most one row and one cell past the region (the
-        // zero pad).  3D: predicated on the sample's counts.  When every
-        // sample of the warp has fewer than NT taps in every dimension (the
-        // common case when W is an even integer) the NT-1 nest runs.
+        // Tap nest, unrolled to NTT taps per dimension, with no per-tap
+        // predicates in x and y: the table weights beyond a footprint are zero
+        // and a footprint starts at most NT-1 cells before the region's end,
+        // so the extra taps read at most one row and one cell past a slice --
+        // the next slice, or after the last one the zero pad.  3D slices stay
+        // predicated on the sample's z count.  When every sample of the warp
+        // has fewer than NT taps in every dimension (the common case when W is
+        // an even integer) the NT-1 nest runs.
         auto nest = [&](auto ntc) {
             constexpr int NTT = decltype(ntc)::value;
 #pragma unroll
@@ -1152,12 +1153,12 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
                 if (tzi < n[2]) {
 #pragma unroll
                     for (int tyi = 0; tyi < NTT; tyi++) {
-                        if (D3 ? tyi < n[1] : true) {
+                        {
                             const float wyz = D3 ? w[1][tyi] * w[2][tzi] : w[1][tyi];
                             const float2 *row = base_s + ((size_t)tzi * R1 + tyi) * R0 * CS;
 #pragma unroll
                             for (int t = 0; t < NTT; t++) {
-                                if (D3 ? t < n[0] : true) {
+                                {
                                     const float wv = w[0][t] * wyz;
                                     if (CPL == 2) {
                                         const float4 q = *reinterpret_cast<const float4 *>(row + t * CS);
@@ -1469,7 +1470,7 @@ static void degrid_dispatch(int cg, const ConvArgs &a, dim3 g, size_t smem, cons
 
 static size_t degrid_table_smem(const KParams &k, int cg) {
     const int cs = k.D == 3 ? cg : cg + 2;   // cell stride of k_degrid_table
-    const size_t pad = k.D == 3 ? 0 : (size_t)(region_dim(k, 0) + 1) * cs;
+    const size_t pad = (size_t)(region_dim(k, 0) + 1) * cs;
     return ((size_t)region_dim(k, 0) * region_dim(k, 1) * region_dim(k, 2) * cs + pad) * sizeof(float2);
 }
 
