@@ -213,8 +213,7 @@ def run_ours(args, rank, world, local_rank):
             import torch.distributed as dist
             dist.barrier()
 
-    clk = ClockSampler(local_rank, os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % rank)
-                       if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else None)
+    clk = ClockSampler(local_rank, (args.clocks_csv % rank) if args.clocks_csv else None)
     launches0 = lib.gb_kernel_launch_count()
     barrier()
     torch.cuda.synchronize()
@@ -851,6 +850,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="cg-sense-2d",
                     choices=["cg-sense-2d", "nufft-2d", "nufft-3d", "batched", "precision", "regularised"])
+    ap.add_argument("--clocks-csv", default=None,
+                    help="also write the raw clock samples of the timed region to this CSV path "
+                         "(%%d = rank)")
     ap.add_argument("--size", default="full", choices=["full", "small"],
                     help="profiling cases: nufft-3d small = 64^3; batched small = 16 frames")
     args = ap.parse_args()
