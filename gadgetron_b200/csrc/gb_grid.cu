@@ -482,6 +482,24 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
 #pragma unroll
         for (int j = 0; j < RW; j++) acc[c][j][0] = acc[c][j][1] = acc[c][j][2] = acc[c][j][3] = 0.f;
 
+    // A tile no sample touches: its cells are zero (nothing to add when
+    // accumulating) -- one pass of coalesced stores, no staging.
+    if (it.begin == it.end && it.split < 0) {
+        if (a.accumulate) return;
+        const int cells = T0 * T1 * k.tile[2];
+        const int64_t ostep = (int64_t)a.F * a.kl.s_bf;
+        float2 *gbase = grid + ((int64_t)b0 * a.F + f) * a.kl.s_bf;
+        for (int e = threadIdx.x; e < cells; e += kThreads) {
+            const int x = e % T0, yz = e / T0, y = yz % T1, z = yz / T1;
+            float2 *o = gbase + (int64_t)(org2 + z) * a.kl.s_z + (int64_t)(org1 + y) * a.kl.s_y + org0 + x;
+            for (int c = 0; c < CG && b0 + c < a.nb; c++) {
+                *o = make_float2(0.f, 0.f);
+                o += ostep;
+            }
+        }
+        return;
+    }
+
     const uint32_t bar[2] = {smem_u32(&s_bar[0]), smem_u32(&s_bar[1])};
     if (threadIdx.x == 0) {
         mbar_init(bar[0], 1);
