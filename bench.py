@@ -804,6 +804,15 @@ def run_regularized(args):
     t0 = time.perf_counter()
     O.radial_dcw_2d(CFG["samples"], CFG["spokes"], 2.0, 0.5)
     gen_cpu_ms = (time.perf_counter() - t0) * 1e3
+    # density compensation estimate of the headline trajectory (Jinc kernel,
+    # width 5.5, oversampling 2, 10 iterations)
+    from gadgetron_b200 import sdc as SDC
+    traj_d = torch.from_numpy(wl["traj"]).to(dev)
+    sdc_ms = _timed(lambda: SDC.estimate_dcw(traj_d, N, 2.0, 10, 5.5), max(2, args.steps // 5), 1, None, stream)
+    w_sdc = SDC.estimate_dcw(traj_d, N, 2.0, 10, 5.5)
+    t0 = time.perf_counter()
+    w_sdc_o = O.estimate_dcw(wl["traj"], N, 2.0, 10, 5.5)
+    sdc_cpu_ms = (time.perf_counter() - t0) * 1e3
     R.set_weight(kappa)
     cg = gb.cuCgSolver()
     cg.set_encoding_operator(E)
@@ -835,6 +844,8 @@ def run_regularized(args):
         "setup_ms_regulariser_and_preconditioner": round(setup_ms, 4),
         "setup_ms_trajectory_and_dcw_96x512": round(gen_ms, 4),
         "cpu_oracle_ms_dcw_96x512": round(gen_cpu_ms, 1),
+        "sdc_ms_96x512_os2_10it": round(sdc_ms, 3), "cpu_oracle_ms_sdc": round(sdc_cpu_ms, 1),
+        "sdc_rel_l2_vs_oracle": O.rel_l2(w_sdc.cpu().numpy(), w_sdc_o),
         "regulariser_offset": R.offset_, "regulariser_offset_oracle": off_o,
         "recon_rel_l2_vs_oracle_fp64_cg": O.rel_l2(x.cpu().numpy(), xr),
         "gpu_launches": int(launches),

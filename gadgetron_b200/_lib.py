@@ -95,6 +95,7 @@ def _load():
         "gb_radial_trajectory_variable_angle_2d": (i32, [P, u32, u32, u32, P, P]),
         "gb_radial_dcw_golden_ratio_2d": (i32, [u32, u32, f32, f32, u32, i32, P, P]),
         "gb_radial_dcw_fixed_angle_2d": (i32, [u32, u32, f32, f32, P, P]),
+        "gb_sdc_estimate_dcw": (i32, [i32, P, f32, u32, f32, P, u64, P, P, P]),
         "gb_cg_set_refinements": (i32, [P, u32]),
         "gb_cg_set_use_graph": (i32, [P, i32]),
         "gb_cg_set_frame_independent": (i32, [P, i32]),
@@ -119,7 +120,7 @@ EXPORTED = (
     "gb_cg_set_refinements gb_cg_set_use_graph gb_cg_set_frame_independent gb_cg_solve "
     "gb_cg_set_image_regularization gb_image_operator_compute gb_sense_precond_weights "
     "gb_radial_trajectory_golden_ratio_2d gb_radial_trajectory_fixed_angle_2d gb_radial_trajectory_variable_angle_2d "
-    "gb_radial_dcw_golden_ratio_2d gb_radial_dcw_fixed_angle_2d").split()
+    "gb_radial_dcw_golden_ratio_2d gb_radial_dcw_fixed_angle_2d gb_sdc_estimate_dcw").split()
 
 
 def check(status: int):

@@ -524,6 +524,15 @@ GB_API gb_status gb_radial_dcw_fixed_angle_2d(uint32_t samples_per_profile, uint
     });
 }
 
+GB_API gb_status gb_sdc_estimate_dcw(int D, const uint64_t *matrix_size, float os_factor, uint32_t num_iterations,
+                                     float kernel_width, const float *trajectory, uint64_t num_samples,
+                                     const float *initial_dcw, float *dcw, void *stream) {
+    return guarded([&] {
+        sdc_estimate_dcw(D, matrix_size, os_factor, (int)num_iterations, kernel_width, trajectory,
+                         (int64_t)num_samples, initial_dcw, dcw, S(stream));
+    });
+}
+
 GB_API gb_status gb_image_operator_compute(const void *reg_image, uint64_t n, int offset_estimation,
                                            float *image, float *offset, void *stream) {
     return guarded([&] {

@@ -438,4 +438,8 @@ void radial_traj_variable(float *traj, const float *angles, int S, int P, int F,
 void radial_dcw(float *dcw, int S, int P, float alpha, float ovs, int profile_offset, bool golden, int mode,
                 cudaStream_t st);
 
+// Iterative density compensation with a Jinc kernel (gb_sdc.cu).
+void sdc_estimate_dcw(int D, const uint64_t *N, float os_factor, int iterations, float kernel_width,
+                      const float *traj, int64_t M, const float *initial, float *dcw, cudaStream_t st);
+
 }  // namespace gb

@@ -329,6 +329,16 @@ GB_API gb_status gb_radial_dcw_golden_ratio_2d(uint32_t samples_per_profile, uin
 GB_API gb_status gb_radial_dcw_fixed_angle_2d(uint32_t samples_per_profile, uint32_t profiles, float alpha,
                                               float one_over_radial_oversampling, float *dcw, void *stream);
 
+/* estimate_dcw (toolboxes/mri/sdc/SDC.hpp:19-80, gpu/cuSDC.cu): iterative
+ * density compensation with the Jinc kernel of width kernel_width (radius
+ * 0.9696 * kernel_width) on a grid of round_up_32(N * os_factor) cells per
+ * dimension: w <- w / C2NC(NC2C(w)), num_iterations times, from w = 1 or
+ * initial_dcw (may be NULL).  trajectory: num_samples x D floats in
+ * [-1/2, 1/2] (device); dcw: num_samples floats (device).  Synchronises. */
+GB_API gb_status gb_sdc_estimate_dcw(int D, const uint64_t *matrix_size, float os_factor, uint32_t num_iterations,
+                                     float kernel_width, const float *trajectory, uint64_t num_samples,
+                                     const float *initial_dcw, float *dcw, void *stream);
+
 /* Preconditioner weights of gpuCgSenseGadget.cpp:167-176:
  * w = 1 / sqrt(sum_c |csm_c|^2 + kappa * reg_image) over the N... pixels of
  * the operator (reg_image NULL: csm term only).  weights: device floats. */

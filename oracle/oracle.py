@@ -34,6 +34,8 @@ cuNonCartesianSenseOperator and cgSolver) on the CPU:
   regularisation terms w_i R_i^H R_i follow ``cgSolver.h:355-390``;
 * radial trajectories and their Voronoi density compensation weights follow
   ``toolboxes/core/gpu/radial_utilities.cu:18-441``;
+* the density compensation estimate follows ``toolboxes/mri/sdc/SDC.hpp:19-80``
+  with the Jinc kernel of ``toolboxes/nfft/ConvolutionKernel.hpp:307-397``;
 * the image regulariser follows ``toolboxes/operators/imageOperator.h:27-67``
   and its offset estimate ``toolboxes/operators/gpu/cuImageOperator.h:35-62``;
   the preconditioner weights follow ``gadgets/pmri/gpuCgSenseGadget.cpp:167-176``.
@@ -600,6 +602,93 @@ def radial_dcw_2d(S: int, P: int, alpha: float, ovs: float, profile_offset: int 
         w[S // 2] = f32(f32(r * r) * _PI32) / f32(P)
         out[p] = w
     return out.reshape(-1)
+
+
+# ------------------------------------------------- density compensation -----
+
+_JINC_NORM_RADIUS = np.float32(0.96960938)
+_JINC_C = [np.float32(c) for c in (0.999923599661866, 0.014023570134078, -2.969947516849635,
+                                   0.891173008769047, 2.326043034495162, -1.270644932677047)]
+
+
+def jinc_weight(ad: np.ndarray, R) -> np.ndarray:
+    """JincKernel::get (ConvolutionKernel.hpp:165-170, 349-397) for absolute
+    offsets ad [..., D] (float32): 0 if any |u_d| > R; else r = |u| / R,
+    0 if r >= 0.96960938, else the degree-5 polynomial clipped at 0."""
+    ad = np.asarray(ad, np.float32)
+    R = np.float32(R)
+    r = np.sqrt(np.sum(ad.astype(np.float64) ** 2, axis=-1)).astype(np.float32) / R
+    v = np.full(r.shape, _JINC_C[0], np.float64)
+    for k in range(1, 6):
+        v = v + np.float64(_JINC_C[k]) * np.power(r.astype(np.float64), k)
+    v = np.maximum(v, 0.0)
+    return np.where((r >= _JINC_NORM_RADIUS) | np.any(ad > R, axis=-1), 0.0, v)
+
+
+def estimate_dcw(traj: np.ndarray, matrix_size, os_factor: float, num_iterations: int, kernel_width: float = 5.5,
+                 initial_dcw=None) -> np.ndarray:
+    """estimate_dcw (SDC.hpp:19-80, cuSDC.cu): w <- w / C2NC(NC2C(w)) with the
+    Jinc kernel on a grid of round_up_32(N * os) cells per dimension (periodic),
+    sample coordinate s = k mos + mos/2, taps [ceil(s - R), floor(s + R)].
+    Sums in FP64."""
+    traj = np.asarray(traj, np.float32).reshape(-1, len(matrix_size))
+    M, D = traj.shape
+    R = np.float32(_JINC_NORM_RADIUS * np.float32(kernel_width))
+    pad = 2 * int(np.ceil(R))
+    mos = []
+    for n in matrix_size:
+        m = int(np.float32(n) * np.float32(os_factor))
+        mos.append(((m + 31) // 32) * 32)
+    s = np.stack([(_fma32(traj[:, d], np.float32(mos[d]), np.float32((mos[d] + pad) >> 1)) -
+                   np.float32(pad // 2)).astype(np.float32) for d in range(D)], -1)
+    lo = np.ceil(s - R).astype(np.int64)
+    K = int(np.floor(2 * R)) + 2
+    # all (sample, footprint cell) pairs with their weights and cell indices
+    offs = np.stack(np.meshgrid(*[np.arange(K)] * D, indexing="ij"), -1).reshape(-1, D)   # [K^D, D]
+    cells = lo[:, None, :] + offs[None]                                                   # [M, K^D, D]
+    ad = np.abs(s[:, None, :] - cells.astype(np.float32))
+    inside = np.all(cells <= np.floor(s + R).astype(np.int64)[:, None, :], axis=-1)
+    w = jinc_weight(ad, R)
+    w[~inside] = 0.0
+    idx = np.zeros(cells.shape[:2], np.int64)
+    for d in range(D - 1, -1, -1):
+        idx = idx * mos[d] + np.mod(cells[..., d], mos[d])
+    G = int(np.prod(mos))
+    dcw = np.ones(M) if initial_dcw is None else np.asarray(initial_dcw, np.float64).copy()
+    for _ in range(num_iterations):
+        grid = np.bincount(idx.ravel(), weights=(w * dcw[:, None]).ravel(), minlength=G)
+        t = np.sum(w * grid[idx], axis=1)
+        dcw = np.where(t == 0, 0.0, dcw / np.where(t == 0, 1.0, t))
+    return dcw
+
+
+def sdc_fixed_point_residual(traj, matrix_size, os_factor, kernel_width, dcw) -> float:
+    """max_j |C2NC(NC2C(w))_j - 1| over samples with w_j > 0: the fixed point
+    the estimate converges to."""
+    traj = np.asarray(traj, np.float32).reshape(-1, len(matrix_size))
+    t = estimate_dcw(traj, matrix_size, os_factor, 0, kernel_width)   # builds nothing, returns ones
+    del t
+    M, D = traj.shape
+    R = np.float32(_JINC_NORM_RADIUS * np.float32(kernel_width))
+    pad = 2 * int(np.ceil(R))
+    mos = [(((int(np.float32(n) * np.float32(os_factor))) + 31) // 32) * 32 for n in matrix_size]
+    s = np.stack([(_fma32(traj[:, d], np.float32(mos[d]), np.float32((mos[d] + pad) >> 1)) -
+                   np.float32(pad // 2)).astype(np.float32) for d in range(D)], -1)
+    lo = np.ceil(s - R).astype(np.int64)
+    K = int(np.floor(2 * R)) + 2
+    offs = np.stack(np.meshgrid(*[np.arange(K)] * D, indexing="ij"), -1).reshape(-1, D)
+    cells = lo[:, None, :] + offs[None]
+    inside = np.all(cells <= np.floor(s + R).astype(np.int64)[:, None, :], axis=-1)
+    w = jinc_weight(np.abs(s[:, None, :] - cells.astype(np.float32)), R)
+    w[~inside] = 0.0
+    idx = np.zeros(cells.shape[:2], np.int64)
+    for d in range(D - 1, -1, -1):
+        idx = idx * mos[d] + np.mod(cells[..., d], mos[d])
+    dcw = np.asarray(dcw, np.float64)
+    grid = np.bincount(idx.ravel(), weights=(w * dcw[:, None]).ravel(), minlength=int(np.prod(mos)))
+    t = np.sum(w * grid[idx], axis=1)
+    m = dcw > 0
+    return float(np.max(np.abs(t[m] - 1.0)))
 
 
 # ---------------------------------------------------------------- NDFT ------

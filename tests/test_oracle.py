@@ -276,3 +276,68 @@ def test_radial_dcw_geometry():
     assert abs(w[0, Sn // 2] - np.pi * 0.25 / P) < 1e-7
     total = w.sum()
     assert abs(total - np.pi * (Sn / 2) ** 2) / (np.pi * (Sn / 2) ** 2) < 0.02
+
+
+def _sdc_python_loops(traj, N, os_factor, iters, kw):
+    """estimate_dcw written out with explicit loops (small cases only)."""
+    import math
+    R = float(np.float32(0.96960938) * np.float32(kw))
+    pad = 2 * math.ceil(R)
+    mos = [((int(np.float32(n) * np.float32(os_factor)) + 31) // 32) * 32 for n in N]
+    D = len(N)
+    pos = []
+    for k in traj:
+        pos.append([float(np.float32(np.float64(k[d]) * mos[d] + ((mos[d] + pad) >> 1)) - np.float32(pad // 2))
+                    for d in range(D)])
+
+    def taps(s):
+        rng = [range(math.ceil(s[d] - R), math.floor(s[d] + R) + 1) for d in range(D)]
+        out = []
+        for cy in (rng[1] if D > 1 else [0]):
+            for cx in rng[0]:
+                c = [cx, cy][:D]
+                ad = [abs(s[d] - c[d]) for d in range(D)]
+                w = float(O.jinc_weight(np.array(ad, np.float32), R))
+                idx = 0
+                for d in range(D - 1, -1, -1):
+                    idx = idx * mos[d] + (c[d] % mos[d])
+                out.append((idx, w))
+        return out
+    T = [taps(s) for s in pos]
+    w = [1.0] * len(traj)
+    for _ in range(iters):
+        grid = {}
+        for j, tj in enumerate(T):
+            for idx, wt in tj:
+                grid[idx] = grid.get(idx, 0.0) + wt * w[j]
+        t = [sum(wt * grid.get(idx, 0.0) for idx, wt in tj) for tj in T]
+        w = [0.0 if t[j] == 0 else w[j] / t[j] for j in range(len(w))]
+    return np.array(w)
+
+
+def test_sdc_restatement_matches_python_loops():
+    rng = np.random.default_rng(3)
+    traj = rng.uniform(-0.5, 0.5, (40, 2)).astype(np.float32)
+    traj[0] = 0.0                      # a sample on a cell centre
+    traj[1] = [0.4999, -0.5]           # samples at the wrap
+    ref = _sdc_python_loops(traj, (32, 32), 2.0, 3, 4.0)
+    np.testing.assert_allclose(O.estimate_dcw(traj, (32, 32), 2.0, 3, 4.0), ref, rtol=1e-12)
+
+
+def test_sdc_converges_towards_fixed_point():
+    """The estimate drives C2NC(NC2C(w)) towards 1 (SDC.hpp:62-77)."""
+    traj = S.radial_golden_angle_2d(32, 128).astype(np.float32)
+    r0 = O.sdc_fixed_point_residual(traj, (64, 64), 2.0, 5.5, np.ones(traj.shape[0]))
+    r10 = O.sdc_fixed_point_residual(traj, (64, 64), 2.0, 5.5, O.estimate_dcw(traj, (64, 64), 2.0, 10, 5.5))
+    r30 = O.sdc_fixed_point_residual(traj, (64, 64), 2.0, 5.5, O.estimate_dcw(traj, (64, 64), 2.0, 30, 5.5))
+    assert r0 > 10 and r10 < 0.1 and r30 < r10
+    # radial density: the estimate grows with |k| away from the centre
+    w = O.estimate_dcw(traj, (64, 64), 2.0, 10, 5.5).reshape(32, 128)
+    assert w[:, 64 + 40].mean() > 5 * w[:, 64 + 4].mean()
+
+
+def test_jinc_weight_shape():
+    R = np.float32(0.96960938) * np.float32(5.5)
+    assert abs(O.jinc_weight(np.zeros((1, 2), np.float32), R)[0] - 0.999923599661866) < 1e-6
+    assert O.jinc_weight(np.array([[R * 0.97, 0.0]], np.float32), R)[0] == 0.0    # r >= 0.9696 -> 0
+    assert O.jinc_weight(np.array([[R + 0.1, 0.0]], np.float32), R)[0] == 0.0
