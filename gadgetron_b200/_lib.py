@@ -96,6 +96,16 @@ def _load():
         "gb_radial_dcw_golden_ratio_2d": (i32, [u32, u32, f32, f32, u32, i32, P, P]),
         "gb_radial_dcw_fixed_angle_2d": (i32, [u32, u32, f32, f32, P, P]),
         "gb_sdc_estimate_dcw": (i32, [i32, P, f32, u32, f32, P, u64, P, P, P]),
+        "gb_sense_buffer_create": (i32, [P]),
+        "gb_sense_buffer_destroy": (i32, [P]),
+        "gb_sense_buffer_setup": (i32, [P, i32, P, P, f32, u32, u32, u32, P]),
+        "gb_sense_buffer_clear": (i32, [P, P]),
+        "gb_sense_buffer_set_dcw": (i32, [P, P]),
+        "gb_sense_buffer_set_csm": (i32, [P, P]),
+        "gb_sense_buffer_add_frame_data": (i32, [P, P, P, u64, P, P]),
+        "gb_sense_buffer_get_accumulated_coil_images": (i32, [P, P, P]),
+        "gb_sense_buffer_get_combined_coil_image": (i32, [P, P, P]),
+        "gb_sense_buffer_get_normalization_factor": (i32, [P, P]),
         "gb_cg_set_refinements": (i32, [P, u32]),
         "gb_cg_set_use_graph": (i32, [P, i32]),
         "gb_cg_set_frame_independent": (i32, [P, i32]),
@@ -120,7 +130,11 @@ EXPORTED = (
     "gb_cg_set_refinements gb_cg_set_use_graph gb_cg_set_frame_independent gb_cg_solve "
     "gb_cg_set_image_regularization gb_image_operator_compute gb_sense_precond_weights "
     "gb_radial_trajectory_golden_ratio_2d gb_radial_trajectory_fixed_angle_2d gb_radial_trajectory_variable_angle_2d "
-    "gb_radial_dcw_golden_ratio_2d gb_radial_dcw_fixed_angle_2d gb_sdc_estimate_dcw").split()
+    "gb_radial_dcw_golden_ratio_2d gb_radial_dcw_fixed_angle_2d gb_sdc_estimate_dcw "
+    "gb_sense_buffer_create gb_sense_buffer_destroy gb_sense_buffer_setup gb_sense_buffer_clear "
+    "gb_sense_buffer_set_dcw gb_sense_buffer_set_csm gb_sense_buffer_add_frame_data "
+    "gb_sense_buffer_get_accumulated_coil_images gb_sense_buffer_get_combined_coil_image "
+    "gb_sense_buffer_get_normalization_factor").split()
 
 
 def check(status: int):

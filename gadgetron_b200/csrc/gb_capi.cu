@@ -92,6 +92,9 @@ struct gb_sense_op_s {
 struct gb_cg_solver_s {
     CgSolver c;
 };
+struct gb_sense_buffer_s {
+    SenseBuffer b;
+};
 
 namespace gb {
 NufftPlan *plan_from_handle(gb_nufft_plan h) { return h ? h->p : nullptr; }
@@ -125,15 +128,6 @@ GB_API const char *gb_version(void) { return "gadgetron_b200 0.1 (sm_100a)"; }
 
 GB_API uint64_t gb_kernel_launch_count(void) { return launch_count(); }
 
-static void default_tiling(NufftPlan &p) {
-    int t[3] = {16, 16, 1};
-    if (p.D == 1) { t[0] = 256; }
-    if (p.D == 3) { t[0] = 8; t[1] = 8; t[2] = 8; }
-    // shrink for small grids while keeping >= 256 cells per tile
-    for (int d = 0; d < p.D; d++)
-        if (t[d] > p.kp.mos[d]) t[d] = (int)p.kp.mos[d];
-    plan_set_tiling(p, t, 16);
-}
 
 GB_API gb_status gb_nufft_plan_create(int D, const uint64_t *matrix_size, const uint64_t *matrix_size_os,
                                       float W, uint32_t flags, gb_nufft_plan *plan) {
@@ -145,7 +139,7 @@ GB_API gb_status gb_nufft_plan_create(int D, const uint64_t *matrix_size, const 
         h->p = h->owned.get();
         try {
             plan_init(*h->p, D, matrix_size, matrix_size_os, W, flags);
-            default_tiling(*h->p);
+            plan_default_tiling(*h->p);
         } catch (...) {
             delete h;
             throw;
@@ -317,7 +311,7 @@ GB_API gb_status gb_sense_create(int D, const uint64_t *matrix_size, const uint6
         auto *h = new gb_sense_op_s();
         try {
             plan_init(h->s.plan, D, matrix_size, matrix_size_os, W, flags);
-            default_tiling(h->s.plan);
+            plan_default_tiling(h->s.plan);
         } catch (...) {
             delete h;
             throw;
@@ -521,6 +515,80 @@ GB_API gb_status gb_radial_dcw_fixed_angle_2d(uint32_t samples_per_profile, uint
     return guarded([&] {
         radial_dcw(dcw, (int)samples_per_profile, (int)profiles, alpha, one_over_radial_oversampling, 0, false, 1,
                    S(stream));
+    });
+}
+
+GB_API gb_status gb_sense_buffer_create(gb_sense_buffer *buffer) {
+    return guarded([&] {
+        if (!buffer) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer pointer");
+        *buffer = new gb_sense_buffer_s();
+    });
+}
+
+GB_API gb_status gb_sense_buffer_destroy(gb_sense_buffer buffer) {
+    return guarded([&] { delete buffer; });
+}
+
+GB_API gb_status gb_sense_buffer_setup(gb_sense_buffer buffer, int D, const uint64_t *matrix_size,
+                                       const uint64_t *matrix_size_os, float W, uint32_t num_coils,
+                                       uint32_t num_cycles, uint32_t num_sub_cycles, void *stream) {
+    return guarded([&] {
+        if (!buffer) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer");
+        buffer->b.setup(D, matrix_size, matrix_size_os, W, (int)num_coils, (int)num_cycles, (int)num_sub_cycles,
+                        S(stream));
+    });
+}
+
+GB_API gb_status gb_sense_buffer_clear(gb_sense_buffer buffer, void *stream) {
+    return guarded([&] {
+        if (!buffer) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer");
+        buffer->b.clear(S(stream));
+    });
+}
+
+GB_API gb_status gb_sense_buffer_set_dcw(gb_sense_buffer buffer, const float *dcw) {
+    return guarded([&] {
+        if (!buffer) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer");
+        buffer->b.dcw = dcw;
+    });
+}
+
+GB_API gb_status gb_sense_buffer_set_csm(gb_sense_buffer buffer, const void *csm) {
+    return guarded([&] {
+        if (!buffer) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer");
+        buffer->b.csm = static_cast<const float2 *>(csm);
+    });
+}
+
+GB_API gb_status gb_sense_buffer_add_frame_data(gb_sense_buffer buffer, const void *samples, const float *trajectory,
+                                                uint64_t num_samples, int *cycle_completed, void *stream) {
+    return guarded([&] {
+        if (!buffer) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer");
+        const bool c = buffer->b.add_frame_data(static_cast<const float2 *>(samples), trajectory,
+                                                (int64_t)num_samples, S(stream));
+        if (cycle_completed) *cycle_completed = c ? 1 : 0;
+    });
+}
+
+GB_API gb_status gb_sense_buffer_get_accumulated_coil_images(gb_sense_buffer buffer, void *images, void *stream) {
+    return guarded([&] {
+        if (!buffer || !images) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer or images");
+        buffer->b.accumulated_coil_images(static_cast<float2 *>(images), S(stream));
+    });
+}
+
+GB_API gb_status gb_sense_buffer_get_combined_coil_image(gb_sense_buffer buffer, void *image, void *stream) {
+    return guarded([&] {
+        if (!buffer || !image) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer or image");
+        buffer->b.combined_coil_image(static_cast<float2 *>(image), S(stream));
+    });
+}
+
+GB_API gb_status gb_sense_buffer_get_normalization_factor(gb_sense_buffer buffer, float *factor) {
+    return guarded([&] {
+        if (!buffer || !factor) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer or factor");
+        if (buffer->b.cycle_length < 2) fail(GB_ERR_INVALID_ARGUMENT, "cuBuffer: setup has not been called");
+        *factor = 1.f / (((float)buffer->b.cycle_length - 1.f) * (float)buffer->b.sub_cycle_length);
     });
 }
 

@@ -291,6 +291,8 @@ void fft_cols(NufftPlan &p, int n, const float2 *in, float2 *out, int64_t ncols,
 void fft_rows(NufftPlan &p, int n, const float2 *in, float2 *out, int64_t nrows, int64_t rpp, int64_t row_off,
               int64_t pstride, int in_lo, int in_hi, int out_lo, int out_hi, bool inverse, cudaStream_t st);
 void plan_set_tiling(NufftPlan &p, const int *tile, int cg);
+// The tiling a new plan starts with (16 x 16 in 2D, 8^3 in 3D, coil group 16).
+void plan_default_tiling(NufftPlan &p);
 // Hash of every buffer address and count the convolution kernels' launches
 // depend on: equal signatures mean a captured graph is still valid.
 uint64_t plan_layout_signature(const NufftPlan &p, int nbf);

@@ -2,6 +2,8 @@
 // plus the NUFFT operation entry points used by the ABI layer.
 #pragma once
 
+#include <memory>
+
 #include "gb_internal.cuh"
 
 namespace gb {
@@ -89,6 +91,24 @@ void nufft_traj_grad(NufftPlan &p, const float2 *img, const float2 *weights, con
                      int nb, cudaStream_t st);
 void nufft_traj_grad_from_grid(NufftPlan &p, const float2 *grid, const float2 *weights, float *grad, int nb,
                                cudaStream_t st);
+
+// Cyclic k-space accumulation buffer (cuBuffer / cuSenseBuffer, gb_buffer.cu).
+struct SenseBuffer {
+    std::unique_ptr<NufftPlan> plan;
+    int D = 0, coils = 0, cycle_length = 0, sub_cycle_length = 0;
+    int cur_idx = 0, cur_sub_idx = 0;
+    bool acc_empty = true;
+    bool has_acc_image = false;   // the last accumulated coil images (reused by the combined image)
+    const float *dcw = nullptr;   // retained
+    const float2 *csm = nullptr;  // retained
+    DevBuf<float2> acc, cyc, scaled, work, acc_image;
+    void setup(int D, const uint64_t *N, const uint64_t *mos, float W, int coils, int num_cycles,
+               int num_sub_cycles, cudaStream_t st);
+    void clear(cudaStream_t st);
+    bool add_frame_data(const float2 *samples, const float *traj, int64_t M, cudaStream_t st);
+    void accumulated_coil_images(float2 *out, cudaStream_t st);
+    void combined_coil_image(float2 *out, cudaStream_t st);
+};
 
 // Gridding with caller-provided scratch (no device allocation).
 void grid_scratch_need(const NufftPlan &p, int nb, size_t *partial_elems, size_t *counter_elems);

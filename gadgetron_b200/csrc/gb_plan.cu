@@ -600,6 +600,17 @@ uint64_t plan_layout_signature(const NufftPlan &p, int nbf) {
     return h;
 }
 
+// The tiling a new plan starts with: 16 x 16 (2D), 256 (1D), 8^3 (3D),
+// shrunk to the grid for small grids; coil group 16.
+void plan_default_tiling(NufftPlan &p) {
+    int t[3] = {16, 16, 1};
+    if (p.D == 1) { t[0] = 256; }
+    if (p.D == 3) { t[0] = 8; t[1] = 8; t[2] = 8; }
+    for (int d = 0; d < p.D; d++)
+        if (t[d] > p.kp.mos[d]) t[d] = (int)p.kp.mos[d];
+    plan_set_tiling(p, t, 16);
+}
+
 // Validates and installs a tiling (tile shape and coil group).
 void plan_set_tiling(NufftPlan &p, const int *tile, int cg) {
     const KParams &k = p.kp;

@@ -79,6 +79,7 @@ typedef enum gb_fft_mode { GB_FFT_FORWARDS = 0, GB_FFT_BACKWARDS = 1 } gb_fft_mo
 typedef struct gb_nufft_plan_s *gb_nufft_plan;
 typedef struct gb_sense_op_s *gb_sense_op;
 typedef struct gb_cg_solver_s *gb_cg_solver;
+typedef struct gb_sense_buffer_s *gb_sense_buffer;
 
 GB_API const char *gb_last_error_message(void);
 GB_API const char *gb_version(void);
@@ -328,6 +329,34 @@ GB_API gb_status gb_radial_dcw_golden_ratio_2d(uint32_t samples_per_profile, uin
                                                float *dcw, void *stream);
 GB_API gb_status gb_radial_dcw_fixed_angle_2d(uint32_t samples_per_profile, uint32_t profiles, float alpha,
                                               float one_over_radial_oversampling, float *dcw, void *stream);
+
+/* ------------------------------------------------------ SENSE buffer --- */
+
+/* cuSenseBuffer<float, D> (toolboxes/mri/pmri/gpu/cuSenseBuffer.h,
+ * cuBuffer.h:13-57): a cycle of num_cycles + 1 oversampled k-space slots
+ * [coils][mos...] filled by gridding (NC2C, accumulating) num_sub_cycles
+ * frames each, and a running sum of the last num_cycles complete slots.
+ * setup allocates and clears (cuBuffer::setup); the dcw and csm pointers are
+ * retained.  add_frame_data: samples [coils][M] complex64, trajectory [M][D]
+ * floats (device); *cycle_completed (may be NULL) = 1 when a slot completed
+ * (cuBuffer::add_frame_data).  get_accumulated_coil_images: [coils][N...]
+ * (centred backward FFT, deapodization, crop of the running sum; ones while
+ * no slot has completed).  get_combined_coil_image: [N...] = sum_c
+ * conj(csm_c) x the last accumulated coil images.  Normalisation factor
+ * 1 / (num_cycles * num_sub_cycles) (cuBuffer::get_normalization_factor). */
+GB_API gb_status gb_sense_buffer_create(gb_sense_buffer *buffer);
+GB_API gb_status gb_sense_buffer_destroy(gb_sense_buffer buffer);
+GB_API gb_status gb_sense_buffer_setup(gb_sense_buffer buffer, int D, const uint64_t *matrix_size,
+                                       const uint64_t *matrix_size_os, float W, uint32_t num_coils,
+                                       uint32_t num_cycles, uint32_t num_sub_cycles, void *stream);
+GB_API gb_status gb_sense_buffer_clear(gb_sense_buffer buffer, void *stream);
+GB_API gb_status gb_sense_buffer_set_dcw(gb_sense_buffer buffer, const float *dcw);
+GB_API gb_status gb_sense_buffer_set_csm(gb_sense_buffer buffer, const void *csm);
+GB_API gb_status gb_sense_buffer_add_frame_data(gb_sense_buffer buffer, const void *samples, const float *trajectory,
+                                                uint64_t num_samples, int *cycle_completed, void *stream);
+GB_API gb_status gb_sense_buffer_get_accumulated_coil_images(gb_sense_buffer buffer, void *images, void *stream);
+GB_API gb_status gb_sense_buffer_get_combined_coil_image(gb_sense_buffer buffer, void *image, void *stream);
+GB_API gb_status gb_sense_buffer_get_normalization_factor(gb_sense_buffer buffer, float *factor);
 
 /* estimate_dcw (toolboxes/mri/sdc/SDC.hpp:19-80, gpu/cuSDC.cu): iterative
  * density compensation with the Jinc kernel of width kernel_width (radius

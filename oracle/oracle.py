@@ -36,6 +36,8 @@ cuNonCartesianSenseOperator and cgSolver) on the CPU:
   ``toolboxes/core/gpu/radial_utilities.cu:18-441``;
 * the density compensation estimate follows ``toolboxes/mri/sdc/SDC.hpp:19-80``
   with the Jinc kernel of ``toolboxes/nfft/ConvolutionKernel.hpp:307-397``;
+* the SENSE accumulation buffer follows ``toolboxes/mri/pmri/gpu/cuBuffer.cpp:7-166``
+  and ``cuSenseBuffer.cpp:18-35``;
 * the image regulariser follows ``toolboxes/operators/imageOperator.h:27-67``
   and its offset estimate ``toolboxes/operators/gpu/cuImageOperator.h:35-62``;
   the preconditioner weights follow ``gadgets/pmri/gpuCgSenseGadget.cpp:167-176``.
@@ -602,6 +604,61 @@ def radial_dcw_2d(S: int, P: int, alpha: float, ovs: float, profile_offset: int 
         w[S // 2] = f32(f32(r * r) * _PI32) / f32(P)
         out[p] = w
     return out.reshape(-1)
+
+
+# ------------------------------------------------------- SENSE buffer -------
+
+class OracleSenseBuffer:
+    """cuBuffer / cuSenseBuffer (cuBuffer.cpp:7-166, cuSenseBuffer.cpp:18-35):
+    num_cycles + 1 oversampled k-space slots; every frame is gridded (NC2C,
+    accumulating) into the current slot; after num_sub_cycles frames the slot
+    is added to the running sum and the next slot is subtracted and cleared."""
+
+    def __init__(self, N, mos, W, num_coils, num_cycles, num_sub_cycles):
+        self.N, self.mos, self.W = tuple(N), tuple(mos), W
+        self.C = num_coils
+        self.cycle_length = num_cycles + 1
+        self.sub_cycle_length = num_sub_cycles
+        self.acc = np.zeros((self.C, 1) + self.mos[::-1], np.complex128)
+        self.cyc = np.zeros((self.cycle_length,) + self.acc.shape, np.complex128)
+        self.cur_idx = self.cur_sub_idx = 0
+        self.acc_empty = True
+        self.dcw = None
+        self.acc_image = None
+
+    def add_frame_data(self, samples, traj) -> bool:
+        plan = OraclePlan(self.N, self.mos, self.W)
+        D = len(self.N)
+        plan.preprocess(np.asarray(traj, np.float32).reshape(1, -1, D))
+        s = np.asarray(samples, np.complex128).reshape(self.C, 1, -1)
+        if self.dcw is not None:
+            s = s * np.asarray(self.dcw, np.float64).reshape(1, 1, -1)
+        self.cyc[self.cur_idx] = plan.convolve_nc2c(s, accumulate_into=self.cyc[self.cur_idx])
+        done = False
+        if self.cur_sub_idx == self.sub_cycle_length - 1:
+            done = True
+            self.acc = self.acc + self.cyc[self.cur_idx]
+            self.acc_empty = False
+            self.cur_idx = (self.cur_idx + 1) % self.cycle_length
+            self.acc = self.acc - self.cyc[self.cur_idx]
+            self.cyc[self.cur_idx] = 0
+        self.cur_sub_idx = (self.cur_sub_idx + 1) % self.sub_cycle_length
+        return done
+
+    def get_accumulated_coil_images(self):
+        D = len(self.N)
+        if self.acc_empty:
+            self.acc_image = np.ones((self.C,) + self.N[::-1], np.complex128)
+        else:
+            plan = OraclePlan(self.N, self.mos, self.W)
+            img = plan.deapodize(plan.fft(self.acc, forward=False, do_scale=True))
+            self.acc_image = crop(img, self.N, D)[:, 0]
+        return self.acc_image
+
+    def get_combined_coil_image(self, csm):
+        if self.acc_image is None:
+            self.get_accumulated_coil_images()
+        return np.sum(np.conj(np.asarray(csm, np.complex128)) * self.acc_image, axis=0)
 
 
 # ------------------------------------------------- density compensation -----

@@ -341,3 +341,28 @@ def test_jinc_weight_shape():
     assert abs(O.jinc_weight(np.zeros((1, 2), np.float32), R)[0] - 0.999923599661866) < 1e-6
     assert O.jinc_weight(np.array([[R * 0.97, 0.0]], np.float32), R)[0] == 0.0    # r >= 0.9696 -> 0
     assert O.jinc_weight(np.array([[R + 0.1, 0.0]], np.float32), R)[0] == 0.0
+
+
+def test_sense_buffer_running_sum_is_last_cycles():
+    """cuBuffer (cuBuffer.cpp:63-134): after each completed slot the running
+    sum is the gridded data of exactly the last num_cycles slots."""
+    N, mos, W, C = (32, 32), (64, 64), 5.5, 2
+    buf = O.OracleSenseBuffer(N, mos, W, C, num_cycles=2, num_sub_cycles=2)
+    rng = np.random.default_rng(9)
+    frames = []
+    for f in range(7):
+        t = S.radial_golden_angle_2d(8, 64, profile_offset=8 * f).astype(np.float32)
+        y = rng.standard_normal((C, t.shape[0])) + 1j * rng.standard_normal((C, t.shape[0]))
+        frames.append((t, y))
+    assert np.all(buf.get_accumulated_coil_images() == 1)
+
+    def gridded(fs):
+        out = np.zeros((C, 1) + mos[::-1], np.complex128)
+        for t, y in fs:
+            P = O.OraclePlan(N, mos, W)
+            P.preprocess(t.reshape(1, -1, 2))
+            out = P.convolve_nc2c(y.reshape(C, 1, -1), accumulate_into=out)
+        return out
+    done = [buf.add_frame_data(y, t) for t, y in frames]
+    assert done == [False, True, False, True, False, True, False]
+    np.testing.assert_allclose(buf.acc, gridded(frames[2:6]), rtol=1e-12, atol=1e-12)
