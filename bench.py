@@ -813,6 +813,17 @@ def run_regularized(args):
     t0 = time.perf_counter()
     w_sdc_o = O.estimate_dcw(wl["traj"], N, 2.0, 10, 5.5)
     sdc_cpu_ms = (time.perf_counter() - t0) * 1e3
+    # coil sensitivities from the coil images of the workload's phantom
+    from gadgetron_b200 import b1map as B1
+    rng_b1 = np.random.default_rng(12)
+    coil_np = (wl["csm"] * wl["phantom"] + 0.01 * (rng_b1.standard_normal(wl["csm"].shape) +
+                                                   1j * rng_b1.standard_normal(wl["csm"].shape))).astype(np.complex64)
+    coil_d = torch.from_numpy(coil_np).to(dev)
+    b1_ms = _timed(lambda: B1.estimate_b1_map(coil_d, 2), max(2, args.steps // 5), 1, None, stream)
+    b1_d = B1.estimate_b1_map(coil_d, 2)
+    t0 = time.perf_counter()
+    b1_o = O.estimate_b1_map(coil_np, 2)
+    b1_cpu_ms = (time.perf_counter() - t0) * 1e3
     R.set_weight(kappa)
     cg = gb.cuCgSolver()
     cg.set_encoding_operator(E)
@@ -846,6 +857,8 @@ def run_regularized(args):
         "cpu_oracle_ms_dcw_96x512": round(gen_cpu_ms, 1),
         "sdc_ms_96x512_os2_10it": round(sdc_ms, 3), "cpu_oracle_ms_sdc": round(sdc_cpu_ms, 1),
         "sdc_rel_l2_vs_oracle": O.rel_l2(w_sdc.cpu().numpy(), w_sdc_o),
+        "b1_map_ms_256x256x16": round(b1_ms, 3), "cpu_oracle_ms_b1_map": round(b1_cpu_ms, 1),
+        "b1_map_rel_l2_vs_oracle": O.rel_l2(b1_d.cpu().numpy(), b1_o),
         "regulariser_offset": R.offset_, "regulariser_offset_oracle": off_o,
         "recon_rel_l2_vs_oracle_fp64_cg": O.rel_l2(x.cpu().numpy(), xr),
         "gpu_launches": int(launches),

@@ -11,7 +11,7 @@ from .nfft import (NFFT, ConvolutionType, NFFT_comp_mode, NFFT_conv_mode, NFFT_f
 from .sense import cuNonCartesianSenseOperator  # noqa: F401
 from .solvers import cuCgSolver  # noqa: F401
 from .operators import cuCgPreconditioner, cuImageOperator, sense_precond_weights  # noqa: F401
-from . import radial, sdc  # noqa: F401
+from . import b1map, radial, sdc  # noqa: F401
 from .buffers import cuSenseBuffer  # noqa: F401
 
 __version__ = "0.1.0"

@@ -96,6 +96,7 @@ def _load():
         "gb_radial_dcw_golden_ratio_2d": (i32, [u32, u32, f32, f32, u32, i32, P, P]),
         "gb_radial_dcw_fixed_angle_2d": (i32, [u32, u32, f32, f32, P, P]),
         "gb_sdc_estimate_dcw": (i32, [i32, P, f32, u32, f32, P, u64, P, P, P]),
+        "gb_estimate_b1_map": (i32, [i32, P, u32, i32, P, P, P]),
         "gb_sense_buffer_create": (i32, [P]),
         "gb_sense_buffer_destroy": (i32, [P]),
         "gb_sense_buffer_setup": (i32, [P, i32, P, P, f32, u32, u32, u32, P]),
@@ -134,7 +135,7 @@ EXPORTED = (
     "gb_sense_buffer_create gb_sense_buffer_destroy gb_sense_buffer_setup gb_sense_buffer_clear "
     "gb_sense_buffer_set_dcw gb_sense_buffer_set_csm gb_sense_buffer_add_frame_data "
     "gb_sense_buffer_get_accumulated_coil_images gb_sense_buffer_get_combined_coil_image "
-    "gb_sense_buffer_get_normalization_factor").split()
+    "gb_sense_buffer_get_normalization_factor gb_estimate_b1_map").split()
 
 
 def check(status: int):

@@ -592,6 +592,14 @@ GB_API gb_status gb_sense_buffer_get_normalization_factor(gb_sense_buffer buffer
     });
 }
 
+GB_API gb_status gb_estimate_b1_map(int D, const uint64_t *image_size, uint32_t num_coils, int target_coils,
+                                    const void *coil_images, void *csm, void *stream) {
+    return guarded([&] {
+        estimate_b1_map(D, image_size, (int)num_coils, target_coils, static_cast<const float2 *>(coil_images),
+                        static_cast<float2 *>(csm), S(stream));
+    });
+}
+
 GB_API gb_status gb_sdc_estimate_dcw(int D, const uint64_t *matrix_size, float os_factor, uint32_t num_iterations,
                                      float kernel_width, const float *trajectory, uint64_t num_samples,
                                      const float *initial_dcw, float *dcw, void *stream) {

@@ -444,4 +444,8 @@ void radial_dcw(float *dcw, int S, int P, float alpha, float ovs, int profile_of
 void sdc_estimate_dcw(int D, const uint64_t *N, float os_factor, int iterations, float kernel_width,
                       const float *traj, int64_t M, const float *initial, float *dcw, cudaStream_t st);
 
+// Coil sensitivity estimation from coil images [ncoils][dims] (gb_b1map.cu).
+void estimate_b1_map(int D, const uint64_t *dims, int ncoils, int target_coils, const float2 *images, float2 *csm,
+                     cudaStream_t st);
+
 }  // namespace gb

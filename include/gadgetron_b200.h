@@ -358,6 +358,17 @@ GB_API gb_status gb_sense_buffer_get_accumulated_coil_images(gb_sense_buffer buf
 GB_API gb_status gb_sense_buffer_get_combined_coil_image(gb_sense_buffer buffer, void *image, void *stream);
 GB_API gb_status gb_sense_buffer_get_normalization_factor(gb_sense_buffer buffer, float *factor);
 
+/* estimate_b1_map<float, D> (toolboxes/mri/pmri/gpu/b1_map.h:14-20,
+ * b1_map.cu:29-118): coil sensitivities from coil images
+ * [num_coils][image_size...] complex64 (device): RSS normalisation over the
+ * first target_coils coils (all when target_coils <= 0 or larger), per-pixel
+ * coil correlation matrices smoothed over a 7^D box (zero outside the
+ * image), dominant eigenvector by two power iterations, phase of coil 0 set
+ * to zero.  csm: [target][image_size...] complex64 (device); at most 32
+ * target coils.  Synchronises. */
+GB_API gb_status gb_estimate_b1_map(int D, const uint64_t *image_size, uint32_t num_coils, int target_coils,
+                                    const void *coil_images, void *csm, void *stream);
+
 /* estimate_dcw (toolboxes/mri/sdc/SDC.hpp:19-80, gpu/cuSDC.cu): iterative
  * density compensation with the Jinc kernel of width kernel_width (radius
  * 0.9696 * kernel_width) on a grid of round_up_32(N * os_factor) cells per

@@ -38,6 +38,9 @@ cuNonCartesianSenseOperator and cgSolver) on the CPU:
   with the Jinc kernel of ``toolboxes/nfft/ConvolutionKernel.hpp:307-397``;
 * the SENSE accumulation buffer follows ``toolboxes/mri/pmri/gpu/cuBuffer.cpp:7-166``
   and ``cuSenseBuffer.cpp:18-35``;
+* the coil sensitivity estimate follows ``toolboxes/mri/pmri/gpu/b1_map.cu:29-118``
+  (RSS normalisation, correlation matrices, 7^D box smoothing, two power
+  iterations, coil-0 phase reference);
 * the image regulariser follows ``toolboxes/operators/imageOperator.h:27-67``
   and its offset estimate ``toolboxes/operators/gpu/cuImageOperator.h:35-62``;
   the preconditioner weights follow ``gadgets/pmri/gpuCgSenseGadget.cpp:167-176``.
@@ -604,6 +607,36 @@ def radial_dcw_2d(S: int, P: int, alpha: float, ovs: float, profile_offset: int 
         w[S // 2] = f32(f32(r * r) * _PI32) / f32(P)
         out[p] = w
     return out.reshape(-1)
+
+
+# ------------------------------------------------------- b1 map -------------
+
+def estimate_b1_map(coil_images: np.ndarray, D: int, target_coils: int = -1) -> np.ndarray:
+    """estimate_b1_map (b1_map.cu:29-118) in FP64: coil_images [C, *image]
+    (x last).  RSS-normalise the first target coils, correlation matrices
+    A[a][b] = x_b conj(x_a), 7^D box smoothing with zeros outside the image
+    (scaled by 1/7^D), two power iterations t_j = sum_k A[k][j] b_k from
+    b = 1, then b_c * exp(-i arg b_0)."""
+    x = np.asarray(coil_images, np.complex128)
+    C = x.shape[0]
+    nt = C if (target_coils <= 0 or target_coils > C) else target_coils
+    x = x[:nt]
+    x = x / np.sqrt(np.sum(np.abs(x) ** 2, axis=0))[None]
+    A = x[None, :] * np.conj(x[:, None])                 # A[a, b] = x_b conj(x_a)
+    for ax in range(2, 2 + D):                           # separable 7-box, zero padded
+        n = A.shape[ax]
+        pad = [(0, 0)] * A.ndim
+        pad[ax] = (3, 3)
+        P = np.pad(A, pad)
+        c = np.cumsum(P, axis=ax)
+        c = np.concatenate([np.zeros_like(np.take(c, [0], axis=ax)), c], axis=ax)
+        A = np.take(c, np.arange(7, n + 7), axis=ax) - np.take(c, np.arange(0, n), axis=ax)
+    A = A / 7.0 ** D
+    b = np.ones((nt,) + x.shape[1:], np.complex128)
+    for _ in range(2):
+        t = np.einsum("kj...,k...->j...", A, b)
+        b = t / np.sqrt(np.sum(np.abs(t) ** 2, axis=0))[None]
+    return b * np.exp(-1j * np.angle(b[0]))[None]
 
 
 # ------------------------------------------------------- SENSE buffer -------

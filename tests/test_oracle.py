@@ -366,3 +366,50 @@ def test_sense_buffer_running_sum_is_last_cycles():
     done = [buf.add_frame_data(y, t) for t, y in frames]
     assert done == [False, True, False, True, False, True, False]
     np.testing.assert_allclose(buf.acc, gridded(frames[2:6]), rtol=1e-12, atol=1e-12)
+
+
+def test_b1_map_recovers_uniform_sensitivities():
+    """estimate_b1_map (b1_map.cu:29-118): with spatially constant coil
+    sensitivities s the correlation matrices are rank one and the estimate is
+    s / |s| with coil 0 made real, at every pixel."""
+    rng = np.random.default_rng(4)
+    s = rng.standard_normal(6) + 1j * rng.standard_normal(6)
+    rho = 1.0 + rng.uniform(0, 1, (20, 24))
+    imgs = s[:, None, None] * rho[None]
+    est = O.estimate_b1_map(imgs, 2)
+    exp = s / np.linalg.norm(s) * np.exp(-1j * np.angle(s[0]))
+    np.testing.assert_allclose(est, np.broadcast_to(exp[:, None, None], est.shape), atol=1e-12)
+    np.testing.assert_allclose(O.estimate_b1_map(imgs, 2, target_coils=3)[:, 5, 5],
+                               s[:3] / np.linalg.norm(s[:3]) * np.exp(-1j * np.angle(s[0])), atol=1e-12)
+
+
+def test_b1_map_box_smoothing_zero_padded():
+    """The 7-box of the smoothing counts cells outside the image as zero."""
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((2, 9, 11)) + 1j * rng.standard_normal((2, 9, 11))
+    xn = x / np.sqrt(np.sum(np.abs(x) ** 2, axis=0))[None]
+    a01 = xn[1] * np.conj(xn[0])
+    ref = np.zeros_like(a01)
+    for y in range(9):
+        for xx in range(11):
+            ref[y, xx] = a01[max(0, y - 3):y + 4, max(0, xx - 3):xx + 4].sum() / 49.0
+    # one power iteration from b = 1 with two coils: t_1 = A[0][1] + A[1][1]
+    A00 = np.abs(xn[0]) ** 2
+    A11 = np.abs(xn[1]) ** 2
+
+    def box(a):
+        out = np.zeros_like(a)
+        for y in range(9):
+            for xx in range(11):
+                out[y, xx] = a[max(0, y - 3):y + 4, max(0, xx - 3):xx + 4].sum() / 49.0
+        return out
+    S00, S11, S01 = box(A00), box(A11), ref
+    # A[k][j]: A[0][1] = x_1 conj(x_0) = S01, A[1][0] = conj(S01)
+    b = np.ones((2, 9, 11), complex)
+    for _ in range(2):
+        t0 = S00 * b[0] + np.conj(S01) * b[1]
+        t1 = S01 * b[0] + S11 * b[1]
+        nrm = np.sqrt(np.abs(t0) ** 2 + np.abs(t1) ** 2)
+        b = np.stack([t0 / nrm, t1 / nrm])
+    b = b * np.exp(-1j * np.angle(b[0]))[None]
+    np.testing.assert_allclose(O.estimate_b1_map(x, 2), b, atol=1e-12)
