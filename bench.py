@@ -641,6 +641,7 @@ def run_batched(args):
     E.set_dcw(sq_d)
     E.preprocess(torch.from_numpy(traj).to(dev), frame_offsets=offs)
     E.autotune()   # tile shape and coil group for this trajectory set
+    tiling = E.get_plan().get_tiling()
     y = torch.empty((C, offs[-1]), dtype=torch.complex64, device=dev)
     E.mult_M(torch.from_numpy(ph).to(dev), y)
     rms = float(y.abs().pow(2).mean().sqrt())
@@ -693,6 +694,7 @@ def run_batched(args):
                    "coils": C, "samples_total": offs[-1], "iterations": iters, "alpha_W": "chosen: 2.0, 5.5"},
         "plain_per_frame_ms": round(ms_p, 3), "speedup_vs_plain": round(ms_p / ms_b, 2),
         "batched_vs_plain_rel_l2": err, "gpu_launches_per_batch": int(launches),
+        "tiling_after_autotune": {"tile": list(tiling[0]), "coil_group": tiling[1]},
     }
 
 

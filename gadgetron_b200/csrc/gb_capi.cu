@@ -542,6 +542,8 @@ GB_API gb_status gb_sense_buffer_setup(gb_sense_buffer buffer, int D, const uint
 GB_API gb_status gb_sense_buffer_clear(gb_sense_buffer buffer, void *stream) {
     return guarded([&] {
         if (!buffer) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer");
+        if (!buffer->b.plan) fail(GB_ERR_INVALID_ARGUMENT, "cuBuffer: setup has not been called");
+        DeviceGuard g(buffer->b.plan->device);
         buffer->b.clear(S(stream));
     });
 }
@@ -564,6 +566,8 @@ GB_API gb_status gb_sense_buffer_add_frame_data(gb_sense_buffer buffer, const vo
                                                 uint64_t num_samples, int *cycle_completed, void *stream) {
     return guarded([&] {
         if (!buffer) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer");
+        if (!buffer->b.plan) fail(GB_ERR_INVALID_ARGUMENT, "cuBuffer: setup has not been called");
+        DeviceGuard g(buffer->b.plan->device);
         const bool c = buffer->b.add_frame_data(static_cast<const float2 *>(samples), trajectory,
                                                 (int64_t)num_samples, S(stream));
         if (cycle_completed) *cycle_completed = c ? 1 : 0;
@@ -573,6 +577,8 @@ GB_API gb_status gb_sense_buffer_add_frame_data(gb_sense_buffer buffer, const vo
 GB_API gb_status gb_sense_buffer_get_accumulated_coil_images(gb_sense_buffer buffer, void *images, void *stream) {
     return guarded([&] {
         if (!buffer || !images) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer or images");
+        if (!buffer->b.plan) fail(GB_ERR_INVALID_ARGUMENT, "cuBuffer: setup has not been called");
+        DeviceGuard g(buffer->b.plan->device);
         buffer->b.accumulated_coil_images(static_cast<float2 *>(images), S(stream));
     });
 }
@@ -580,6 +586,8 @@ GB_API gb_status gb_sense_buffer_get_accumulated_coil_images(gb_sense_buffer buf
 GB_API gb_status gb_sense_buffer_get_combined_coil_image(gb_sense_buffer buffer, void *image, void *stream) {
     return guarded([&] {
         if (!buffer || !image) fail(GB_ERR_INVALID_ARGUMENT, "NULL buffer or image");
+        if (!buffer->b.plan) fail(GB_ERR_INVALID_ARGUMENT, "cuBuffer: setup has not been called");
+        DeviceGuard g(buffer->b.plan->device);
         buffer->b.combined_coil_image(static_cast<float2 *>(image), S(stream));
     });
 }
