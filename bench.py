@@ -640,7 +640,11 @@ def run_batched(args):
     sq_d = torch.from_numpy(sq).to(dev)
     E.set_dcw(sq_d)
     E.preprocess(torch.from_numpy(traj).to(dev), frame_offsets=offs)
-    E.autotune()   # tile shape and coil group for this trajectory set
+    if getattr(args, "tiling", None):
+        tx, ty, cgr = (int(v) for v in args.tiling.split(","))
+        E.get_plan().set_tiling((tx, ty), cgr)
+    else:
+        E.autotune()   # tile shape and coil group for this trajectory set
     tiling = E.get_plan().get_tiling()
     y = torch.empty((C, offs[-1]), dtype=torch.complex64, device=dev)
     E.mult_M(torch.from_numpy(ph).to(dev), y)
@@ -881,6 +885,9 @@ def main():
                          "(%%d = rank)")
     ap.add_argument("--size", default="full", choices=["full", "small"],
                     help="profiling cases: nufft-3d small = 64^3; batched small = 16 frames")
+    ap.add_argument("--tiling", default=None,
+                    help="batched workload: fixed tile and coil group 'tx,ty,cg' instead of the "
+                         "autotuner's choice (profiling runs, whose launch timings the profiler skews)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
