@@ -584,11 +584,20 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
         z = rem / k.N[1];
         y = rem - z * k.N[1];
     };
+    // The block's rows are blockIdx.x, blockIdx.x + nbx, ...; its threads run
+    // over the (row, column) pairs of all of them, so that every thread has
+    // work when a row is narrower than the block (the host keeps
+    // seg_rows * mos[0] below 2^31).
+    const int n0 = k.N[0];
+    const int my_rows = (int)blockIdx.x < t.seg_rows ? (t.seg_rows - 1 - (int)blockIdx.x) / nbx + 1 : 0;
+    const int my_elems = my_rows * n0;
 
     // Phase 1: q = weight * crop(kg) * conj(csm) summed + kappa p ; <p, q>.
     double2 acc = make_double2(0.0, 0.0);
     if (!was_done) {
-        for (int rr = blockIdx.x; rr < t.seg_rows; rr += nbx) {
+        for (int l = threadIdx.x; l < my_elems; l += blockDim.x) {
+            const int i = l / n0, x = l - i * n0;
+            const int rr = (int)blockIdx.x + i * nbx;
             int f, z, y, rem;
             row_coords(row0 + rr, f, z, y, rem);
             const int gy = y + oy, gz = z + oz;
@@ -596,9 +605,9 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
             if (k.D > 1) fyz = t.deap[t.deap_stride + y];
             if (k.D > 2) fyz *= t.deap[2 * t.deap_stride + z];
             const int64_t grow = (int64_t)gz * t.kl.s_z + (int64_t)gy * t.kl.s_y + ox;
-            const int64_t nrow = (int64_t)rem * k.N[0];
-            const int64_t erow = (int64_t)(row0 + rr) * k.N[0];
-            for (int x = threadIdx.x; x < k.N[0]; x += blockDim.x) {
+            const int64_t nrow = (int64_t)rem * n0;
+            const int64_t erow = (int64_t)(row0 + rr) * n0;
+            {
                 const int gx = x + ox;
                 float fac = t.deap[x] * fyz;
                 if ((gx + gy + gz) & 1) fac = -fac;
@@ -636,10 +645,11 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
         alpha_re = rq * pq.x / den;
         alpha_im = -rq * pq.y / den;
         const float ar = (float)alpha_re, ai = (float)alpha_im;
-        for (int rr = blockIdx.x; rr < t.seg_rows; rr += nbx) {
-            const int64_t erow = (int64_t)(row0 + rr) * k.N[0];
-            for (int x = threadIdx.x; x < k.N[0]; x += blockDim.x) {
-                const int64_t e = erow + x;
+        for (int l = threadIdx.x; l < my_elems; l += blockDim.x) {
+            const int i = l / n0, x = l - i * n0;
+            const int rr = (int)blockIdx.x + i * nbx;
+            {
+                const int64_t e = (int64_t)(row0 + rr) * n0 + x;
                 const float2 pv = t.p[e], qv = t.q[e];
                 float2 xv = t.x[e], rv = t.r[e];
                 xv.x += ar * pv.x - ai * pv.y;
@@ -698,7 +708,13 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
         }
     }
     if (!t.pad) return;
-    for (int rr = blockIdx.x; rr < t.seg_rows; rr += nbx) {
+    // interior only when the FFT passes read nothing else
+    const int gx0 = t.pad_full ? 0 : ox, gx1 = t.pad_full ? k.mos[0] : ox + n0;
+    const int w3 = gx1 - gx0;
+    const int my_pad = my_rows * w3;
+    for (int l = threadIdx.x; l < my_pad; l += blockDim.x) {
+        const int i = l / w3;
+        const int rr = (int)blockIdx.x + i * nbx;
         int f, z, y, rem;
         row_coords(row0 + rr, f, z, y, rem);
         const int gy = y + oy, gz = z + oz;
@@ -706,11 +722,10 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
         if (k.D > 1) fyz *= t.deap[t.deap_stride + y];
         if (k.D > 2) fyz *= t.deap[2 * t.deap_stride + z];
         const int64_t gline = (int64_t)gz * t.kl.s_z + (int64_t)gy * t.kl.s_y;
-        const int64_t nrow = (int64_t)rem * k.N[0];
-        const int64_t erow = (int64_t)(row0 + rr) * k.N[0];
-        // interior only when the FFT passes read nothing else
-        const int gx0 = t.pad_full ? 0 : ox, gx1 = t.pad_full ? k.mos[0] : ox + k.N[0];
-        for (int gx = gx0 + threadIdx.x; gx < gx1; gx += blockDim.x) {
+        const int64_t nrow = (int64_t)rem * n0;
+        const int64_t erow = (int64_t)(row0 + rr) * n0;
+        {
+            const int gx = gx0 + (l - i * w3);
             const int x = gx - ox;
             const bool in = x >= 0 && x < k.N[0];
             float fac = 0.f;
@@ -983,7 +998,7 @@ static void cg_prepare(CgSolver &cg, cudaStream_t st) {
         const int64_t cap = (int64_t)per_sm * nsm;
         const int64_t seg_rows = cg.seg_len / p.kp.N[0];
         const int64_t bx = std::min<int64_t>(seg_rows, cap / cg.nseg);
-        cg.use_tail = coop != 0 && bx >= 1;
+        cg.use_tail = coop != 0 && bx >= 1 && seg_rows * (int64_t)p.kp.mos[0] < (int64_t)INT32_MAX;
         if (cg.use_tail) {
             cg.tail_grid = dim3((unsigned)bx, (unsigned)cg.nseg);
             cg.partials.ensure((size_t)bx * cg.nseg);
