@@ -11,8 +11,15 @@
 //   5. rotate every pixel's vector so that coil 0 is real and non-negative:
 //      b_c *= exp(-i arg b_0) (:775-808).
 // The box is applied as separable passes (x, then y, then z), the same sums
-// in a different order.  Scratch: the C^2 correlation planes, twice.
+// in a different order; the correlation products are formed inside the x
+// pass, so the unsmoothed planes never reach memory.  Scratch: the
+// normalised coil images and the C^2 correlation planes twice, kept per
+// device between calls (grown to the largest call, never shrunk) so that a
+// pipeline re-estimating the map every frame allocates nothing.
 #include <cmath>
+#include <map>
+#include <memory>
+#include <mutex>
 
 #include "gb_internal.cuh"
 
@@ -41,12 +48,26 @@ __global__ void k_b1_rss_normalize(const float2 *__restrict__ in, int nc, int64_
     }
 }
 
-// plane (a * nc + b) = x_b conj(x_a); grid.y = a * nc + b
-__global__ void k_b1_correlation(const float2 *__restrict__ x, int nc, int64_t n, float2 *__restrict__ A) {
+// Correlation and its box sum along x in one pass: plane (a * nc + b) at
+// pixel p = sum over the kB1Box x-neighbours q of p inside the image of
+// x_b(q) conj(x_a(q)); grid.y = a * nc + b.  `scale` is applied when x is
+// the last smoothed dimension.
+__global__ void k_b1_corr_box_x(const float2 *__restrict__ x, int nc, int64_t n, int len0, float scale,
+                                float2 *__restrict__ A) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const int a = blockIdx.y / nc, b = blockIdx.y - a * nc;
-    A[(int64_t)blockIdx.y * n + p] = cmulc(x[(int64_t)b * n + p], x[(int64_t)a * n + p]);
+    const float2 *xa = x + (int64_t)a * n, *xb = x + (int64_t)b * n;
+    const int pos = (int)(p % len0);
+    float2 s = make_float2(0.f, 0.f);
+    for (int k = -(kB1Box >> 1); k <= (kB1Box >> 1); k++) {
+        const int q = pos + k;
+        if (q < 0 || q >= len0) continue;
+        const float2 v = cmulc(xb[p + k], xa[p + k]);
+        s.x += v.x;
+        s.y += v.y;
+    }
+    A[(int64_t)blockIdx.y * n + p] = make_float2(s.x * scale, s.y * scale);
 }
 
 // Box sum of width kB1Box along one dimension (stride between neighbours
@@ -68,34 +89,61 @@ __global__ void k_b1_box(const float2 *__restrict__ in, float2 *__restrict__ out
     out[plane + p] = make_float2(s.x * scale, s.y * scale);
 }
 
-// Two power iterations and the coil-0 phase reference; one pixel per thread,
-// the vector in registers (nc <= kB1MaxCoils).
+// Two power iterations and the coil-0 phase reference; one pixel per thread.
+// NCB bounds the coil count at compile time so that the vectors stay in
+// registers (loops fully unrolled, coils >= nc predicated off).
 constexpr int kB1MaxCoils = 32;
 
-__global__ void k_b1_power(const float2 *__restrict__ A, int nc, int64_t n, float2 *__restrict__ csm) {
+template <int NCB>
+__global__ void __launch_bounds__(256, NCB <= 16 ? 2 : 1) k_b1_power(const float2 *__restrict__ A, int nc, int64_t n, float2 *__restrict__ csm) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
-    float2 b[kB1MaxCoils], t[kB1MaxCoils];
-    for (int c = 0; c < nc; c++) b[c] = make_float2(1.f, 0.f);
+    float2 b[NCB], t[NCB];
+#pragma unroll
+    for (int c = 0; c < NCB; c++) b[c] = make_float2(c < nc ? 1.f : 0.f, 0.f);
     for (int it = 0; it < 2; it++) {
         float nrm = 0.f;
-        for (int j = 0; j < nc; j++) {
+#pragma unroll
+        for (int j = 0; j < NCB; j++) {
             float2 s = make_float2(0.f, 0.f);
-            for (int k = 0; k < nc; k++) {
-                const float2 a = A[((int64_t)k * nc + j) * n + p];
-                s.x += a.x * b[k].x - a.y * b[k].y;
-                s.y += a.x * b[k].y + a.y * b[k].x;
+            if (j < nc) {
+#pragma unroll
+                for (int k = 0; k < NCB; k++) {
+                    if (k < nc) {
+                        const float2 a = A[((int64_t)k * nc + j) * n + p];
+                        s.x += a.x * b[k].x - a.y * b[k].y;
+                        s.y += a.x * b[k].y + a.y * b[k].x;
+                    }
+                }
+                nrm += s.x * s.x + s.y * s.y;
             }
             t[j] = s;
-            nrm += s.x * s.x + s.y * s.y;
         }
         const float r = 1.f / sqrtf(nrm);
-        for (int c = 0; c < nc; c++) b[c] = make_float2(t[c].x * r, t[c].y * r);
+#pragma unroll
+        for (int c = 0; c < NCB; c++) b[c] = make_float2(t[c].x * r, t[c].y * r);
     }
     float sn, cs;
     sincosf(atan2f(b[0].y, b[0].x), &sn, &cs);
-    for (int c = 0; c < nc; c++)   // b_c * conj(cos + i sin)
-        csm[(int64_t)c * n + p] = make_float2(b[c].x * cs + b[c].y * sn, b[c].y * cs - b[c].x * sn);
+#pragma unroll
+    for (int c = 0; c < NCB; c++)   // b_c * conj(cos + i sin)
+        if (c < nc) csm[(int64_t)c * n + p] = make_float2(b[c].x * cs + b[c].y * sn, b[c].y * cs - b[c].x * sn);
+}
+
+// Scratch kept per device between calls; the mutex is held for a whole call.
+struct B1Scratch {
+    std::mutex mu;
+    DevBuf<float2> x, A, B;
+};
+
+B1Scratch &b1_scratch(int device) {
+    static std::mutex map_mu;
+    // never destroyed: device memory is returned with the context at exit
+    static auto *cache = new std::map<int, std::unique_ptr<B1Scratch>>();
+    std::lock_guard<std::mutex> lock(map_mu);
+    auto &slot = (*cache)[device];
+    if (!slot) slot.reset(new B1Scratch());
+    return *slot;
 }
 
 unsigned int nblk(int64_t n) { return (unsigned int)((n + 255) / 256); }
@@ -117,24 +165,37 @@ void estimate_b1_map(int D, const uint64_t *dims, int ncoils, int target_coils, 
     }
     const int planes = nc * nc;
     if ((int64_t)planes * n > ((int64_t)1 << 31)) fail(GB_ERR_INVALID_ARGUMENT, "estimate_b1_map: images too large");
-    DevBuf<float2> x, A, B;
-    x.ensure((size_t)nc * n);
-    A.ensure((size_t)planes * n);
-    B.ensure((size_t)planes * n);
-    k_b1_rss_normalize<<<nblk(n), 256, 0, st>>>(images, nc, n, x.get()); note_launch();
-    k_b1_correlation<<<dim3(nblk(n), planes), 256, 0, st>>>(x.get(), nc, n, A.get()); note_launch();
-    float2 *src = A.get(), *dst = B.get();
-    int64_t stride = 1;
+    int dev = 0;
+    GB_CUDA(cudaGetDevice(&dev));
+    B1Scratch &sc = b1_scratch(dev);
+    std::lock_guard<std::mutex> lock(sc.mu);
+    sc.x.ensure((size_t)nc * n);
+    sc.A.ensure((size_t)planes * n);
+    if (D > 1) sc.B.ensure((size_t)planes * n);
     const float scale = 1.f / std::pow((float)kB1Box, (float)D);
-    for (int d = 0; d < D; d++) {
+    k_b1_rss_normalize<<<nblk(n), 256, 0, st>>>(images, nc, n, sc.x.get()); note_launch();
+    k_b1_corr_box_x<<<dim3(nblk(n), planes), 256, 0, st>>>(sc.x.get(), nc, n, len[0], D == 1 ? scale : 1.f,
+                                                            sc.A.get());
+    note_launch();
+    float2 *src = sc.A.get(), *dst = sc.B.get();
+    int64_t stride = len[0];
+    for (int d = 1; d < D; d++) {
         k_b1_box<<<dim3(nblk(n), planes), 256, 0, st>>>(src, dst, n, stride, len[d], d == D - 1 ? scale : 1.f);
         note_launch();
         std::swap(src, dst);
         stride *= len[d];
     }
-    k_b1_power<<<nblk(n), 256, 0, st>>>(src, nc, n, csm); note_launch();
+    if (nc <= 4)
+        k_b1_power<4><<<nblk(n), 256, 0, st>>>(src, nc, n, csm);
+    else if (nc <= 8)
+        k_b1_power<8><<<nblk(n), 256, 0, st>>>(src, nc, n, csm);
+    else if (nc <= 16)
+        k_b1_power<16><<<nblk(n), 256, 0, st>>>(src, nc, n, csm);
+    else
+        k_b1_power<32><<<nblk(n), 256, 0, st>>>(src, nc, n, csm);
+    note_launch();
     GB_CUDA(cudaGetLastError());
-    GB_CUDA(cudaStreamSynchronize(st));   // scratch is freed on return
+    GB_CUDA(cudaStreamSynchronize(st));   // the scratch is free for the next call on return
 }
 
 }  // namespace gb
