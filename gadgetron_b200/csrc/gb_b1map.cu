@@ -17,9 +17,6 @@
 // device between calls (grown to the largest call, never shrunk) so that a
 // pipeline re-estimating the map every frame allocates nothing.
 #include <cmath>
-#include <map>
-#include <memory>
-#include <mutex>
 
 #include "gb_internal.cuh"
 
@@ -136,16 +133,6 @@ struct B1Scratch {
     DevBuf<float2> x, A, B;
 };
 
-B1Scratch &b1_scratch(int device) {
-    static std::mutex map_mu;
-    // never destroyed: device memory is returned with the context at exit
-    static auto *cache = new std::map<int, std::unique_ptr<B1Scratch>>();
-    std::lock_guard<std::mutex> lock(map_mu);
-    auto &slot = (*cache)[device];
-    if (!slot) slot.reset(new B1Scratch());
-    return *slot;
-}
-
 unsigned int nblk(int64_t n) { return (unsigned int)((n + 255) / 256); }
 
 }  // namespace
@@ -167,7 +154,7 @@ void estimate_b1_map(int D, const uint64_t *dims, int ncoils, int target_coils, 
     if ((int64_t)planes * n > ((int64_t)1 << 31)) fail(GB_ERR_INVALID_ARGUMENT, "estimate_b1_map: images too large");
     int dev = 0;
     GB_CUDA(cudaGetDevice(&dev));
-    B1Scratch &sc = b1_scratch(dev);
+    B1Scratch &sc = device_scratch<B1Scratch>(dev);
     std::lock_guard<std::mutex> lock(sc.mu);
     sc.x.ensure((size_t)nc * n);
     sc.A.ensure((size_t)planes * n);

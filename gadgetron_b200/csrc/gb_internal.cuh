@@ -19,6 +19,8 @@
 #include <stdint.h>
 
 #include <map>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -81,6 +83,20 @@ struct DevBuf {
     }
     T *get() const { return ptr; }
 };
+
+// Scratch of a setup routine kept per device between calls (grown to the
+// largest call, never shrunk): a struct S with a std::mutex `mu`, which a
+// call holds until its stream is done with the scratch.  The cache is never
+// destroyed; its device memory goes back with the context at exit.
+template <class S>
+S &device_scratch(int device) {
+    static std::mutex map_mu;
+    static auto *cache = new std::map<int, std::unique_ptr<S>>();
+    std::lock_guard<std::mutex> lock(map_mu);
+    auto &slot = (*cache)[device];
+    if (!slot) slot.reset(new S());
+    return *slot;
+}
 
 // --------------------------------------------------------- kernel params ---
 

@@ -16,8 +16,13 @@
 // [ceil(s - R), floor(s + R)] per dimension, periodic wrap.
 //
 // It is a setup computation (once per trajectory), so the gridding here is a
-// plain per-sample scatter with float atomics (the sum order per cell is not
-// fixed, unlike the CG-loop gridding) and the degridding a per-sample gather.
+// per-sample scatter with float atomics (the sum order per cell is not fixed,
+// unlike the CG-loop gridding) and the degridding a per-sample gather.  A warp
+// serves one sample, its lanes spread over the footprint's taps (up to 11^D
+// at width 5.5, each with a square root, a division and a degree-5 polynomial), so
+// that the tap arithmetic fills the SMs; the degridding sums the lanes'
+// partial sums in a fixed butterfly order.  The grid and the trajectory-range
+// flag are kept per device between calls.
 #include <cmath>
 
 #include "gb_internal.cuh"
@@ -49,56 +54,67 @@ __device__ __forceinline__ float jinc_weight(const float *ad, int D, float R) {
     r = sqrtf(r);
     r /= R;
     if (r >= kJincNormRadius) return 0.f;
-    float v = kJc0 + kJc1 * powf(r, 1.f) + kJc2 * powf(r, 2.f) + kJc3 * powf(r, 3.f) + kJc4 * powf(r, 4.f) +
-              kJc5 * powf(r, 5.f);
+    // the reference's sum c0 + c1 r + ... + c5 r^5 in its order, the powers
+    // formed by products (within a few ulp of pow(r, k))
+    const float r2 = r * r, r3 = r2 * r, r4 = r2 * r2, r5 = r4 * r;
+    float v = kJc0 + kJc1 * r + kJc2 * r2 + kJc3 * r3 + kJc4 * r4 + kJc5 * r5;
     return v < 0.f ? 0.f : v;
 }
 
 __device__ __forceinline__ int wrap_cell(int c, int m) { return c < 0 ? c + m : (c >= m ? c - m : c); }
 
-// Visits the footprint cells of sample j (z, y, x ascending), calling
-// f(cell_index, weight).
+// Visits this lane's share of the footprint cells of sample j (tap t =
+// lane, lane + 32, ... in z, y, x order), calling f(cell_index, weight).
 template <class F>
-__device__ __forceinline__ void for_footprint(const SdcArgs &a, const float *traj, int64_t j, F &&f) {
+__device__ __forceinline__ void for_footprint_lane(const SdcArgs &a, const float *traj, int64_t j, int lane,
+                                                   F &&f) {
     float s[3] = {0.f, 0.f, 0.f};
-    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    int lo[3] = {0, 0, 0}, n[3] = {1, 1, 1};
     for (int d = 0; d < a.D; d++) {
         s[d] = fmaf(traj[j * a.D + d], (float)a.mos[d], a.half_mos_pad[d]) - a.hp;
         lo[d] = (int)ceilf(s[d] - a.radius);
-        hi[d] = (int)floorf(s[d] + a.radius);
+        const int hi = (int)floorf(s[d] + a.radius);
+        n[d] = hi >= lo[d] ? hi - lo[d] + 1 : 0;
     }
-    for (int cz = lo[2]; cz <= hi[2]; cz++) {
-        for (int cy = lo[1]; cy <= hi[1]; cy++) {
-            for (int cx = lo[0]; cx <= hi[0]; cx++) {
-                const int c[3] = {cx, cy, cz};
-                float ad[3];
-                for (int d = 0; d < a.D; d++) ad[d] = fabsf(s[d] - (float)c[d]);
-                const float w = jinc_weight(ad, a.D, a.radius);
-                if (!isfinite(w) || w == 0.f) continue;
-                int64_t idx = 0;
-                for (int d = a.D - 1; d >= 0; d--) idx = idx * a.mos[d] + wrap_cell(c[d], a.mos[d]);
-                f(idx, w);
-            }
-        }
+    const int taps = n[0] * n[1] * n[2];
+    for (int t = lane; t < taps; t += 32) {
+        const int tx = t % n[0], tyz = t / n[0];
+        const int c[3] = {lo[0] + tx, lo[1] + tyz % n[1], lo[2] + tyz / n[1]};
+        float ad[3];
+        for (int d = 0; d < a.D; d++) ad[d] = fabsf(s[d] - (float)c[d]);
+        const float w = jinc_weight(ad, a.D, a.radius);
+        if (!isfinite(w) || w == 0.f) continue;
+        int64_t idx = 0;
+        for (int d = a.D - 1; d >= 0; d--) idx = idx * a.mos[d] + wrap_cell(c[d], a.mos[d]);
+        f(idx, w);
     }
 }
 
 __global__ void k_sdc_grid(SdcArgs a, const float *__restrict__ traj, const float *__restrict__ w,
                            float *__restrict__ grid) {
-    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (j >= a.M) return;
     const float v = w[j];
-    for_footprint(a, traj, j, [&](int64_t idx, float wt) { atomicAdd(&grid[idx], wt * v); });
+    for_footprint_lane(a, traj, j, threadIdx.x & 31, [&](int64_t idx, float wt) { atomicAdd(&grid[idx], wt * v); });
 }
 
 __global__ void k_sdc_degrid_update(SdcArgs a, const float *__restrict__ traj, const float *__restrict__ grid,
                                     float *__restrict__ w) {
-    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= a.M) return;
+    const int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (j >= a.M) return;   // whole warps leave together (blockDim is a multiple of 32)
+    const int lane = threadIdx.x & 31;
     float t = 0.f;
-    for_footprint(a, traj, j, [&](int64_t idx, float wt) { t += wt * grid[idx]; });
-    w[j] = t == 0.f ? 0.f : w[j] / t;
+    for_footprint_lane(a, traj, j, lane, [&](int64_t idx, float wt) { t += wt * grid[idx]; });
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) w[j] = t == 0.f ? 0.f : w[j] / t;
 }
+
+// Scratch kept per device between calls; the mutex is held for a whole call.
+struct SdcScratch {
+    std::mutex mu;
+    DevBuf<unsigned int> bad;
+    DevBuf<float> grid;
+};
 
 __global__ void k_fill(float *p, int64_t n, float v) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -141,14 +157,17 @@ void sdc_estimate_dcw(int D, const uint64_t *N, float os_factor, int iterations,
     }
     const unsigned int tb = 256;
     const unsigned int sb = (unsigned int)((M + tb - 1) / tb);
+    int dev = 0;
+    GB_CUDA(cudaGetDevice(&dev));
+    SdcScratch &sc = device_scratch<SdcScratch>(dev);
+    std::lock_guard<std::mutex> lock(sc.mu);
     {
-        DevBuf<unsigned int> bad;
-        bad.ensure(1);
-        GB_CUDA(cudaMemsetAsync(bad.get(), 0, sizeof(unsigned int), st));
+        sc.bad.ensure(1);
+        GB_CUDA(cudaMemsetAsync(sc.bad.get(), 0, sizeof(unsigned int), st));
         const int64_t nt = M * D;
-        k_traj_range<<<(unsigned int)((nt + tb - 1) / tb), tb, 0, st>>>(traj, nt, bad.get()); note_launch();
+        k_traj_range<<<(unsigned int)((nt + tb - 1) / tb), tb, 0, st>>>(traj, nt, sc.bad.get()); note_launch();
         unsigned int hb = 0;
-        GB_CUDA(cudaMemcpyAsync(&hb, bad.get(), sizeof(hb), cudaMemcpyDeviceToHost, st));
+        GB_CUDA(cudaMemcpyAsync(&hb, sc.bad.get(), sizeof(hb), cudaMemcpyDeviceToHost, st));
         GB_CUDA(cudaStreamSynchronize(st));
         if (hb) fail(GB_ERR_TRAJECTORY_RANGE, "trajectory out of range [-1/2, 1/2]");
     }
@@ -157,15 +176,17 @@ void sdc_estimate_dcw(int D, const uint64_t *N, float os_factor, int iterations,
     } else {
         k_fill<<<sb, tb, 0, st>>>(dcw, M, 1.f); note_launch();
     }
-    DevBuf<float> grid;
+    DevBuf<float> &grid = sc.grid;
     grid.ensure((size_t)G);
+    // one warp per sample
+    const unsigned int wb = (unsigned int)((M + (tb / 32) - 1) / (tb / 32));
     for (int it = 0; it < iterations; it++) {
         GB_CUDA(cudaMemsetAsync(grid.get(), 0, (size_t)G * sizeof(float), st));
-        k_sdc_grid<<<sb, tb, 0, st>>>(a, traj, dcw, grid.get()); note_launch();
-        k_sdc_degrid_update<<<sb, tb, 0, st>>>(a, traj, grid.get(), dcw); note_launch();
+        k_sdc_grid<<<wb, tb, 0, st>>>(a, traj, dcw, grid.get()); note_launch();
+        k_sdc_degrid_update<<<wb, tb, 0, st>>>(a, traj, grid.get(), dcw); note_launch();
     }
     GB_CUDA(cudaGetLastError());
-    GB_CUDA(cudaStreamSynchronize(st));   // the grid is freed on return
+    GB_CUDA(cudaStreamSynchronize(st));   // the grid is free for the next call on return
 }
 
 }  // namespace gb

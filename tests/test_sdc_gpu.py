@@ -36,3 +36,19 @@ def test_sdc_rejects_out_of_range(cuda):
     traj = torch.tensor([[0.2, 0.7]], dtype=torch.float32, device=cuda)
     with pytest.raises(gb.TrajectoryRangeError):
         gb.sdc.estimate_dcw(traj, (32, 32), 2.0, 2)
+
+
+def test_sdc_repeated_calls_and_call_after_rejection(cuda):
+    """Calls of changing grid sizes in turn, and a call after a rejected
+    trajectory, reuse the kept scratch and still match the oracle."""
+    small = S.radial_golden_angle_2d(16, 64).astype(np.float32)
+    big = S.radial_golden_angle_2d(32, 128).astype(np.float32)
+    cases = [(big, (96, 96)), (small, (32, 32)), (big, (96, 96))]
+    for traj, N in cases:
+        w = gb.sdc.estimate_dcw(torch.from_numpy(traj).to(cuda), N, 2.0, 5, 5.5)
+        assert O.rel_l2(w.cpu().numpy(), O.estimate_dcw(traj, N, 2.0, 5, 5.5)) <= 1e-5
+    bad = torch.tensor([[0.2, 0.7]], dtype=torch.float32, device=cuda)
+    with pytest.raises(gb.TrajectoryRangeError):
+        gb.sdc.estimate_dcw(bad, (32, 32), 2.0, 2)
+    w = gb.sdc.estimate_dcw(torch.from_numpy(small).to(cuda), (32, 32), 2.0, 5, 5.5)
+    assert O.rel_l2(w.cpu().numpy(), O.estimate_dcw(small, (32, 32), 2.0, 5, 5.5)) <= 1e-5
