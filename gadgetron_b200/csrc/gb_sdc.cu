@@ -77,16 +77,27 @@ __device__ __forceinline__ void for_footprint_lane(const SdcArgs &a, const float
         n[d] = hi >= lo[d] ? hi - lo[d] + 1 : 0;
     }
     const int taps = n[0] * n[1] * n[2];
+    if (lane >= taps) return;
+    // tap coordinates of t, stepped by 32 taps per round without divisions
+    int tx = lane % n[0], ty = (lane / n[0]) % n[1], tz = lane / (n[0] * n[1]);
     for (int t = lane; t < taps; t += 32) {
-        const int tx = t % n[0], tyz = t / n[0];
-        const int c[3] = {lo[0] + tx, lo[1] + tyz % n[1], lo[2] + tyz / n[1]};
+        const int c[3] = {lo[0] + tx, lo[1] + ty, lo[2] + tz};
         float ad[3];
         for (int d = 0; d < a.D; d++) ad[d] = fabsf(s[d] - (float)c[d]);
         const float w = jinc_weight(ad, a.D, a.radius);
-        if (!isfinite(w) || w == 0.f) continue;
-        int64_t idx = 0;
-        for (int d = a.D - 1; d >= 0; d--) idx = idx * a.mos[d] + wrap_cell(c[d], a.mos[d]);
-        f(idx, w);
+        if (isfinite(w) && w != 0.f) {
+            int64_t idx = 0;
+            for (int d = a.D - 1; d >= 0; d--) idx = idx * a.mos[d] + wrap_cell(c[d], a.mos[d]);
+            f(idx, w);
+        }
+        tx += 32;
+        while (tx >= n[0]) {
+            tx -= n[0];
+            if (++ty == n[1]) {
+                ty = 0;
+                ++tz;
+            }
+        }
     }
 }
 
