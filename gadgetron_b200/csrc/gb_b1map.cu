@@ -67,6 +67,60 @@ __global__ void k_b1_corr_box_x(const float2 *__restrict__ x, int nc, int64_t n,
     A[(int64_t)blockIdx.y * n + p] = make_float2(s.x * scale, s.y * scale);
 }
 
+// 2D: correlation products of a TX x TY pixel tile plus a 3-cell halo in
+// shared memory (zero outside the image), the x pass, then the y pass and the
+// 1 / 7^2 scale, one plane per blockIdx.y -- the sums and their order are
+// those of k_b1_corr_box_x followed by k_b1_box, without the intermediate
+// planes in memory.
+constexpr int kB1TX = 32, kB1TY = 16, kB1H = kB1Box >> 1;
+
+__global__ void __launch_bounds__(256) k_b1_corr_box_xy(const float2 *__restrict__ x, int nc, int nx, int ny,
+                                                        int tiles_x, float scale, float2 *__restrict__ A) {
+    constexpr int PW = kB1TX + 2 * kB1H, PH = kB1TY + 2 * kB1H;
+    __shared__ float2 P[PH][PW];       // products, halo included
+    __shared__ float2 Q[PH][kB1TX];    // x-pass sums
+    const int64_t n = (int64_t)nx * ny;
+    const int a = blockIdx.y / nc, b = blockIdx.y - a * nc;
+    const float2 *xa = x + (int64_t)a * n, *xb = x + (int64_t)b * n;
+    const int tx0 = (blockIdx.x % tiles_x) * kB1TX, ty0 = (blockIdx.x / tiles_x) * kB1TY;
+    for (int e = threadIdx.x; e < PH * PW; e += blockDim.x) {
+        const int py = e / PW, px = e - py * PW;
+        const int gx = tx0 + px - kB1H, gy = ty0 + py - kB1H;
+        float2 v = make_float2(0.f, 0.f);
+        if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) {
+            const int64_t g = (int64_t)gy * nx + gx;
+            v = cmulc(xb[g], xa[g]);
+        }
+        P[py][px] = v;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < PH * kB1TX; e += blockDim.x) {
+        const int py = e / kB1TX, qx = e - py * kB1TX;
+        float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < kB1Box; k++) {
+            const float2 v = P[py][qx + k];
+            s.x += v.x;
+            s.y += v.y;
+        }
+        Q[py][qx] = s;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kB1TY * kB1TX; e += blockDim.x) {
+        const int oy = e / kB1TX, ox = e - oy * kB1TX;
+        const int gx = tx0 + ox, gy = ty0 + oy;
+        if (gx >= nx || gy >= ny) continue;
+        float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < kB1Box; k++) {
+            const float2 v = Q[oy + k][ox];
+            s.x += v.x;
+            s.y += v.y;
+        }
+        A[(int64_t)blockIdx.y * n + (int64_t)gy * nx + gx] = make_float2(s.x * scale, s.y * scale);
+    }
+}
+
 // Box sum of width kB1Box along one dimension (stride between neighbours
 // `stride`, extent `len`, zero outside), every plane; the last pass scales.
 __global__ void k_b1_box(const float2 *__restrict__ in, float2 *__restrict__ out, int64_t n, int64_t stride,
@@ -158,15 +212,24 @@ void estimate_b1_map(int D, const uint64_t *dims, int ncoils, int target_coils, 
     std::lock_guard<std::mutex> lock(sc.mu);
     sc.x.ensure((size_t)nc * n);
     sc.A.ensure((size_t)planes * n);
-    if (D > 1) sc.B.ensure((size_t)planes * n);
+    if (D > 2) sc.B.ensure((size_t)planes * n);
     const float scale = 1.f / std::pow((float)kB1Box, (float)D);
     k_b1_rss_normalize<<<nblk(n), 256, 0, st>>>(images, nc, n, sc.x.get()); note_launch();
-    k_b1_corr_box_x<<<dim3(nblk(n), planes), 256, 0, st>>>(sc.x.get(), nc, n, len[0], D == 1 ? scale : 1.f,
-                                                            sc.A.get());
-    note_launch();
     float2 *src = sc.A.get(), *dst = sc.B.get();
     int64_t stride = len[0];
-    for (int d = 1; d < D; d++) {
+    int d = 1;
+    if (D == 2) {   // both passes on shared-memory tiles
+        const int tiles_x = (len[0] + kB1TX - 1) / kB1TX, tiles_y = (len[1] + kB1TY - 1) / kB1TY;
+        k_b1_corr_box_xy<<<dim3((unsigned)(tiles_x * tiles_y), planes), 256, 0, st>>>(
+            sc.x.get(), nc, len[0], len[1], tiles_x, scale, sc.A.get());
+        note_launch();
+        d = D;
+    } else {
+        k_b1_corr_box_x<<<dim3(nblk(n), planes), 256, 0, st>>>(sc.x.get(), nc, n, len[0], D == 1 ? scale : 1.f,
+                                                                sc.A.get());
+        note_launch();
+    }
+    for (; d < D; d++) {
         k_b1_box<<<dim3(nblk(n), planes), 256, 0, st>>>(src, dst, n, stride, len[d], d == D - 1 ? scale : 1.f);
         note_launch();
         std::swap(src, dst);
