@@ -173,7 +173,7 @@ GB_API gb_status gb_nufft_compute(gb_nufft_plan plan, const void *in, void *out,
     return guarded([&] {
         if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
         DeviceGuard g((*plan->p).device);
-        nufft_compute((*plan->p), in, out, dcw, mode, (int)num_batches, image_oversampled != 0, S(stream));
+        nufft_compute((*plan->p), in, out, dcw, mode, count_arg(num_batches, "number of batches"), image_oversampled != 0, S(stream));
     });
 }
 
@@ -181,9 +181,8 @@ GB_API gb_status gb_nufft_mult_MH_M(gb_nufft_plan plan, const void *in, void *ou
                                     uint32_t num_batches, void *stream) {
     return guarded([&] {
         if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
-        if (num_batches == 0) fail(GB_ERR_INVALID_ARGUMENT, "number of batches must be positive");
         DeviceGuard g((*plan->p).device);
-        nufft_mult_MH_M((*plan->p), in, out, dcw, (int)num_batches, S(stream));
+        nufft_mult_MH_M((*plan->p), in, out, dcw, count_arg(num_batches, "number of batches"), S(stream));
     });
 }
 
@@ -191,9 +190,8 @@ GB_API gb_status gb_nufft_convolve(gb_nufft_plan plan, const void *in, void *out
                                    int accumulate, uint32_t num_batches, void *stream) {
     return guarded([&] {
         if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
-        if (num_batches == 0) fail(GB_ERR_INVALID_ARGUMENT, "number of batches must be positive");
         DeviceGuard g((*plan->p).device);
-        nufft_convolve((*plan->p), in, out, mode, accumulate != 0, (int)num_batches, S(stream));
+        nufft_convolve((*plan->p), in, out, mode, accumulate != 0, count_arg(num_batches, "number of batches"), S(stream));
     });
 }
 
@@ -202,7 +200,7 @@ GB_API gb_status gb_nufft_fft(gb_nufft_plan plan, void *data, gb_fft_mode mode, 
     return guarded([&] {
         if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
         DeviceGuard g((*plan->p).device);
-        nufft_fft((*plan->p), data, mode, do_scale != 0, (int)num_frames_x_batches, S(stream));
+        nufft_fft((*plan->p), data, mode, do_scale != 0, count_arg(num_frames_x_batches, "number of frames x batches"), S(stream));
     });
 }
 
@@ -212,7 +210,7 @@ GB_API gb_status gb_nufft_deapodize(gb_nufft_plan plan, void *image, int fourier
         if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
         (void)fourier_domain;   // both filters carry the same real values
         DeviceGuard g((*plan->p).device);
-        nufft_deapodize((*plan->p), image, (int)num_frames_x_batches, S(stream));
+        nufft_deapodize((*plan->p), image, count_arg(num_frames_x_batches, "number of frames x batches"), S(stream));
     });
 }
 
@@ -221,10 +219,9 @@ GB_API gb_status gb_nufft_traj_grad(gb_nufft_plan plan, const void *image, const
     return guarded([&] {
         if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
         if (!image || !weights || !grad_traj) fail(GB_ERR_INVALID_ARGUMENT, "NULL argument");
-        if (num_batches == 0) fail(GB_ERR_INVALID_ARGUMENT, "number of batches must be positive");
         DeviceGuard g((*plan->p).device);
         nufft_traj_grad((*plan->p), static_cast<const float2 *>(image), static_cast<const float2 *>(weights), dcw,
-                        grad_traj, (int)num_batches, S(stream));
+                        grad_traj, count_arg(num_batches, "number of batches"), S(stream));
     });
 }
 
@@ -233,10 +230,9 @@ GB_API gb_status gb_nufft_traj_grad_from_grid(gb_nufft_plan plan, const void *gr
     return guarded([&] {
         if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
         if (!grid || !weights || !grad_traj) fail(GB_ERR_INVALID_ARGUMENT, "NULL argument");
-        if (num_batches == 0) fail(GB_ERR_INVALID_ARGUMENT, "number of batches must be positive");
         DeviceGuard g((*plan->p).device);
         nufft_traj_grad_from_grid((*plan->p), static_cast<const float2 *>(grid), static_cast<const float2 *>(weights),
-                                  grad_traj, (int)num_batches, S(stream));
+                                  grad_traj, count_arg(num_batches, "number of batches"), S(stream));
     });
 }
 
@@ -275,7 +271,7 @@ GB_API gb_status gb_nufft_autotune(gb_nufft_plan plan, uint32_t num_batches, voi
     return guarded([&] {
         if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
         DeviceGuard g((*plan->p).device);
-        plan_autotune(*plan->p, (int)num_batches, S(stream));
+        plan_autotune(*plan->p, count_arg(num_batches, "number of batches"), S(stream));
     });
 }
 

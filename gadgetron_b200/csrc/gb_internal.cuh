@@ -48,6 +48,14 @@ uint64_t launch_count();
 void check_cuda(cudaError_t e, const char *what);
 void check_cufft(cufftResult r, const char *what);
 
+// A batch (or frame x batch) count taken from the C ABI as uint32_t and used
+// as int: zero and values above INT_MAX are rejected before the conversion.
+inline int count_arg(uint32_t v, const char *what) {
+    if (v == 0 || v > 0x7fffffffu)
+        fail(GB_ERR_INVALID_ARGUMENT, std::string(what) + " must be in [1, 2^31 - 1]");
+    return static_cast<int>(v);
+}
+
 #define GB_CUDA(x) ::gb::check_cuda((x), #x)
 #define GB_CUFFT(x) ::gb::check_cufft((x), #x)
 

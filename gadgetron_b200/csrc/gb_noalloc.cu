@@ -2,10 +2,9 @@
 // any device allocation, for callers that cannot call cudaMalloc.
 //
 // Who needs it: code that runs where allocating is not allowed or not safe --
-// inside a host callback or a real-time thread with a fixed memory budget, in
-// a process whose device memory is owned by another allocator (a framework
-// caching allocator that must not be bypassed), or between the launches of a
-// stream capture.  The regular entry point (gb_nufft_convolve with
+// inside a host callback or a real-time thread with a fixed memory budget, or
+// in a process whose device memory is owned by another allocator (a framework
+// caching allocator that must not be bypassed).  The regular entry point (gb_nufft_convolve with
 // GB_CONV_NC2C) allocates the scratch of its split-tile reduction lazily with
 // cudaMalloc; this one takes it from a fixed array in device memory instead.
 //
@@ -70,7 +69,7 @@ extern "C" GB_API gb_status gb_nufft_convolve_nc2c_noalloc(gb_nufft_plan plan, c
         NufftPlan *p = plan_from_handle(plan);
         if (!p) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
         if (!samples || !grid) fail(GB_ERR_INVALID_ARGUMENT, "NULL input/output");
-        if (num_batches == 0) fail(GB_ERR_INVALID_ARGUMENT, "number of batches must be positive");
+        const int nb = count_arg(num_batches, "number of batches");
         if (!p->prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
         int old = -1;
         check_cuda(cudaGetDevice(&old), "cudaGetDevice");
@@ -80,7 +79,7 @@ extern "C" GB_API gb_status gb_nufft_convolve_nc2c_noalloc(gb_nufft_plan plan, c
             ~Restore() { if (dev != cur && dev >= 0) cudaSetDevice(dev); }
         } restore{old, p->device};
         size_t need_partials = 0, need_counters = 0;
-        grid_scratch_need(*p, (int)num_batches, &need_partials, &need_counters);
+        grid_scratch_need(*p, nb, &need_partials, &need_counters);
         if (need_partials > kPartialElems || need_counters > kCounterElems)
             fail(GB_ERR_INVALID_ARGUMENT,
                  "gb_nufft_convolve_nc2c_noalloc: this plan and batch count need " +
@@ -93,7 +92,7 @@ extern "C" GB_API gb_status gb_nufft_convolve_nc2c_noalloc(gb_nufft_plan plan, c
         if (need_counters) check_cuda(cudaMemsetAsync(counters, 0, need_counters * sizeof(unsigned int), st),
                                       "cudaMemsetAsync");
         launch_grid_external_scratch(*p, static_cast<const float2 *>(samples), static_cast<float2 *>(grid),
-                                     (int)num_batches, accumulate != 0, partials, counters, st);
+                                     nb, accumulate != 0, partials, counters, st);
         return GB_OK;
     } catch (...) {
         return current_exception_status();

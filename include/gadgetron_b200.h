@@ -147,8 +147,7 @@ GB_API gb_status gb_nufft_convolve(gb_nufft_plan plan, const void *in, void *out
  * gb_nufft_convolve with GB_CONV_NC2C, but without allocating device memory.
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
  * code running in a host callback or a real-time thread with a fixed memory
- * budget, under another allocator that must not be bypassed, or inside a
- * stream capture.  Its scratch (the partial tiles of heavily loaded tiles) is
+ * budget, or under another allocator that must not be bypassed.  Its scratch (the partial tiles of heavily loaded tiles) is
  * a fixed 16 MiB array in device memory that each GPU loading this library
  * keeps until exit; a plan and batch count needing more is rejected with
  * GB_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's

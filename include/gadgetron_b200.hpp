@@ -6,9 +6,8 @@
 //   cuCgSolver<float_complext>                        (toolboxes/solvers/gpu/cuCgSolver.h:24-29)
 // Same method names and argument meaning; errors throw std::runtime_error as
 // the reference does.  Arrays are raw device pointers (complex data as
-// interleaved float pairs) with the reference's x-fastest layouts; the
-// Gadgetron-side adapter that wraps cuNDArray around these calls is shown in
-// INTEGRATION.md.
+// interleaved float pairs) with the reference's x-fastest layouts; a
+// Gadgetron-side adapter wraps cuNDArray::get_data_ptr() around these calls.
 #pragma once
 
 #include <cstdint>

@@ -1,0 +1,261 @@
+"""Parity against the reference's own GPU path on the same seeded inputs.
+
+oracle/_ref/libgbref.so is the reference's cuNFFT_impl<float,D,STANDARD>,
+cuNonCartesianSenseOperator and cuCgSolver compiled from its sources
+(oracle/build_ref.py); oracle/ref.py runs them through their public C++ API
+exactly as their callers do.  Every case compares three things:
+
+* the product (gadgetron_b200 through the C ABI) against the reference,
+  relative L2 <= 1e-5 (the bar of test/hoNFFT_test.cpp:137-152);
+* the CPU oracle (oracle/oracle.py) against the reference, <= 1e-5, which
+  pins the oracle that the rest of the suite checks against;
+* where stated, both against the FP64 direct NDFT on a sample subset, as a
+  statement of the approximation error (not a parity bound).
+
+The configurations are the benchmark's: 2D radial alpha 2 / W 5.5 (full size
+of the 128^2 single-coil NUFFT and of the 256^2 16-coil CG-SENSE), 3D
+kooshball alpha 1.5 / W 4, 2D variable-density spiral alpha 1.25 / W 4 with
+and without compensated accumulation, multi-frame and batched data.
+"""
+import numpy as np
+import pytest
+import torch
+
+from gadgetron_b200 import synthetic as S
+from oracle import oracle as O
+from oracle import ref as R
+from tests.helpers import PARITY_TOL, rel_l2
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not R.available(), reason="reference build (oracle/_ref) not present")]
+
+import gadgetron_b200 as gb  # noqa: E402
+
+# CG iterates: the reference reduces in FP32 (cublasCdotc/Scnrm2), the product
+# in FP64, so the iterates drift apart by rounding of the step sizes; bound
+# per iteration of a 10-iteration solve.
+CG_TOL = 1e-4
+
+
+def _t(a, dev):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def _plan(N, mos, W, traj, frames=1, flags=0, dev="cuda:0"):
+    plan = gb.NFFT.make_plan(N, mos, W, flags=flags)
+    plan.preprocess(_t(traj, dev), gb.NFFT_prep_mode.ALL, num_frames=frames)
+    return plan
+
+
+def _fwd_adj_case(N, mos, W, traj, frames, batches, dcw, seed, flags=0, oracle_check=True):
+    dev = torch.device("cuda:0")
+    D = len(N)
+    img = S.gaussian_image((batches, frames) + tuple(reversed(N)), seed)
+    plan = _plan(N, mos, W, traj, frames, flags)
+    M = traj.shape[0] // frames
+    y = torch.empty((batches, frames * M), dtype=torch.complex64, device=dev)
+    plan.compute(_t(img, dev), y, None, gb.NFFT_comp_mode.FORWARDS_C2NC)
+    y_ref = R.nfft_compute(N, mos, W, traj, frames, img, None, "FORWARDS_C2NC", batches)
+    yg = y.cpu().numpy()
+    e_fwd = rel_l2(yg, y_ref)
+    assert e_fwd <= PARITY_TOL, e_fwd
+    # adjoint of the reference's samples with density weights
+    x = torch.empty((batches, frames) + tuple(reversed(N)), dtype=torch.complex64, device=dev)
+    plan.compute(_t(y_ref, dev), x, _t(dcw, dev), gb.NFFT_comp_mode.BACKWARDS_NC2C)
+    x_ref = R.nfft_compute(N, mos, W, traj, frames, y_ref, dcw, "BACKWARDS_NC2C", batches)
+    e_adj = rel_l2(x.cpu().numpy(), x_ref)
+    assert e_adj <= PARITY_TOL, e_adj
+    if oracle_check:
+        orc = O.OraclePlan(N, mos, W)
+        orc.preprocess(traj.reshape(frames, -1, D))
+        assert rel_l2(orc.forward_c2nc(img), y_ref) <= PARITY_TOL
+        assert rel_l2(orc.backwards_nc2c(y_ref, dcw.reshape(frames, -1)), x_ref) <= PARITY_TOL
+    return img, yg, y_ref, x.cpu().numpy(), x_ref
+
+
+def test_ref_2d_radial_128_full_size_fwd_adj_and_ndft():
+    """128^2 single coil, 128 golden-angle spokes x 256 samples, alpha 2,
+    W 5.5: forward C2NC then adjoint NC2C with |k| ramp weights, at full size."""
+    N, mos, W = (128, 128), (256, 256), 5.5
+    traj = S.radial_golden_angle_2d(128, 256)
+    dcw = S.ramp_dcw(traj)
+    img, yg, y_ref, xg, x_ref = _fwd_adj_case(N, mos, W, traj, 1, 1, dcw, seed=1)
+    # approximation error of both against the FP64 direct NDFT (4096 samples)
+    sub = np.random.default_rng(2).choice(traj.shape[0], 4096, replace=False)
+    y_ndft = O.ndft_forward(img.reshape(1, 128, 128), traj[sub], mos)
+    e_prod, e_ref = rel_l2(yg[:, sub], y_ndft), rel_l2(y_ref[:, sub], y_ndft)
+    print("fwd vs NDFT: product %.3e reference %.3e" % (e_prod, e_ref))
+    assert e_prod <= 1e-4 and abs(e_prod - e_ref) <= 1e-5
+
+
+def test_ref_mult_MH_M_and_frames_batches():
+    N, mos, W = (64, 64), (128, 128), 5.5
+    frames, batches = 3, 3
+    traj = np.concatenate([S.radial_golden_angle_2d(16, 128, profile_offset=16 * f) for f in range(frames)], 0)
+    dcw = np.concatenate([S.ramp_dcw(traj[f * 2048:(f + 1) * 2048]) for f in range(frames)], 0)
+    _fwd_adj_case(N, mos, W, traj, frames, batches, dcw, seed=3)
+    dev = torch.device("cuda:0")
+    plan = _plan(N, mos, W, traj, frames)
+    img = S.gaussian_image((batches, frames, 64, 64), 4)
+    out = torch.empty_like(_t(img, dev))
+    plan.mult_MH_M(_t(img, dev), out, _t(dcw, dev))
+    ref = R.nfft_mult_MH_M(N, mos, W, traj, frames, img, dcw, batches)
+    assert rel_l2(out.cpu().numpy(), ref) <= PARITY_TOL
+
+
+def test_ref_3d_kooshball_alpha_1_5_w4():
+    """3D golden-means kooshball, alpha 1.5 (64 -> 96), W 4, two coils."""
+    N, mos, W = (64, 64, 64), (96, 96, 96), 4.0
+    traj = S.kooshball_golden_means_3d(1500, 96)
+    dcw = S.ramp_dcw(traj)
+    _fwd_adj_case(N, mos, W, traj, 1, 2, dcw, seed=5, oracle_check=False)
+    # oracle pinned on a smaller 3D case of the same alpha and W (32 -> 48 is
+    # not a multiple of 32, which the reference requires; 64 -> 96 is)
+    traj_s = S.kooshball_golden_means_3d(300, 64)
+    _fwd_adj_case(N, mos, W, traj_s, 1, 1, S.ramp_dcw(traj_s), seed=6, oracle_check=True)
+
+
+def test_ref_3d_kooshball_full_sample_count():
+    """The 3D benchmark geometry: 128^3 -> 192^3, 20000 spokes x 256 samples
+    (5.12M samples), W 4; one coil (the per-coil arithmetic is the same)."""
+    N, mos, W = (128, 128, 128), (192, 192, 192), 4.0
+    traj = S.kooshball_golden_means_3d(20000, 256)
+    dcw = S.ramp_dcw(traj)
+    _fwd_adj_case(N, mos, W, traj, 1, 1, dcw, seed=7, oracle_check=False)
+
+
+@pytest.mark.parametrize("compensated", [False, True])
+def test_ref_2d_spiral_alpha_1_25_w4(compensated):
+    """Variable-density Archimedean spiral (4x centre density), alpha 1.25
+    (128 -> 160), W 4, with and without compensated in-bin accumulation."""
+    N, mos, W = (128, 128), (160, 160), 4.0
+    traj = S.spiral_archimedean_2d(24, 1024, 128)
+    dcw = S.ramp_dcw(traj)
+    flags = gb.FLAG_COMPENSATED if compensated else 0
+    img, yg, y_ref, xg, x_ref = _fwd_adj_case(N, mos, W, traj, 1, 2, dcw, seed=8, flags=flags)
+    sub = np.random.default_rng(9).choice(traj.shape[0], 4096, replace=False)
+    y_ndft = O.ndft_forward(img.reshape(2, 128, 128), traj[sub], mos)
+    print("spiral fwd vs NDFT (compensated=%d): product %.3e reference %.3e" %
+          (compensated, rel_l2(yg[:, sub], y_ndft), rel_l2(y_ref[:, sub], y_ndft)))
+
+
+def test_ref_standalone_convolve_fft_deapodize():
+    dev = torch.device("cuda:0")
+    N, mos, W = (64, 64), (128, 128), 5.5
+    traj = S.radial_golden_angle_2d(48, 128)
+    plan = _plan(N, mos, W, traj)
+    rng = np.random.default_rng(10)
+    grid = (rng.standard_normal((2, 1, 128, 128)) + 1j * rng.standard_normal((2, 1, 128, 128))).astype(np.complex64)
+    y = torch.empty((2, traj.shape[0]), dtype=torch.complex64, device=dev)
+    plan.convolve(_t(grid, dev), y, gb.NFFT_conv_mode.C2NC)
+    y_ref = R.nfft_convolve(N, mos, W, traj, 1, grid, "C2NC", 2)
+    assert rel_l2(y.cpu().numpy(), y_ref) <= PARITY_TOL
+    g = torch.empty((2, 1, 128, 128), dtype=torch.complex64, device=dev)
+    plan.convolve(_t(y_ref, dev), g, gb.NFFT_conv_mode.NC2C)
+    g_ref = R.nfft_convolve(N, mos, W, traj, 1, y_ref, "NC2C", 2)
+    assert rel_l2(g.cpu().numpy(), g_ref) <= PARITY_TOL
+    plan.convolve(_t(y_ref, dev), g, gb.NFFT_conv_mode.NC2C, accumulate=True)
+    g_ref2 = R.nfft_convolve(N, mos, W, traj, 1, y_ref, "NC2C", 2, out=g_ref, accumulate=True)
+    assert rel_l2(g.cpu().numpy(), g_ref2) <= PARITY_TOL
+    for fwd in (True, False):
+        for scale in (True, False):
+            t = _t(grid, dev)
+            plan.fft(t, gb.NFFT_fft_mode.FORWARDS if fwd else gb.NFFT_fft_mode.BACKWARDS, do_scale=scale)
+            assert rel_l2(t.cpu().numpy(), R.nfft_fft(N, mos, W, grid, fwd, scale)) <= PARITY_TOL
+    for fourier in (False, True):
+        t = _t(grid, dev)
+        plan.deapodize(t, fourier_domain=fourier)
+        assert rel_l2(t.cpu().numpy(), R.nfft_deapodize(N, mos, W, grid, fourier)) <= PARITY_TOL
+
+
+def _sense_setup(N, mos, W, spokes, samples, coils, frames=1, seed=0):
+    traj = np.concatenate([S.radial_golden_angle_2d(spokes, samples, profile_offset=f * spokes)
+                           for f in range(frames)], 0)
+    M = spokes * samples
+    dcw = np.concatenate([S.ramp_dcw(traj[f * M:(f + 1) * M]) for f in range(frames)], 0)
+    sq = np.sqrt(dcw).astype(np.float32)
+    csm = S.gaussian_bump_csm(tuple(reversed(N)), coils)
+    ph = np.stack([S.ellipse_phantom(tuple(reversed(N)), 20, seed + f) for f in range(frames)], 0)
+    dev = torch.device("cuda:0")
+    E = gb.cuNonCartesianSenseOperator(len(N))
+    E.setup(N, mos, W)
+    E.set_csm(_t(csm, dev))
+    E.set_dcw(_t(sq, dev))
+    E.preprocess(_t(traj, dev), num_frames=frames)
+    return E, traj, sq, csm, ph
+
+
+def test_ref_sense_operator_256_16_coils_full_size():
+    """The CG-SENSE operator at full size: 256^2, 16 Gaussian-bump coils,
+    96 golden-angle spokes x 512 samples, alpha 2, W 5.5, sqrt(w) weights."""
+    N, mos, W, C = (256, 256), (512, 512), 5.5, 16
+    E, traj, sq, csm, ph = _sense_setup(N, mos, W, 96, 512, C, seed=11)
+    dev = torch.device("cuda:0")
+    y = torch.empty((C, traj.shape[0]), dtype=torch.complex64, device=dev)
+    E.mult_M(_t(ph, dev), y)
+    y_ref = R.sense_mult(N, mos, W, traj, 1, csm, sq, ph, adjoint=False)
+    assert rel_l2(y.cpu().numpy(), y_ref) <= PARITY_TOL
+    x = torch.empty((1, 256, 256), dtype=torch.complex64, device=dev)
+    E.mult_MH(_t(y_ref, dev), x)
+    x_ref = R.sense_mult(N, mos, W, traj, 1, csm, sq, y_ref, adjoint=True)
+    assert rel_l2(x.cpu().numpy(), x_ref) <= PARITY_TOL
+
+
+def test_ref_sense_multiframe_and_oracle():
+    N, mos, W, C = (64, 64), (128, 128), 5.5, 6
+    E, traj, sq, csm, ph = _sense_setup(N, mos, W, 24, 128, C, frames=2, seed=12)
+    dev = torch.device("cuda:0")
+    y = torch.empty((C, traj.shape[0]), dtype=torch.complex64, device=dev)
+    E.mult_M(_t(ph, dev), y)
+    y_ref = R.sense_mult(N, mos, W, traj, 2, csm, sq, ph)
+    assert rel_l2(y.cpu().numpy(), y_ref) <= PARITY_TOL
+    x = torch.empty((2, 64, 64), dtype=torch.complex64, device=dev)
+    E.mult_MH(_t(y_ref, dev), x)
+    x_ref = R.sense_mult(N, mos, W, traj, 2, csm, sq, y_ref, adjoint=True)
+    assert rel_l2(x.cpu().numpy(), x_ref) <= PARITY_TOL
+    plan = O.OraclePlan(N, mos, W)
+    plan.preprocess(traj.reshape(2, -1, 2))
+    orc = O.OracleSense(plan, csm, sq.reshape(2, -1))
+    assert rel_l2(orc.mult_M(ph).reshape(C, -1), y_ref) <= PARITY_TOL
+    assert rel_l2(orc.mult_MH(y_ref.reshape(C, 2, -1)), x_ref) <= PARITY_TOL
+
+
+def test_ref_cg_sense_10_iterations_per_iteration_divergence():
+    """The CG-SENSE benchmark solve at full size (256^2, 16 coils, 96 x 512,
+    10 iterations, tc_tolerance 0 so both run all 10): every iterate of the
+    product against the reference's iterate (cuCgSolver's solver_dump hook)."""
+    N, mos, W, C = (256, 256), (512, 512), 5.5, 16
+    E, traj, sq, csm, ph = _sense_setup(N, mos, W, 96, 512, C, seed=13)
+    dev = torch.device("cuda:0")
+    y = R.sense_mult(N, mos, W, traj, 1, csm, sq, ph)
+    rng = np.random.default_rng(14)
+    rms = np.sqrt(np.mean(np.abs(y) ** 2))
+    d = (y + 0.01 * rms * (rng.standard_normal(y.shape) + 1j * rng.standard_normal(y.shape)) / np.sqrt(2)
+         ).astype(np.complex64)
+    x_ref, its = R.cg_sense(N, mos, W, traj, 1, csm, sq, d, 10, 0.0, keep_iterates=True)
+    assert its.shape[0] == 10
+    cg = gb.cuCgSolver()
+    cg.set_encoding_operator(E)
+    cg.set_tc_tolerance(0.0)
+    errs = []
+    for k in range(1, 11):
+        cg.set_max_iterations(k)
+        xk = cg.solve(_t(d, dev)).cpu().numpy()
+        errs.append(rel_l2(xk, its[k - 1]))
+    print("per-iteration rel-L2 vs reference:", " ".join("%.2e" % e for e in errs))
+    assert max(errs) <= CG_TOL, errs
+    assert rel_l2(xk, x_ref) <= CG_TOL
+
+
+def test_ref_cg_oracle_pinned():
+    """The oracle's CG (FP64) against the reference's cuCgSolver on a small
+    case, 8 iterations."""
+    N, mos, W, C = (64, 64), (128, 128), 5.5, 4
+    _, traj, sq, csm, ph = _sense_setup(N, mos, W, 32, 128, C, seed=15)
+    plan = O.OraclePlan(N, mos, W)
+    plan.preprocess(traj.reshape(1, -1, 2))
+    orc = O.OracleSense(plan, csm, sq.reshape(1, -1))
+    d = orc.mult_M(ph).astype(np.complex64)
+    x_ref = R.cg_sense(N, mos, W, traj, 1, csm, sq, d.reshape(C, -1), 8, 0.0)
+    x_orc = O.cg_solve(orc, d, iterations=8, tc_tolerance=0.0)
+    assert rel_l2(x_orc, x_ref) <= CG_TOL

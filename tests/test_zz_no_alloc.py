@@ -1,7 +1,6 @@
 """GPU test of gb_nufft_convolve_nc2c_noalloc, the gridding entry point that
 allocates no device memory (for callers that cannot call cudaMalloc: host
-callbacks, real-time threads with a fixed budget, foreign allocators, stream
-captures).  It is called through the C ABI and must reproduce the regular
+callbacks, real-time threads with a fixed budget, foreign allocators).  It is called through the C ABI and must reproduce the regular
 entry point (gb_nufft_convolve, GB_CONV_NC2C) on two calls in a row, with
 heavily loaded tiles so that the split-tile scratch is exercised.
 
