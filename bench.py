@@ -19,8 +19,13 @@ step, outside the timed events.
 
 N > 1 runs N independent replicas (one per GPU; the path has no data
 exchange) under torchrun; timing is the max over ranks.  `--impl reference`
-times the reference algorithm's CPU restatement (the oracle port: C/OpenMP
-gridding, threaded FFT, the cgSolver iteration) on the host cores.
+times the reference's CPU reconstruction path in its own float arithmetic
+(hoGriddingConvolution's convolution matrix with OpenMP over coils, a
+complex64 FFT on every host thread, the cgSolver iteration) on the host
+cores; it loads no CUDA library.  At N = 1 the headline line also carries
+the NUFFT throughput, the preprocess time, the batched-vs-per-frame figure
+and the reference's own GPU path timed on the same device
+(headline_extras).
 """
 from __future__ import annotations
 
@@ -360,33 +365,30 @@ def run_ours(args, rank, world, local_rank):
 
 
 def cpu_cg_sample(wl, d_host, iters_timed=3):
-    """Times the oracle's CG-SENSE (C/OpenMP gridding, threaded FFT) on this
-    host: one E^H d and `iters_timed` CG iterations, scaled to 10 iterations."""
+    """Times the reference's CPU path in its float arithmetic
+    (oracle.HoSenseFloat) on this host: one E^H d and `iters_timed` CG
+    iterations, scaled to 10 iterations; the convolution-matrix build
+    (preprocess) is not part of the recon time."""
     from oracle import oracle as O
     ncpu = os.cpu_count() or 1
-    O.set_fft_workers(ncpu)
-    N, mos, W = wl["N"], wl["mos"], wl["W"]
-    P = O.OraclePlan(N, mos, W)
-    P.preprocess(wl["traj"][None])
-    sq = wl["sqrt_dcw"].reshape(1, -1)
-    E = O.OracleSense(P, wl["csm"], sq)
-    d = (d_host * sq)[:, None, :]
+    H = O.HoSenseFloat(wl["N"], wl["mos"], wl["W"], wl["traj"], wl["csm"], wl["sqrt_dcw"], workers=ncpu)
+    d = (d_host * wl["sqrt_dcw"].reshape(1, -1)).astype(np.complex64)
     t0 = time.perf_counter()
-    rhs = E.mult_MH(d)
+    rhs = H.mult_MH(d)
     t_rhs = time.perf_counter() - t0
-    x = np.zeros_like(rhs)
     r = rhs.copy()
     p = r.copy()
-    rq = float(np.real(np.vdot(r, r)))
+    x = np.zeros_like(rhs)
+    rq = np.float32(np.real(np.vdot(r, r)))
     times = []
-    for it in range(iters_timed):
+    for _ in range(iters_timed):
         t0 = time.perf_counter()
-        q = E.mult_MH_M(p)
-        alpha = rq / np.vdot(p.ravel(), q.ravel())
-        x = x + alpha * p
-        r = r - alpha * q
-        rq2 = float(np.real(np.vdot(r, r)))
-        p = p * (rq2 / rq) + r
+        q = H.mult_MH_M(p)
+        alpha = np.complex64(rq / np.vdot(p, q))
+        x += alpha * p
+        r -= alpha * q
+        rq2 = np.float32(np.real(np.vdot(r, r)))
+        p = p * np.float32(rq2 / rq) + r
         rq = rq2
         times.append(time.perf_counter() - t0)
     t_iter = float(np.mean(times))
@@ -394,40 +396,58 @@ def cpu_cg_sample(wl, d_host, iters_timed=3):
     return ms, ncpu, t_rhs, t_iter
 
 
-def run_reference(args):
-    """The reference arm: the reference algorithm's CPU restatement, timed on
-    the host cores.  Each step is one CG iteration of the full workload; the
-    recon time is one measured E^H d plus 10 x the mean iteration time."""
+def make_noisy_data_cpu(wl):
+    """The workload's k-space on the host: FP64 oracle forward operator plus
+    1% RMS complex noise (the same seed as the GPU arm's data)."""
     from oracle import oracle as O
-    wl = make_workload()
-    ncpu = os.cpu_count() or 1
-    O.set_fft_workers(ncpu)
-    N, mos, W = wl["N"], wl["mos"], wl["W"]
-    P = O.OraclePlan(N, mos, W)
+    P = O.OraclePlan(wl["N"], wl["mos"], wl["W"])
     P.preprocess(wl["traj"][None])
-    sq = wl["sqrt_dcw"].reshape(1, -1)
-    E = O.OracleSense(P, wl["csm"], sq)
+    E = O.OracleSense(P, wl["csm"], wl["sqrt_dcw"].reshape(1, -1))
     d = E.mult_M(wl["phantom"]).astype(np.complex128)
     rng = np.random.default_rng(CFG["seed"] + 1)
     rms = np.sqrt(np.mean(np.abs(d) ** 2))
     d = d + CFG["noise"] * rms * (rng.standard_normal(d.shape) + 1j * rng.standard_normal(d.shape)) / np.sqrt(2)
+    return E, d
+
+
+def run_reference(args):
+    """The reference arm: the reference's CPU reconstruction path in its own
+    float arithmetic (oracle.HoSenseFloat: hoGriddingConvolution's
+    per-sample convolution matrix and its transpose, complext<float> sums,
+    OpenMP over coils; complex64 FFT on every host thread; the cgSolver
+    iteration in complex64), timed on the host cores.  Each step is one CG
+    iteration of the full workload (E^H E p and the vector updates); the
+    recon time is one measured E^H d plus 10 x the mean iteration time.  The
+    convolution-matrix build (the reference's preprocess) is timed on its
+    own.  Loads no CUDA library."""
+    from oracle import oracle as O
+    wl = make_workload()
+    ncpu = os.cpu_count() or 1
+    E64, d64 = make_noisy_data_cpu(wl)
+    d = d64.reshape(CFG["coils"], -1).astype(np.complex64)
     t0 = time.perf_counter()
-    rhs = E.mult_MH(d)
+    H = O.HoSenseFloat(wl["N"], wl["mos"], wl["W"], wl["traj"], wl["csm"], wl["sqrt_dcw"], workers=ncpu)
+    t_prep = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    rhs = H.mult_MH(d)
     t_rhs = time.perf_counter() - t0
     x = np.zeros_like(rhs)
     r = rhs.copy()
     p = r.copy()
-    rq = float(np.real(np.vdot(r, r)))
+    rq = np.float32(np.real(np.vdot(r, r)))
+    state = {"x": x, "r": r, "p": p, "rq": rq, "it": 0, "x10": None}
 
     def step():
-        nonlocal x, r, p, rq
-        q = E.mult_MH_M(p)
-        alpha = rq / np.vdot(p.ravel(), q.ravel())
-        x = x + alpha * p
-        r = r - alpha * q
-        rq2 = float(np.real(np.vdot(r, r)))
-        p = p * (rq2 / rq) + r
-        rq = rq2
+        q = H.mult_MH_M(state["p"])
+        alpha = np.complex64(state["rq"] / np.vdot(state["p"], q))
+        state["x"] += alpha * state["p"]
+        state["r"] -= alpha * q
+        rq2 = np.float32(np.real(np.vdot(state["r"], state["r"])))
+        state["p"] = state["p"] * np.float32(rq2 / state["rq"]) + state["r"]
+        state["rq"] = rq2
+        state["it"] += 1
+        if state["it"] == CFG["iterations"]:
+            state["x10"] = state["x"].copy()
 
     for _ in range(args.warmup):
         step()
@@ -438,19 +458,26 @@ def run_reference(args):
         times.append(time.perf_counter() - t0)
     t_iter = float(np.mean(times))
     value = (t_rhs + CFG["iterations"] * t_iter) * 1e3
-    sample = ("%d timed CG iterations (E^H E + updates) of the full workload, recon = one measured E^H d "
-              "+ %d x mean iteration" % (args.steps, CFG["iterations"]))
+    acc = None
+    if state["x10"] is not None:
+        xr = O.cg_solve(E64, d64, iterations=CFG["iterations"], tc_tolerance=0.0)
+        acc = O.rel_l2(state["x10"], xr)
+    sample = ("%d timed CG iterations (E^H E + updates) of the full workload; recon = one measured E^H d "
+              "+ %d x mean iteration; float CSR gridding (OpenMP over %d coils), complex64 pocketfft FFT on "
+              "%d threads standing in for FFTW" % (args.steps, CFG["iterations"], CFG["coils"], ncpu))
     return {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_iter * 1e3, 3), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c128 (fp64 sums, fp32 kernel weights)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32, complext<float> as the reference)",
         "data": "synthetic (seeded)", "impl": "reference",
         "config": {"workload": "cg-sense-2d-radial", "matrix": 256, "matrix_os": 512, "W": CFG["W"],
                    "coils": CFG["coils"], "spokes": CFG["spokes"], "samples_per_spoke": CFG["samples"],
-                   "iterations": CFG["iterations"], "parallelism": "host cores"},
+                   "iterations": CFG["iterations"], "tc_tolerance": 0.0, "parallelism": "host cores"},
         "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": ncpu, "kind": "port",
                          "sample": sample},
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "preprocess_ms": round(t_prep * 1e3, 2),
+        "recon_rel_l2_vs_fp64_oracle_cg": acc,
     }
 
 
@@ -878,6 +905,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline line without the NUFFT/preprocess/batched/reference-GPU figures")
     ap.add_argument("--workload", default="cg-sense-2d",
                     choices=["cg-sense-2d", "nufft-2d", "nufft-3d", "batched", "precision", "regularised"])
     ap.add_argument("--clocks-csv", default=None,
@@ -923,18 +952,138 @@ def main():
         if world == 1 and not args.no_cpu_baseline:
             ms, ncpu, t_rhs, t_iter = cpu_cg_sample(wl, d_host)
             result["cpu_baseline"] = {"value": round(ms, 2), "unit": UNIT, "cores": ncpu, "kind": "port",
-                                      "sample": "one E^H d + 3 CG iterations of the full workload on the oracle "
-                                                "port (C/OpenMP gridding, scipy.fft threads), scaled to 10 iterations"}
+                                      "sample": "one E^H d + 3 CG iterations of the full workload on the reference's "
+                                                "CPU path restated in float (CSR gridding, OpenMP over coils; "
+                                                "complex64 pocketfft threads), scaled to 10 iterations"}
         try:
             result["accuracy"] = accuracy_report(wl, d_host, x_out)
         except Exception as e:  # accuracy is reported, never gates the timing
             result["accuracy"] = {"error": str(e)}
+        if world == 1 and not args.no_extras:
+            try:
+                result.update(headline_extras(args, wl, d_host, x_out))
+            except Exception as e:  # reported, never gates the timing
+                result["extras_error"] = str(e)
         print(json.dumps(result), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _copy_args(args, **kw):
+    a = argparse.Namespace(**vars(args))
+    for k, v in kw.items():
+        setattr(a, k, v)
+    return a
+
+
+def headline_extras(args, wl, d_host, x_out):
+    """Figures the headline line carries besides the CG-SENSE time (N = 1
+    only; computed after the timed region, never inside it):
+
+    preprocess_ms  -- the SENSE operator's preprocess of the 49152-sample
+                      trajectory alone (device time, CUDA events, L2 flushed);
+    nufft_2d       -- the metric's first half: NUFFT forward C2NC + adjoint
+                      NC2C throughput on 128^2, one coil, 128 golden-angle
+                      spokes x 256 samples, alpha 2, W 5.5, with its error
+                      against the reference's own cuNFFT and the FP64 NDFT;
+    batched        -- 64 uneven frames (192^2, 12 coils, 15 iterations):
+                      batched graph-captured solve vs the plain per-frame form;
+    reference_gpu  -- the reference's own GPU path (built from its sources)
+                      on the same B200: cuCgSolver ms/recon on this workload
+                      and cuNFFT on the 2D NUFFT case, and the product's
+                      per-iteration rel-L2 against the reference's iterates."""
+    import torch
+    import gadgetron_b200 as gb
+    from gadgetron_b200 import synthetic as S
+    from oracle import oracle as O
+    from oracle import ref as R
+    dev = x_out.device
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    out = {}
+    # --- preprocess alone
+    traj_d = torch.from_numpy(wl["traj"]).to(dev)
+    E3 = gb.cuNonCartesianSenseOperator(2)
+    E3.setup(wl["N"], wl["mos"], wl["W"])
+    out["preprocess_ms"] = round(_timed(lambda: E3.preprocess(traj_d), 10, 3, flush, stream), 4)
+
+    # --- NUFFT 2D forward + adjoint (single coil)
+    N2, mos2, W2 = (128, 128), (256, 256), 5.5
+    traj2 = S.radial_golden_angle_2d(128, 256)
+    dcw2 = S.ramp_dcw(traj2)
+    img2 = S.gaussian_image((1, 1, 128, 128), 11)
+    M2 = traj2.shape[0]
+    plan2 = gb.NFFT.make_plan(N2, mos2, W2)
+    plan2.preprocess(torch.from_numpy(traj2).to(dev))
+    x2 = torch.from_numpy(img2).to(dev)
+    w2 = torch.from_numpy(dcw2).to(dev)
+    y2 = torch.empty((1, M2), dtype=torch.complex64, device=dev)
+    xb2 = torch.empty_like(x2)
+    t_f = _timed(lambda: plan2.compute(x2, y2, None, gb.NFFT_comp_mode.FORWARDS_C2NC), 20, 3, flush, stream)
+    t_a = _timed(lambda: plan2.compute(y2, xb2, w2, gb.NFFT_comp_mode.BACKWARDS_NC2C), 20, 3, flush, stream)
+    nu = {"value": round(M2 / ((t_f + t_a) * 1e-3) / 1e6, 2), "unit": "Msample-coils/s",
+          "ms_forward": round(t_f, 4), "ms_adjoint": round(t_a, 4),
+          "config": {"workload": "nufft-2d-radial", "matrix": 128, "matrix_os": 256, "W": 5.5, "coils": 1,
+                     "samples": M2, "l2": "flushed before every timed call"}}
+    idx = np.random.default_rng(5).choice(M2, 4096, replace=False)
+    yn = O.ndft_forward(img2[0, 0][None], traj2[idx], mos2)
+    nu["forward_rel_l2_vs_fp64_ndft"] = O.rel_l2(y2[0].cpu().numpy()[idx], yn[0])
+    ref_gpu = {}
+    if R.available():
+        y_ref = R.nfft_compute(N2, mos2, W2, traj2, 1, img2, None, "FORWARDS_C2NC")
+        x_ref = R.nfft_compute(N2, mos2, W2, traj2, 1, y2.cpu().numpy(), dcw2, "BACKWARDS_NC2C")
+        nu["forward_rel_l2_vs_reference"] = O.rel_l2(y2.cpu().numpy(), y_ref)
+        nu["adjoint_rel_l2_vs_reference"] = O.rel_l2(xb2.cpu().numpy(), x_ref)
+        rf, ra, rp = R.time_nfft(N2, mos2, W2, traj2, 1, img2, dcw2, 1, reps=10)
+        ref_gpu["nufft_2d"] = {"ms_forward": round(rf, 4), "ms_adjoint": round(ra, 4),
+                               "ms_preprocess": round(rp, 4),
+                               "value": round(M2 / ((rf + ra) * 1e-3) / 1e6, 2), "unit": "Msample-coils/s"}
+    out["nufft_2d"] = nu
+
+    # --- batched uneven frames vs the plain per-frame form
+    try:
+        b = run_batched(_copy_args(args, steps=5, warmup=3, size="full", tiling=None))
+        out["batched"] = {k: b[k] for k in ("value", "unit", "plain_per_frame_ms", "speedup_vs_plain",
+                                            "batched_vs_plain_rel_l2", "tiling_after_autotune",
+                                            "gpu_launches_per_batch")}
+        out["batched"]["config"] = b["config"]
+    except Exception as e:  # reported, never gates the headline
+        out["batched"] = {"error": str(e)}
+
+    # --- the reference's own GPU path on this workload
+    if R.available():
+        sq = wl["sqrt_dcw"]
+        d = (d_host * sq.reshape(1, -1)).astype(np.complex64)
+        ms_ref = R.time_cg_sense(wl["N"], wl["mos"], wl["W"], wl["traj"], 1, wl["csm"], sq, d,
+                                 CFG["iterations"], reps=5)
+        ref_gpu["cg_sense_ms_per_recon"] = round(ms_ref, 3)
+        x_ref, its = R.cg_sense(wl["N"], wl["mos"], wl["W"], wl["traj"], 1, wl["csm"], sq, d,
+                                CFG["iterations"], 0.0, keep_iterates=True)
+        E = gb.cuNonCartesianSenseOperator(2)
+        E.setup(wl["N"], wl["mos"], wl["W"])
+        E.set_csm(torch.from_numpy(wl["csm"]).to(dev))
+        E.set_dcw(torch.from_numpy(sq).to(dev))
+        E.preprocess(traj_d)
+        cg = gb.cuCgSolver()
+        cg.set_encoding_operator(E)
+        cg.set_tc_tolerance(0.0)
+        d_t = torch.from_numpy(d).to(dev)
+        per_it = []
+        for k in range(1, CFG["iterations"] + 1):
+            cg.set_max_iterations(k)
+            per_it.append(O.rel_l2(cg.solve(d_t).cpu().numpy(), its[k - 1]))
+        ref_gpu["recon_rel_l2_vs_reference"] = O.rel_l2(x_out.cpu().numpy(), x_ref)
+        ref_gpu["per_iteration_rel_l2_vs_reference"] = [float("%.3g" % e) for e in per_it]
+        ref_gpu["note"] = ("reference cuNFFT/cuNonCartesianSenseOperator/cuCgSolver compiled from its sources "
+                           "for sm_100a, timed on this GPU with CUDA events (operator preprocessed, inputs "
+                           "resident)")
+    else:
+        ref_gpu["unavailable"] = "oracle/_ref/libgbref.so not built"
+    out["reference_gpu"] = ref_gpu
+    return out
 
 
 def accuracy_report(wl, d_host, x_out, n_sub=2048):

@@ -640,6 +640,13 @@ GB_API gb_status gb_cg_set_refinements(gb_cg_solver solver, uint32_t refinements
     });
 }
 
+GB_API gb_status gb_cg_set_barrier_spin_limit(gb_cg_solver solver, uint32_t spin_limit) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
+        solver->c.barrier_spin_limit = spin_limit;
+    });
+}
+
 GB_API gb_status gb_cg_set_frame_independent(gb_cg_solver solver, int independent) {
     return guarded([&] {
         if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");

@@ -518,14 +518,20 @@ struct TailArgs {
     double *hist;
     unsigned int *bar;       // grid barrier: arrival count, generation
     unsigned int *err;
+    uint32_t spin_limit;     // polls of a barrier wait before giving up
     float2 *pad;             // next iteration's padded image (outer-major), or null after the last iteration
     int pad_full;            // 1: whole band lines with their zeros (a cuFFT pass follows); 0: interior only
     int seg_rows;            // image rows (of N0 pixels) per segment
 };
 
 // Grid-wide barrier for a cooperative launch (all blocks resident).  The
-// wait is bounded: past ~4 s it records the failure in *err and returns.
-__device__ void tail_grid_barrier(unsigned int *bar, unsigned int nblocks, unsigned int *err) {
+// wait is bounded: after spin_limit polls (2^26 by default, about 4 s) the
+// block records the failure in bit 1 of *err and goes on.  Past such a
+// timeout the barrier counters no longer match the launch's phases, so the
+// host clears them before every solve, and the solve's values are void (the
+// caller learns it from the error word).
+__device__ void tail_grid_barrier(unsigned int *bar, unsigned int nblocks, unsigned int *err,
+                                  uint32_t spin_limit) {
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned int *vb = bar;
@@ -538,7 +544,7 @@ __device__ void tail_grid_barrier(unsigned int *bar, unsigned int nblocks, unsig
             atomicAdd(&bar[1], 1u);
         } else {
             for (uint32_t i = 0; vb[1] == gen; i++) {
-                if (i >= (1u << 26)) {
+                if (i >= spin_limit) {
                     atomicOr(err, 2u);
                     break;
                 }
@@ -634,7 +640,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
     }
     acc = block_reduce_d2(acc, sh);
     if (threadIdx.x == 0) t.part1[(size_t)seg * nbx + blockIdx.x] = acc;
-    tail_grid_barrier(t.bar, nblocks, t.err);
+    tail_grid_barrier(t.bar, nblocks, t.err, t.spin_limit);
 
     // Phase 2: alpha = rq / <p,q> ; x += alpha p ; r -= alpha q ; <r, P^2 r>.
     const double2 pq = tail_segment_sum(t.part1 + (size_t)seg * nbx, nbx, sh);
@@ -666,7 +672,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
     }
     acc = block_reduce_d2(acc, sh);
     if (threadIdx.x == 0) t.part2[(size_t)seg * nbx + blockIdx.x] = acc;
-    tail_grid_barrier(t.bar, nblocks, t.err);
+    tail_grid_barrier(t.bar, nblocks, t.err, t.spin_limit);
 
     // Phase 3: segment scalars, stop rule, history; then the direction update
     // p = beta p + P^2 r and the forward pad of p for the next iteration.
@@ -926,6 +932,7 @@ static void cg_iteration_fused(CgSolver &cg, cudaStream_t st, double *hist, bool
     ta.hist = hist;
     ta.bar = cg.tail_bar.get();
     ta.err = p.err_flag.get();
+    ta.spin_limit = cg.barrier_spin_limit ? cg.barrier_spin_limit : (1u << 26);
     ta.pad = last ? nullptr : pad;
     ta.pad_full = fft_custom_ok(p) ? 0 : 1;
     ta.seg_rows = (int)(cg.seg_len / p.kp.N[0]);
@@ -1025,6 +1032,9 @@ static void cg_record(CgSolver &cg, const float2 *d, float2 *x_out, double *hist
     SenseOp &s = *cg.E;
     NufftPlan &p = s.plan;
     const int64_t n = (int64_t)p.F * p.kp.NN;
+    // A grid barrier that timed out in an earlier solve leaves its counters
+    // out of step: start every solve from cleared ones.
+    if (cg.use_tail) GB_CUDA(cudaMemsetAsync(cg.tail_bar.get(), 0, 2 * sizeof(unsigned int), st));
     // rhs0 = weight * E^H d
     nufft_adjoint(p, d, LAYOUT_ORIGINAL, s.dcw, s.csm, s.ncoils, cg.rhs0.get(), false, false, cg.weight,
                   CUFFT_INVERSE, st);
@@ -1070,7 +1080,7 @@ void cg_solve(CgSolver &cg, const void *d, void *x_out, double *hist, uint32_t *
     if (cg.use_graph) {
         GraphKey key{d, x_out, hist, cg.iterations, cg.refinements, cg.x0, cg.precond, cg.reg, cg.kappa, cg.weight,
                      cg.tol, s.csm, s.dcw, s.ncoils, plan_layout_signature(s.plan, s.ncoils * (int)s.plan.F),
-                     cg.independent_frames};
+                     cg.independent_frames, cg.barrier_spin_limit};
         if (!cg.graph_exec || !(key == cg.graph_key)) {
             cudaStream_t cs;
             GB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));

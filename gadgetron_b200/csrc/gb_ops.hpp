@@ -28,8 +28,9 @@ struct GraphKey {
     int ncoils;
     uint64_t generation;
     bool independent;
+    uint32_t spin_limit;
     bool operator==(const GraphKey &o) const {
-        return generation == o.generation && independent == o.independent && d == o.d && x == o.x && hist == o.hist && iterations == o.iterations &&
+        return generation == o.generation && independent == o.independent && spin_limit == o.spin_limit && d == o.d && x == o.x && hist == o.hist && iterations == o.iterations &&
                refinements == o.refinements && x0 == o.x0 && precond == o.precond && reg == o.reg && kappa == o.kappa &&
                weight == o.weight && tol == o.tol && csm == o.csm && dcw == o.dcw && ncoils == o.ncoils;
     }
@@ -52,6 +53,10 @@ struct CgSolver {
     uint32_t refinements = 1;
     bool use_graph = false;
     bool independent_frames = false;   // per-frame CG scalars (frames solved independently)
+    // Polls of the fused tail's grid barrier before a block gives up (0: the
+    // default of 2^26, about 4 s); a diagnostic setting, see
+    // gb_cg_set_barrier_spin_limit.
+    uint32_t barrier_spin_limit = 0;
     int nseg = 1;
     int64_t seg_len = 0;
 

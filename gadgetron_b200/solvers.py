@@ -117,6 +117,11 @@ class cuCgSolver:
         self.refinements = int(n)
         check(lib.gb_cg_set_refinements(self._h, self.refinements))
 
+    def set_barrier_spin_limit(self, polls: int):
+        """Diagnostic: polls of the fused iteration's grid barrier before a
+        block gives up and flags bit 1 of the device error word (0: default)."""
+        check(lib.gb_cg_set_barrier_spin_limit(self._h, int(polls)))
+
     def set_use_graph(self, use: bool):
         check(lib.gb_cg_set_use_graph(self._h, int(bool(use))))
 

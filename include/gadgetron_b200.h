@@ -386,6 +386,14 @@ GB_API gb_status gb_sense_precond_weights(gb_sense_op op, const float *reg_image
 /* Outer iterative refinement: solve `refinements` times, each from the FP64
  * residual of the previous solution (x <- x + CG(E^H d - E^H E x)).  1 = off. */
 GB_API gb_status gb_cg_set_refinements(gb_cg_solver solver, uint32_t refinements);
+/* Diagnostic: how many times a block of the fused CG iteration polls the
+ * grid barrier before it gives up (0 = the default, 2^26 polls, about 4 s).
+ * A block that gives up sets bit 1 of the plan's device error word
+ * (gb_nufft_device_errors) and carries on, so a solve never hangs; that
+ * solve's values are void, and the next solve starts from cleared barrier
+ * counters.  A small limit makes the timeout path run on purpose (tests).
+ * No reference counterpart. */
+GB_API gb_status gb_cg_set_barrier_spin_limit(gb_cg_solver solver, uint32_t spin_limit);
 /* Solve the frames of a multi-frame operator as independent problems: each
  * frame gets its own CG scalars (rq, alpha, beta, stop flag) while every
  * kernel still covers all frames in one launch.  0 (default) = the

@@ -23,13 +23,26 @@
  *   - deapodization kernel image (a sample at mos/2):
  *                                              toolboxes/nfft/gpu/cuNFFT.cu:136-164
  *
- * Parity status: unpinned against reference outputs.  The reference cannot
- * be built here (its GPU path needs Boost and CMake-generated headers), and
- * its own tests hold no golden values for this path, so this restatement is
- * pinned instead by the known-answer case of the reference's cuNFFT test
- * (constant trajectory, analytic adjoint), norm preservation of the centred
- * FFT (its cuNDFFT test), the FP64 direct NDFT and exact adjointness
- * (tests/test_known_answers.py, tests/test_oracle.py).
+ * Parity status: pinned against the reference's own outputs.  The
+ * reference's GPU path (cuNFFT, cuNonCartesianSenseOperator, cuCgSolver) is
+ * built from its sources into oracle/_ref/libgbref.so (oracle/build_ref.py)
+ * and tests/test_ref_parity_gpu.py checks this restatement against it on the
+ * same seeded inputs (relative L2 <= 1e-5), besides the known-answer case of
+ * the reference's cuNFFT test, norm preservation of the centred FFT, the FP64
+ * direct NDFT and exact adjointness (tests/test_known_answers.py,
+ * tests/test_oracle.py).
+ *
+ * Fold of the padding ring (gridding, NC2C).  By default the ring is folded
+ * periodically: every tap lands on its cell modulo mos, once.  That is what
+ * the reference computes in 1D and 2D.  In 3D the reference's
+ * wrap_image_kernel (ConvolverNC2C_standard.cuh:394-437) selects the
+ * dimensions of each wrap combination with `i & combination` for i = 1..D,
+ * which for i = 3 tests bits 0|1 instead of bit 2: on cells within the ring
+ * width of a z face some periodic images are added twice and others not at
+ * all.  or_grid_nc2c_fold(..., fold = 1) restates that loop exactly (a
+ * per-cell multiplicity for each periodic image), so the oracle can be
+ * pinned to the reference in 3D too; the product and the default oracle keep
+ * the periodic fold, which the FP64 direct NDFT adjoint confirms.
  *
  * Kernel weights are computed in float exactly as the reference writes them
  * (host arithmetic, no fused multiply-add except the trajectory scaling, which
@@ -167,14 +180,60 @@ static inline int64_t or_wrap(int64_t x, int64_t m)
     return x < 0 ? x + m : x;
 }
 
+/* Multiplicity with which the reference's fold adds the periodic image at
+ * stride sigma (each component -1, 0, +1) to a cell whose per-dimension
+ * state is st (0 interior, 1 within the ring width of the low face, 2 of the
+ * high face): the combination/stride loop of wrap_image_kernel
+ * (ConvolverNC2C_standard.cuh:394-437), including its `i & combination`
+ * dimension test.  sigma = 0 (the cell itself) always counts once. */
+static int or_ref_fold_multiplicity(int D, const int *st, const int *sigma)
+{
+    int zero = 1;
+    for (int d = 0; d < D; d++)
+        zero &= sigma[d] == 0;
+    if (zero)
+        return 1;
+    int count = 0;
+    for (int comb = 1; comb < (1 << D); comb++) {
+        int nd = 0;
+        for (int i = 0; i < D; i++)
+            nd += (comb & (1 << i)) != 0;
+        for (int sel = 0; sel < (1 << nd); sel++) {
+            int stride[OR_MAXD], wraps = 0, skipped = 0;
+            for (int i = 1; i <= D; i++) {
+                stride[i - 1] = 0;
+                if (i & comb) {
+                    if (i & (sel << skipped)) {
+                        if (st[i - 1] == 2) { stride[i - 1] = -1; wraps++; }
+                    } else {
+                        if (st[i - 1] == 1) { stride[i - 1] = 1; wraps++; }
+                    }
+                } else {
+                    skipped++;
+                }
+            }
+            if (wraps == nd) {
+                int same = 1;
+                for (int d = 0; d < D; d++)
+                    same &= stride[d] == sigma[d];
+                count += same;
+                break;
+            }
+        }
+    }
+    return count;
+}
+
 /* Gridding NC2C (the adjoint convolution).  samples: [nb][F][M] complex
  * double; grid_out: [nb][F][prod(mos)] complex double, overwritten (or added
  * to when accumulate != 0).  scaled: [F][M] D-vectors from
- * or_scale_trajectory.  The padded-grid/wrap of the reference is reproduced
- * by folding each padded cell p onto (p - pad/2) mod mos. */
-void or_grid_nc2c(int D, const uint64_t *N, const uint64_t *mos, float W,
-                  int64_t M, int64_t F, int64_t nb, const float *scaled,
-                  const double *samples, double *grid_out, int accumulate)
+ * or_scale_trajectory.  The reference's padded grid and wrap pass are
+ * reproduced by folding each padded cell p onto (p - pad/2) mod mos, with
+ * multiplicity 1 (fold 0, periodic) or the reference's multiplicity (fold 1,
+ * see the header). */
+void or_grid_nc2c_fold(int D, const uint64_t *N, const uint64_t *mos, float W,
+                       int64_t M, int64_t F, int64_t nb, const float *scaled,
+                       const double *samples, double *grid_out, int accumulate, int fold)
 {
     or_plan p;
     or_plan_init(&p, D, N, mos, W);
@@ -204,21 +263,36 @@ void or_grid_nc2c(int D, const uint64_t *N, const uint64_t *mos, float W,
             for (int64_t t = 0; t < ntaps; t++) {
                 int64_t rem = t, idx = 0, stride = 1;
                 float delta[OR_MAXD];
+                int st[OR_MAXD], sigma[OR_MAXD];
                 for (int d = 0; d < D; d++) {
                     int64_t pc = lo[d] + rem % cnt[d];
                     rem /= cnt[d];
                     delta[d] = fabsf(s[d] - (float)pc);
-                    idx += or_wrap(pc - hw, p.mos[d]) * stride;
+                    const int64_t u = pc - hw;                 /* unwrapped cell */
+                    const int64_t co = or_wrap(u, p.mos[d]);
+                    sigma[d] = u < 0 ? -1 : (u >= p.mos[d] ? 1 : 0);
+                    st[d] = co < hw ? 1 : (co >= p.mos[d] - hw ? 2 : 0);
+                    idx += co * stride;
                     stride *= p.mos[d];
                 }
                 float w = or_kb_get(D, delta, p.mos_f, p.one_over_W, p.beta, p.radius);
                 if (!isfinite(w))
                     continue;
-                grid[2 * idx] += (double)w * yr;
-                grid[2 * idx + 1] += (double)w * yi;
+                double mult = 1.0;
+                if (fold == 1)
+                    mult = (double)or_ref_fold_multiplicity(D, st, sigma);
+                grid[2 * idx] += mult * (double)w * yr;
+                grid[2 * idx + 1] += mult * (double)w * yi;
             }
         }
     }
+}
+
+void or_grid_nc2c(int D, const uint64_t *N, const uint64_t *mos, float W,
+                  int64_t M, int64_t F, int64_t nb, const float *scaled,
+                  const double *samples, double *grid_out, int accumulate)
+{
+    or_grid_nc2c_fold(D, N, mos, W, M, F, nb, scaled, samples, grid_out, accumulate, 0);
 }
 
 /* Degridding C2NC (the forward convolution).  grid: [nb][F][prod(mos)]
@@ -503,5 +577,151 @@ void or_degrid_traj_grad(int D, const uint64_t *N, const uint64_t *mos, float W,
             }
         }
         for (int d = 0; d < D; d++) out[fj * D + d] = acc[d] * (double)p.mos_f[d];
+    }
+}
+
+/* ------------------------------------------------------------------------
+ * The reference's CPU gridding (hoGriddingConvolution with its
+ * ConvolutionMatrix), restated in float for the timed CPU baseline:
+ *   - scaling without padding, s = (k + 1/2) * mos:
+ *                                   toolboxes/nfft/cpu/hoGriddingConvolution.cpp:50-57
+ *   - per sample, the taps i in [ceil(s - W/2), floor(s + W/2)] per
+ *     dimension (last dimension outermost, x innermost), wrapped modulo mos,
+ *     weight kernel.get(|i - s|):    toolboxes/nfft/cpu/ConvolutionMatrix.cpp:18-76,84-100
+ *   - the transpose (per cell, its samples in increasing order):
+ *                                   ConvolutionMatrix.cpp:104-137
+ *   - C2NC: samples[j] += sum_n grid[idx[n]] * w[n];  NC2C: grid[g] +=
+ *     sum_n samples[j_n] * w_n, complext<float> arithmetic, OpenMP over the
+ *     batches (coils):              hoGriddingConvolution.cpp:86-150
+ * ------------------------------------------------------------------------ */
+
+typedef struct {
+    int64_t M, G;
+    int64_t *row_ptr;      /* [M+1] per sample */
+    uint32_t *row_idx;     /* grid cell of each tap */
+    float *row_w;
+    int64_t *col_ptr;      /* [G+1] per cell (transpose) */
+    uint32_t *col_idx;     /* sample of each tap */
+    float *col_w;
+} ho_matrix;
+
+void *ho_matrix_create(int D, const uint64_t *N, const uint64_t *mos, float W,
+                       const float *traj, int64_t M)
+{
+    or_plan p;
+    or_plan_init(&p, D, N, mos, W);
+    ho_matrix *m = (ho_matrix *)calloc(1, sizeof(ho_matrix));
+    int64_t G = 1;
+    for (int d = 0; d < D; d++) G *= p.mos[d];
+    m->M = M;
+    m->G = G;
+    m->row_ptr = (int64_t *)malloc(sizeof(int64_t) * (size_t)(M + 1));
+    /* pass 1: taps per sample */
+    m->row_ptr[0] = 0;
+    for (int64_t j = 0; j < M; j++) {
+        int64_t n = 1;
+        for (int d = 0; d < D; d++) {
+            const float s = (traj[j * D + d] + 0.5f) * p.mos_f[d];
+            n *= (int64_t)floorf(s + p.radius) - (int64_t)ceilf(s - p.radius) + 1;
+        }
+        m->row_ptr[j + 1] = m->row_ptr[j] + n;
+    }
+    const int64_t nnz = m->row_ptr[M];
+    m->row_idx = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)nnz);
+    m->row_w = (float *)malloc(sizeof(float) * (size_t)nnz);
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < M; j++) {
+        float s[OR_MAXD];
+        int64_t lo[OR_MAXD], cnt[OR_MAXD], stride[OR_MAXD];
+        int64_t ntaps = 1, st = 1;
+        for (int d = 0; d < D; d++) {
+            s[d] = (traj[j * D + d] + 0.5f) * p.mos_f[d];
+            lo[d] = (int64_t)ceilf(s[d] - p.radius);
+            cnt[d] = (int64_t)floorf(s[d] + p.radius) - lo[d] + 1;
+            stride[d] = st;
+            st *= p.mos[d];
+            ntaps *= cnt[d];
+        }
+        int64_t o = m->row_ptr[j];
+        for (int64_t t = 0; t < ntaps; t++) {
+            /* x innermost, the last dimension outermost */
+            int64_t rem = t, idx = 0;
+            float delta[OR_MAXD];
+            for (int d = 0; d < D; d++) {
+                const int64_t i = lo[d] + rem % cnt[d];
+                rem /= cnt[d];
+                delta[d] = fabsf((float)i - s[d]);
+                idx += ((i + p.mos[d]) % p.mos[d]) * stride[d];
+            }
+            m->row_idx[o] = (uint32_t)idx;
+            m->row_w[o] = or_kb_get(D, delta, p.mos_f, p.one_over_W, p.beta, p.radius);
+            o++;
+        }
+    }
+    /* transpose by counting sort over cells (samples stay in order) */
+    m->col_ptr = (int64_t *)calloc((size_t)(G + 1), sizeof(int64_t));
+    for (int64_t n = 0; n < nnz; n++) m->col_ptr[m->row_idx[n] + 1]++;
+    for (int64_t g = 0; g < G; g++) m->col_ptr[g + 1] += m->col_ptr[g];
+    m->col_idx = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)nnz);
+    m->col_w = (float *)malloc(sizeof(float) * (size_t)nnz);
+    int64_t *fill = (int64_t *)malloc(sizeof(int64_t) * (size_t)G);
+    memcpy(fill, m->col_ptr, sizeof(int64_t) * (size_t)G);
+    for (int64_t j = 0; j < M; j++)
+        for (int64_t n = m->row_ptr[j]; n < m->row_ptr[j + 1]; n++) {
+            const int64_t at = fill[m->row_idx[n]]++;
+            m->col_idx[at] = (uint32_t)j;
+            m->col_w[at] = m->row_w[n];
+        }
+    free(fill);
+    return m;
+}
+
+void ho_matrix_destroy(void *h)
+{
+    ho_matrix *m = (ho_matrix *)h;
+    if (!m) return;
+    free(m->row_ptr); free(m->row_idx); free(m->row_w);
+    free(m->col_ptr); free(m->col_idx); free(m->col_w);
+    free(m);
+}
+
+/* grid: [nb][G] complex float; samples: [nb][M] complex float */
+void ho_c2nc(void *h, int64_t nb, const float *grid, float *samples, int accumulate)
+{
+    const ho_matrix *m = (const ho_matrix *)h;
+#pragma omp parallel for schedule(static)
+    for (int64_t b = 0; b < nb; b++) {
+        const float *g = grid + 2 * b * m->G;
+        float *y = samples + 2 * b * m->M;
+        for (int64_t j = 0; j < m->M; j++) {
+            float re = accumulate ? y[2 * j] : 0.0f, im = accumulate ? y[2 * j + 1] : 0.0f;
+            for (int64_t n = m->row_ptr[j]; n < m->row_ptr[j + 1]; n++) {
+                const float w = m->row_w[n];
+                re += g[2 * (int64_t)m->row_idx[n]] * w;
+                im += g[2 * (int64_t)m->row_idx[n] + 1] * w;
+            }
+            y[2 * j] = re;
+            y[2 * j + 1] = im;
+        }
+    }
+}
+
+void ho_nc2c(void *h, int64_t nb, const float *samples, float *grid, int accumulate)
+{
+    const ho_matrix *m = (const ho_matrix *)h;
+#pragma omp parallel for schedule(static)
+    for (int64_t b = 0; b < nb; b++) {
+        const float *y = samples + 2 * b * m->M;
+        float *g = grid + 2 * b * m->G;
+        for (int64_t c = 0; c < m->G; c++) {
+            float re = accumulate ? g[2 * c] : 0.0f, im = accumulate ? g[2 * c + 1] : 0.0f;
+            for (int64_t n = m->col_ptr[c]; n < m->col_ptr[c + 1]; n++) {
+                const float w = m->col_w[n];
+                re += y[2 * (int64_t)m->col_idx[n]] * w;
+                im += y[2 * (int64_t)m->col_idx[n] + 1] * w;
+            }
+            g[2 * c] = re;
+            g[2 * c + 1] = im;
+        }
     }
 }

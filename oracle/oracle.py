@@ -4,11 +4,15 @@ This module is the checker for the CUDA library in ``gadgetron_b200``.  Only
 ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` import it; the product never does.
 
-Parity status: unpinned against reference outputs (the reference is not
-buildable here and its tests hold no golden values for this path); the
-restatement is pinned by the reference's own known-answer test setups, the
-FP64 direct NDFT and exact adjointness (tests/test_known_answers.py,
-tests/test_oracle.py).
+Parity status: pinned against the reference's own outputs.  The reference's
+GPU path is built from its sources (oracle/build_ref.py -> oracle/_ref) and
+tests/test_ref_parity_gpu.py checks this restatement against it on the same
+seeded inputs (NUFFT in 2D and 3D, SENSE operator, CG iterates), besides the
+reference's own known-answer test setups, the FP64 direct NDFT and exact
+adjointness (tests/test_known_answers.py, tests/test_oracle.py).  In 3D the
+reference folds the gridding's padding ring differently from the periodic
+fold near z faces; ``OraclePlan(..., reference_fold=True)`` restates that
+fold so the 3D adjoint is pinned as well (see nufft_oracle.c).
 
 It restates the reference GPU path (Gadgetron cuNFFT, STANDARD convolution,
 cuNonCartesianSenseOperator and cgSolver) on the CPU:
@@ -100,6 +104,13 @@ def lib():
         L.or_scale_trajectory.restype = ctypes.c_int
         L.or_scale_trajectory.argtypes = [ctypes.c_int, P, P, f32, P, i64, P]
         L.or_grid_nc2c.argtypes = [ctypes.c_int, P, P, f32, i64, i64, i64, P, P, P, ctypes.c_int]
+        L.ho_matrix_create.restype = P
+        L.ho_matrix_create.argtypes = [ctypes.c_int, P, P, f32, P, i64]
+        L.ho_matrix_destroy.argtypes = [P]
+        L.ho_c2nc.argtypes = [P, i64, P, P, ctypes.c_int]
+        L.ho_nc2c.argtypes = [P, i64, P, P, ctypes.c_int]
+        L.or_grid_nc2c_fold.argtypes = [ctypes.c_int, P, P, f32, i64, i64, i64, P, P, P, ctypes.c_int,
+                                        ctypes.c_int]
         L.or_degrid_c2nc.argtypes = [ctypes.c_int, P, P, f32, i64, i64, i64, P, P, P, ctypes.c_int]
         L.or_deapod_kernel_image.argtypes = [ctypes.c_int, P, P, f32, P]
         L.or_ndft_forward.argtypes = [ctypes.c_int, P, ctypes.c_double, i64, i64, P, P, P, P]
@@ -210,9 +221,16 @@ def crop(grid: np.ndarray, N, D: int) -> np.ndarray:
 # ------------------------------------------------------------------ plan ----
 
 class OraclePlan:
-    """CPU restatement of cuNFFT_impl<float, D, STANDARD>."""
+    """CPU restatement of cuNFFT_impl<float, D, STANDARD>.
 
-    def __init__(self, N, mos, W):
+    reference_fold=True folds the gridding's padding ring as the reference's
+    wrap_image_kernel does (ConvolverNC2C_standard.cuh:394-437), which in 3D
+    differs from the periodic fold on cells near a z face (see
+    nufft_oracle.c); the default is the periodic fold the product computes.
+    """
+
+    def __init__(self, N, mos, W, reference_fold=False):
+        self.fold = 1 if reference_fold else 0
         self.D = len(N)
         self.N = tuple(int(n) for n in N)
         self.mos = tuple(int(m) for m in mos)
@@ -278,9 +296,9 @@ class OraclePlan:
         s = np.ascontiguousarray(samples, dtype=np.complex128).reshape(nb, self.F, self.M)
         out = (np.zeros((nb, self.F) + self.mos[::-1], np.complex128) if accumulate_into is None
                else np.ascontiguousarray(accumulate_into, dtype=np.complex128).copy())
-        lib().or_grid_nc2c(self.D, _p(_u64(self.N)), _p(_u64(self.mos)), np.float32(self.W),
-                           self.M, self.F, nb, _p(self._scaled), _p(s), _p(out),
-                           0 if accumulate_into is None else 1)
+        lib().or_grid_nc2c_fold(self.D, _p(_u64(self.N)), _p(_u64(self.mos)), np.float32(self.W),
+                                self.M, self.F, nb, _p(self._scaled), _p(s), _p(out),
+                                0 if accumulate_into is None else 1, self.fold)
         return out
 
     def deapodize(self, image: np.ndarray, fourier_domain: bool = False) -> np.ndarray:
@@ -360,6 +378,104 @@ class OraclePlan:
         return self.traj_grad_from_grid(self.forward_grid(image), w)
 
 
+# ------------------------------------------- reference CPU path (float) ------
+
+class HoSenseFloat:
+    """The reference's CPU reconstruction path in its own float arithmetic,
+    for the timed CPU baseline: gridding by the per-sample convolution matrix
+    and its transpose of hoGriddingConvolution (ho_matrix_* in
+    nufft_oracle.c, complext<float> sums, OpenMP over coils), the centred FFT
+    in complex64 (pocketfft through scipy.fft with every host thread, standing
+    in for the FFTW the reference links), deapodization, csm multiply and the
+    cgSolver iteration (cgSolver.h:105-390) in complex64 with float dots.
+    Same operator as OracleSense: E = D^(1/2) NUFFT S."""
+
+    def __init__(self, N, mos, W, traj, csm, dcw, workers=None):
+        import scipy.fft as sfft
+        self._fft = sfft
+        self.D = len(N)
+        self.N = tuple(int(n) for n in N)
+        self.mos = tuple(int(m) for m in mos)
+        self.W = float(np.float32(W))
+        self.workers = workers or (os.cpu_count() or 1)
+        traj = np.ascontiguousarray(traj, np.float32).reshape(-1, self.D)
+        self.M = traj.shape[0]
+        self.G = int(np.prod(self.mos))
+        self._h = lib().ho_matrix_create(self.D, _p(_u64(self.N)), _p(_u64(self.mos)), np.float32(self.W),
+                                         _p(traj), self.M)
+        plan = OraclePlan(N, mos, W)
+        self.deap = plan.deapodization_filter(False).astype(np.complex64)
+        self.csm = np.ascontiguousarray(csm, np.complex64)
+        self.C = self.csm.shape[0]
+        self.dcw = np.ascontiguousarray(dcw, np.float32).reshape(1, -1)
+        self.scale = np.float32(1.0 / np.sqrt(self.G))
+        ax = tuple(range(-self.D, 0))
+        self._axes = ax
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().ho_matrix_destroy(self._h)
+            self._h = None
+
+    def _cfft(self, a, forward):
+        f = self._fft
+        a = f.ifftshift(a, axes=self._axes)
+        a = (f.fftn if forward else f.ifftn)(a, axes=self._axes, workers=self.workers,
+                                             norm="ortho", overwrite_x=True)
+        return f.fftshift(a, axes=self._axes).astype(np.complex64, copy=False)
+
+    def _pad(self, img):
+        out = np.zeros((img.shape[0],) + self.mos[::-1], np.complex64)
+        sl = tuple(slice((m - n) // 2, (m - n) // 2 + n) for n, m in zip(self.N[::-1], self.mos[::-1]))
+        out[(slice(None),) + sl] = img
+        return out
+
+    def _crop(self, grid):
+        sl = tuple(slice((m - n) // 2, (m - n) // 2 + n) for n, m in zip(self.N[::-1], self.mos[::-1]))
+        return np.ascontiguousarray(grid[(slice(None),) + sl])
+
+    def mult_M(self, x):
+        """x [*N] -> samples [C, M]."""
+        g = self._pad(self.csm * x[None])
+        g *= self.deap
+        g = self._cfft(g, True)
+        y = np.empty((self.C, self.M), np.complex64)
+        lib().ho_c2nc(self._h, self.C, _p(g), _p(y), 0)
+        y *= self.dcw
+        return y
+
+    def mult_MH(self, y):
+        """samples [C, M] -> image [*N]."""
+        ys = np.ascontiguousarray(y * self.dcw, np.complex64)
+        g = np.empty((self.C,) + self.mos[::-1], np.complex64)
+        lib().ho_nc2c(self._h, self.C, _p(ys), _p(g), 0)
+        g = self._cfft(g, False)
+        g *= self.deap
+        return np.sum(self._crop(g) * np.conj(self.csm), axis=0)
+
+    def mult_MH_M(self, x):
+        return self.mult_MH(self.mult_M(x))
+
+    def cg(self, d, iterations, snapshot=None):
+        """cgSolver iteration in complex64 (tc_tolerance 0).  Returns a
+        generator that yields after every iteration, so a caller can time
+        single iterations; x is in self.x."""
+        rhs = self.mult_MH(d)
+        self.x = np.zeros_like(rhs)
+        r = rhs.copy()
+        p = r.copy()
+        rq = np.float32(np.real(np.vdot(r, r)))
+        for _ in range(iterations):
+            q = self.mult_MH_M(p)
+            alpha = np.complex64(rq / np.vdot(p, q))
+            self.x += alpha * p
+            r -= alpha * q
+            rq2 = np.float32(np.real(np.vdot(r, r)))
+            p = p * np.float32(rq2 / rq) + r
+            rq = rq2
+            yield self.x
+
+
 # --------------------------------------------------------------- SENSE ------
 
 class OracleSense:
@@ -423,6 +539,30 @@ def sense_precond_weights(csm: np.ndarray, reg_image=None, kappa: float = 0.0) -
     if reg_image is not None:
         w = w + kappa * np.asarray(reg_image, np.float64)
     return 1.0 / np.sqrt(w)
+
+
+def cg_solve_refined(op, d: np.ndarray, iterations: int, refinements: int):
+    """Outer iterative refinement around cg_solve (new surface, no reference
+    counterpart): x_0 = 0; for k = 0..R-1, solve the normal equations for the
+    residual right-hand side b - A x_k with `iterations` CG steps from zero
+    and add the correction.  complex128 throughout."""
+    rhs0 = op.mult_MH(d)
+    x = np.zeros_like(rhs0)
+
+    class _Res:
+        def __init__(self, rhs):
+            self.rhs = rhs
+
+        def mult_MH(self, _):
+            return self.rhs
+
+        def mult_MH_M(self, v):
+            return op.mult_MH_M(v)
+
+    for k in range(refinements):
+        rhs = rhs0 if k == 0 else rhs0 - op.mult_MH_M(x)
+        x = x + cg_solve(_Res(rhs), None, iterations=iterations, tc_tolerance=0.0)
+    return x
 
 
 def cg_solve(op, d: np.ndarray, iterations: int = 10, tc_tolerance: float = 1e-3,

@@ -49,7 +49,10 @@ def lib():
         L.gbref_sense_mult.argtypes = [i, u64p, u64p, f, fp, u64, u64, vp, u64, fp, vp, vp, i]
         L.gbref_cg_sense.argtypes = [i, u64p, u64p, f, fp, u64, u64, vp, u64, fp, vp, vp, i, f, vp,
                                      ctypes.POINTER(ctypes.c_int)]
-        for name in ("gbref_nfft_compute", "gbref_nfft_mult_MH_M", "gbref_nfft_convolve",
+        fpp = ctypes.POINTER(ctypes.c_float)
+        L.gbref_time_cg_sense.argtypes = [i, u64p, u64p, f, fp, u64, u64, vp, u64, fp, vp, i, i, fpp]
+        L.gbref_time_nfft.argtypes = [i, u64p, u64p, f, fp, u64, u64, vp, fp, u64, i, fpp, fpp, fpp]
+        for name in ("gbref_time_cg_sense", "gbref_time_nfft", "gbref_nfft_compute", "gbref_nfft_mult_MH_M", "gbref_nfft_convolve",
                      "gbref_nfft_fft_deapodize", "gbref_sense_mult", "gbref_cg_sense"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
@@ -182,3 +185,32 @@ def cg_sense(N, mos, W, traj, frames, csm, dcw, data, iterations, tc_tolerance=0
     if keep_iterates:
         return x, its[:ran.value]
     return x
+
+
+def time_cg_sense(N, mos, W, traj, frames, csm, dcw, data, iterations, reps=5):
+    """Device ms of one reference cuCgSolver::solve (tc_tolerance 0) on the
+    current GPU, operator preprocessed, inputs resident."""
+    D = len(N)
+    t, tp = _traj(traj, D)
+    M = t.shape[0] // frames
+    csm = _c64(csm)
+    keep, dp = (None, None) if dcw is None else _f32(dcw)
+    d = _c64(data)
+    ms = ctypes.c_float(0)
+    _check(lib().gbref_time_cg_sense(D, _u64(N), _u64(mos), float(W), tp, M, frames, csm.ctypes.data, csm.shape[0],
+                                     dp, d.ctypes.data, int(iterations), int(reps), ctypes.byref(ms)))
+    return float(ms.value)
+
+
+def time_nfft(N, mos, W, traj, frames, img, dcw, batches=1, reps=5):
+    """Device ms of the reference's preprocess, compute(FORWARDS_C2NC) and
+    compute(BACKWARDS_NC2C, dcw): (fwd, adj, preprocess)."""
+    D = len(N)
+    t, tp = _traj(traj, D)
+    M = t.shape[0] // frames
+    x = _c64(img)
+    keep, dp = (None, None) if dcw is None else _f32(dcw)
+    a, b, c = ctypes.c_float(0), ctypes.c_float(0), ctypes.c_float(0)
+    _check(lib().gbref_time_nfft(D, _u64(N), _u64(mos), float(W), tp, M, frames, x.ctypes.data, dp, batches,
+                                 int(reps), ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+    return float(a.value), float(b.value), float(c.value)

@@ -237,6 +237,66 @@ int cg_sense(const uint64_t *n, const uint64_t *mos, float W, const float *traj,
     return 0;
 }
 
+// Device time of fn() on the legacy default stream (the stream the
+// reference runs on), averaged over reps after two warm-up calls.
+template <class Fn> float time_ms(int reps, Fn &&fn) {
+    for (int i = 0; i < 2; i++) fn();
+    cudaEvent_t a, b;
+    cuda_ok(cudaEventCreate(&a), "event");
+    cuda_ok(cudaEventCreate(&b), "event");
+    float total = 0.f;
+    for (int i = 0; i < reps; i++) {
+        cuda_ok(cudaEventRecord(a, 0), "record");
+        fn();
+        cuda_ok(cudaEventRecord(b, 0), "record");
+        cuda_ok(cudaEventSynchronize(b), "sync");
+        float ms = 0.f;
+        cuda_ok(cudaEventElapsedTime(&ms, a, b), "elapsed");
+        total += ms;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return total / (float)reps;
+}
+
+// Times one cuCgSolver::solve (E^H d and `iterations` iterations, everything
+// the reference does per call) with the operator set up and preprocessed.
+template <unsigned D>
+int time_cg_sense(const uint64_t *n, const uint64_t *mos, float W, const float *traj, uint64_t M, uint64_t F,
+                  const void *csm, uint64_t C, const float *dcw, const void *data, int iterations, int reps,
+                  float *ms) {
+    auto E = make_sense<D>(n, mos, W, traj, M, F, csm, C, dcw);
+    cuCgSolver<complext<float>> cg;
+    cg.set_encoding_operator(E);
+    cg.set_max_iterations((unsigned)iterations);
+    cg.set_tc_tolerance(0.f);
+    auto d = upload<complext<float>>({(size_t)(M * F), (size_t)C}, data);
+    *ms = time_ms(reps, [&] { auto x = cg.solve(&d); (void)x; });
+    return 0;
+}
+
+// Times compute(FORWARDS_C2NC) and compute(BACKWARDS_NC2C, dcw) on a
+// preprocessed plan; also the preprocess itself.
+template <unsigned D>
+int time_nfft(const uint64_t *n, const uint64_t *mos, float W, const float *traj, uint64_t M, uint64_t F,
+              const void *img, const float *dcw, uint64_t B, int reps, float *ms_fwd, float *ms_adj,
+              float *ms_prep) {
+    auto plan = NFFT<cuNDArray, float, D>::make_plan(vec<D>(n), vec<D>(mos), W, ConvolutionType::STANDARD);
+    auto t = upload_traj<D>(traj, M, F);
+    *ms_prep = time_ms(reps, [&] { plan->preprocess(t, NFFT_prep_mode::ALL); });
+    std::vector<size_t> im = dims_of<D>(n);
+    im.push_back((size_t)F);
+    im.push_back((size_t)B);
+    auto x = upload<complext<float>>(im, img);
+    cuNDArray<complext<float>> y(std::vector<size_t>{(size_t)M, (size_t)F, (size_t)B});
+    cuNDArray<complext<float>> xb(im);
+    cuNDArray<float> w;
+    if (dcw) w = upload<float>({(size_t)M, (size_t)F}, dcw);
+    *ms_fwd = time_ms(reps, [&] { plan->compute(x, y, nullptr, NFFT_comp_mode::FORWARDS_C2NC); });
+    *ms_adj = time_ms(reps, [&] { plan->compute(y, xb, dcw ? &w : nullptr, NFFT_comp_mode::BACKWARDS_NC2C); });
+    return 0;
+}
+
 template <class Fn> int guarded(Fn &&fn) {
     try {
         g_err.clear();
@@ -317,6 +377,26 @@ int gbref_cg_sense(int D, const uint64_t *n, const uint64_t *mos, float W, const
     return guarded([&]() -> int {
 #define C_(d) cg_sense<d>(n, mos, W, traj, M, F, csm, C, dcw, data, x_out, iterations, tc_tolerance, \
                           iterates, iterations_run)
+        GBREF_DISPATCH(D, C_)
+#undef C_
+    });
+}
+
+int gbref_time_cg_sense(int D, const uint64_t *n, const uint64_t *mos, float W, const float *traj, uint64_t M,
+                        uint64_t F, const void *csm, uint64_t C, const float *dcw, const void *data, int iterations,
+                        int reps, float *ms) {
+    return guarded([&]() -> int {
+#define C_(d) time_cg_sense<d>(n, mos, W, traj, M, F, csm, C, dcw, data, iterations, reps, ms)
+        GBREF_DISPATCH(D, C_)
+#undef C_
+    });
+}
+
+int gbref_time_nfft(int D, const uint64_t *n, const uint64_t *mos, float W, const float *traj, uint64_t M,
+                    uint64_t F, const void *img, const float *dcw, uint64_t B, int reps, float *ms_fwd,
+                    float *ms_adj, float *ms_prep) {
+    return guarded([&]() -> int {
+#define C_(d) time_nfft<d>(n, mos, W, traj, M, F, img, dcw, B, reps, ms_fwd, ms_adj, ms_prep)
         GBREF_DISPATCH(D, C_)
 #undef C_
     });

@@ -21,9 +21,13 @@ def radial_case(N=64, alpha=2.0, W=5.5, spokes=32, samples=128, frames=1, seed=0
                 M=spokes * samples, batches=batches)
 
 
-def kooshball_case(N=32, alpha=1.5, W=4.0, spokes=200, samples=64, seed=0, batches=1):
+def kooshball_case(N=64, alpha=1.5, W=4.0, spokes=200, samples=64, seed=0, batches=1):
     mos = int(round(N * alpha))
-    mos = ((mos + 31) // 32) * 32
+    if mos % 32 or N % 32:
+        # the plan (like the reference, cuGriddingConvolution.cu:71-80) takes
+        # only multiples of 32: pick N so that N * alpha is one
+        raise ValueError("N = %d, alpha = %g gives an oversampled size %d that is not a multiple of 32"
+                         % (N, alpha, mos))
     traj = S.kooshball_golden_means_3d(spokes, samples)
     dcw = S.ramp_dcw(traj)
     img = S.gaussian_image((batches, 1, N, N, N), seed)

@@ -144,7 +144,7 @@ def test_uneven_frames_match_per_frame(cuda):
 
 
 def test_3d_forward_adjoint(cuda):
-    case = kooshball_case(N=32, spokes=300, samples=64, batches=3, seed=12)
+    case = kooshball_case(N=64, spokes=300, samples=64, batches=3, seed=12)
     plan, orc, _ = _plan_and_oracle(case)
     x = torch.from_numpy(case["img"]).to(cuda)
     dcw = torch.from_numpy(case["dcw"]).to(cuda)

@@ -47,7 +47,15 @@ def _plan(N, mos, W, traj, frames=1, flags=0, dev="cuda:0"):
     return plan
 
 
-def _fwd_adj_case(N, mos, W, traj, frames, batches, dcw, seed, flags=0, oracle_check=True):
+def _fwd_adj_case(N, mos, W, traj, frames, batches, dcw, seed, flags=0, oracle_check=True, pin_tol=PARITY_TOL):
+    """Forward C2NC and adjoint NC2C of the product against the reference.
+
+    In 1D/2D both directions must agree with the reference.  In 3D the forward
+    must agree; the reference's adjoint folds the padding ring differently
+    near z faces (wrap_image_kernel's dimension test,
+    ConvolverNC2C_standard.cuh:411-413), so there the oracle restating that
+    fold must reproduce the reference, and the product must reproduce the
+    periodic-fold oracle.  The 3D adjoint always gets the oracle checks."""
     dev = torch.device("cuda:0")
     D = len(N)
     img = S.gaussian_image((batches, frames) + tuple(reversed(N)), seed)
@@ -63,14 +71,45 @@ def _fwd_adj_case(N, mos, W, traj, frames, batches, dcw, seed, flags=0, oracle_c
     x = torch.empty((batches, frames) + tuple(reversed(N)), dtype=torch.complex64, device=dev)
     plan.compute(_t(y_ref, dev), x, _t(dcw, dev), gb.NFFT_comp_mode.BACKWARDS_NC2C)
     x_ref = R.nfft_compute(N, mos, W, traj, frames, y_ref, dcw, "BACKWARDS_NC2C", batches)
-    e_adj = rel_l2(x.cpu().numpy(), x_ref)
-    assert e_adj <= PARITY_TOL, e_adj
-    if oracle_check:
+    xg = x.cpu().numpy()
+    dcw_f = dcw.reshape(frames, -1)
+    if D < 3:
+        e_adj = rel_l2(xg, x_ref)
+        assert e_adj <= PARITY_TOL, e_adj
+    if oracle_check or D == 3:
         orc = O.OraclePlan(N, mos, W)
         orc.preprocess(traj.reshape(frames, -1, D))
-        assert rel_l2(orc.forward_c2nc(img), y_ref) <= PARITY_TOL
-        assert rel_l2(orc.backwards_nc2c(y_ref, dcw.reshape(frames, -1)), x_ref) <= PARITY_TOL
-    return img, yg, y_ref, x.cpu().numpy(), x_ref
+        if oracle_check:
+            assert rel_l2(orc.forward_c2nc(img), y_ref) <= PARITY_TOL
+        x_orc = orc.backwards_nc2c(y_ref, dcw_f)
+        if D == 3:
+            assert rel_l2(xg, x_orc) <= PARITY_TOL
+            orc_ref = O.OraclePlan(N, mos, W, reference_fold=True)
+            orc_ref.preprocess(traj.reshape(frames, -1, D))
+            x_orc_ref = orc_ref.backwards_nc2c(y_ref, dcw_f)
+            e_pin = rel_l2(x_orc_ref, x_ref)
+            print("3D adjoint: oracle(reference fold) vs reference %.2e, product vs reference %.2e"
+                  % (e_pin, rel_l2(xg, x_ref)))
+            assert e_pin <= pin_tol, e_pin
+        else:
+            assert rel_l2(x_orc, x_ref) <= PARITY_TOL
+    return img, yg, y_ref, xg, x_ref
+
+
+def _adjoint_vs_ndft(N, mos, W, traj, dcw, sub, seed):
+    """Relative L2 error of the product's and the reference's adjoint NUFFT
+    against the FP64 direct adjoint NDFT, on data nonzero at the samples sub."""
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(seed)
+    n_sub = len(sub)
+    y = np.zeros((1, traj.shape[0]), np.complex64)
+    y[0, sub] = (rng.standard_normal(n_sub) + 1j * rng.standard_normal(n_sub)).astype(np.complex64)
+    plan = _plan(N, mos, W, traj)
+    x = torch.empty((1, 1) + tuple(reversed(N)), dtype=torch.complex64, device=dev)
+    plan.compute(_t(y, dev), x, _t(dcw, dev), gb.NFFT_comp_mode.BACKWARDS_NC2C)
+    x_ref = R.nfft_compute(N, mos, W, traj, 1, y, dcw, "BACKWARDS_NC2C", 1)
+    x_ndft = O.ndft_adjoint(y[:, sub], traj[sub], N, mos, dcw[sub])
+    return rel_l2(x.cpu().numpy(), x_ndft), rel_l2(x_ref, x_ndft)
 
 
 def test_ref_2d_radial_128_full_size_fwd_adj_and_ndft():
@@ -104,15 +143,26 @@ def test_ref_mult_MH_M_and_frames_batches():
 
 
 def test_ref_3d_kooshball_alpha_1_5_w4():
-    """3D golden-means kooshball, alpha 1.5 (64 -> 96), W 4, two coils."""
+    """3D golden-means kooshball, alpha 1.5 (64 -> 96), W 4, two coils; the
+    adjoint of both against the FP64 direct NDFT adjoint, where the periodic
+    fold of the product must be the closer one."""
     N, mos, W = (64, 64, 64), (96, 96, 96), 4.0
     traj = S.kooshball_golden_means_3d(1500, 96)
     dcw = S.ramp_dcw(traj)
-    _fwd_adj_case(N, mos, W, traj, 1, 2, dcw, seed=5, oracle_check=False)
-    # oracle pinned on a smaller 3D case of the same alpha and W (32 -> 48 is
-    # not a multiple of 32, which the reference requires; 64 -> 96 is)
-    traj_s = S.kooshball_golden_means_3d(300, 64)
-    _fwd_adj_case(N, mos, W, traj_s, 1, 1, S.ramp_dcw(traj_s), seed=6, oracle_check=True)
+    _fwd_adj_case(N, mos, W, traj, 1, 2, dcw, seed=5, oracle_check=True)
+    # Samples whose taps reach the padding ring across a z face (|k_z| within
+    # half a kernel width of 1/2) are where the two folds differ; elsewhere
+    # both carry the same kernel approximation error (about 3e-3 at alpha
+    # 1.5, W 4).
+    edge = np.nonzero(np.abs(traj[:, 2].astype(np.float64)) * mos[2] > mos[2] / 2 - W / 2)[0]
+    rng = np.random.default_rng(6)
+    inner = rng.choice(np.setdiff1d(np.arange(traj.shape[0]), edge), 1024, replace=False)
+    e_prod, e_ref = _adjoint_vs_ndft(N, mos, W, traj, dcw, edge[:1024], seed=6)
+    print("3D adjoint vs FP64 NDFT, z-face samples: product %.3e reference %.3e" % (e_prod, e_ref))
+    assert e_prod <= 1e-2 and e_ref > 3 * e_prod
+    e_prod_i, e_ref_i = _adjoint_vs_ndft(N, mos, W, traj, dcw, inner, seed=7)
+    print("3D adjoint vs FP64 NDFT, other samples: product %.3e reference %.3e" % (e_prod_i, e_ref_i))
+    assert e_prod_i <= 1e-2 and abs(e_prod_i - e_ref_i) <= 1e-5
 
 
 def test_ref_3d_kooshball_full_sample_count():
@@ -121,7 +171,11 @@ def test_ref_3d_kooshball_full_sample_count():
     N, mos, W = (128, 128, 128), (192, 192, 192), 4.0
     traj = S.kooshball_golden_means_3d(20000, 256)
     dcw = S.ramp_dcw(traj)
-    _fwd_adj_case(N, mos, W, traj, 1, 1, dcw, seed=7, oracle_check=False)
+    # The reference sums each cell's contributions in FP32 in bucket order; at
+    # the centre of 20000 spokes that is tens of thousands of terms, and its
+    # adjoint drifts about 2e-5 from the FP64-summed oracle (1.6e-6 at the
+    # 64^3 size above).  The product stays within 1e-5 of the oracle.
+    _fwd_adj_case(N, mos, W, traj, 1, 1, dcw, seed=7, oracle_check=False, pin_tol=5e-5)
 
 
 @pytest.mark.parametrize("compensated", [False, True])

@@ -253,3 +253,31 @@ def test_cg_image_regularization_and_preconditioner(cuda, frames, use_graph):
     if use_graph:
         assert torch.equal(x, cg.solve(d_t))
     assert E.get_plan().device_errors() == 0
+
+
+def test_grid_barrier_timeout_flags_error_and_next_solve_recovers(cuda):
+    """The fused CG iteration's grid barrier is a bounded wait.  With its limit
+    set to one poll, blocks give up instead of waiting: the solve returns, the
+    device error word reports bit 1, and nothing hangs.  Solves after it at
+    the default limit (plain and graph-captured) start from cleared barrier
+    counters and match the oracle again."""
+    case = sense_case(coils=4, seed=31)
+    E, orc = make_ops(case, cuda)
+    d = orc.mult_M(case["phantom"]).astype(np.complex64)
+    dt = torch.from_numpy(d.reshape(4, -1)).to(cuda)
+    cg = gb.cuCgSolver()
+    cg.set_encoding_operator(E)
+    cg.set_max_iterations(6)
+    cg.set_tc_tolerance(0.0)
+    assert E.get_plan().device_errors() == 0
+    cg.set_barrier_spin_limit(1)
+    cg.solve(dt)
+    torch.cuda.synchronize()
+    assert E.get_plan().device_errors() & 2
+    cg.set_barrier_spin_limit(0)
+    xr = O.cg_solve(orc, d, iterations=6, tc_tolerance=0.0)
+    for use_graph in (False, True):
+        cg.set_use_graph(use_graph)
+        x = cg.solve(dt)
+        assert rel_l2(x.cpu().numpy(), xr) <= 1e-4
+    assert E.get_plan().device_errors() == 0
