@@ -92,6 +92,13 @@ struct DevBuf {
     T *get() const { return ptr; }
 };
 
+// Preprocess sorting (gb_sort.cu): stable radix sort of (key, value) pairs by
+// the low end_bit bits of the key, and an exclusive scan of n counts; both
+// take their scratch from tmp (grown as needed).
+void sort_pairs(const uint32_t *keys_in, uint32_t *keys_out, const uint32_t *vals_in, uint32_t *vals_out, int64_t n,
+                int end_bit, DevBuf<unsigned char> &tmp, cudaStream_t st);
+void exclusive_scan(const uint32_t *in, uint32_t *out, int64_t n, DevBuf<unsigned char> &tmp, cudaStream_t st);
+
 // Scratch of a setup routine kept per device between calls (grown to the
 // largest call, never shrunk): a struct S with a std::mutex `mu`, which a
 // call holds until its stream is done with the scratch.  The cache is never
@@ -230,7 +237,7 @@ struct NufftPlan {
     // preprocessing scratch, kept between calls (no allocation when sizes repeat)
     DevBuf<float> pp_pos;
     DevBuf<uint32_t> pp_key, pp_idx, pp_key_sorted, pp_counts, pp_pcnt, pp_poff, pp_pkey, pp_pval, pp_pkey_sorted;
-    DevBuf<unsigned char> pp_cub;
+    DevBuf<unsigned char> pp_sort;   // sort and scan scratch
     DevBuf<int64_t> pp_off;
     DevBuf<int> pp_err;
     gb_prep_mode prep_mode = GB_PREP_ALL;

@@ -16,7 +16,6 @@
 // cuGriddingConvolution.cu:361-422) samples are binned by tile: one key per
 // sample for its home tile, plus one (tile, sample) pair per tile touched
 // (at most 2^D per sample) for the gridding lists.
-#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -335,24 +334,6 @@ __global__ void k_pair_rows(KParams k, int64_t M, int64_t npairs, const float *_
     if (d == 0 && k.D == 2) reinterpret_cast<uint32_t *>(row + row_weights)[2] = 0u;
 }
 
-template <class T>
-static void exclusive_scan(const T *in, T *out, int64_t n, DevBuf<unsigned char> &tmp, cudaStream_t st) {
-    size_t bytes = 0;
-    GB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, st));
-    tmp.ensure(bytes);
-    GB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, st));
-}
-
-static void sort_pairs(uint32_t *keys_in, uint32_t *keys_out, uint32_t *vals_in, uint32_t *vals_out, int64_t n,
-                       int end_bit, DevBuf<unsigned char> &tmp, cudaStream_t st) {
-    size_t bytes = 0;
-    GB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys_in, keys_out, vals_in, vals_out, (int)n, 0,
-                                            end_bit, st));
-    tmp.ensure(bytes);
-    GB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, keys_in, keys_out, vals_in, vals_out, (int)n, 0,
-                                            end_bit, st));
-}
-
 static int bits_for(uint64_t n) {
     int b = 1;
     while ((1ull << b) < n) b++;
@@ -411,7 +392,7 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
 
     // Stable sort of samples by home key (frame, tile).
     p.perm.ensure(M);
-    sort_pairs(key.get(), key_sorted.get(), idx.get(), p.perm.get(), M, bits_for(nkeys), p.pp_cub, st);
+    sort_pairs(key.get(), key_sorted.get(), idx.get(), p.perm.get(), M, bits_for(nkeys), p.pp_sort, st);
     p.pos_sorted.ensure((size_t)D * M);
     k_gather_pos<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(D, M, pos.get(), p.perm.get(),
                                                                 p.pos_sorted.get()); ::gb::note_launch();
@@ -434,7 +415,7 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     GB_CUDA(cudaMemsetAsync(pcnt.get() + M, 0, sizeof(uint32_t), st));
     k_count_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(), pcnt.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
-    exclusive_scan(pcnt.get(), poff.get(), M + 1, p.pp_cub, st);
+    exclusive_scan(pcnt.get(), poff.get(), M + 1, p.pp_sort, st);
     uint32_t npairs = 0;
     int h_err = 0;
     GB_CUDA(cudaMemcpyAsync(&npairs, poff.get() + M, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -450,7 +431,7 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     k_write_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(), key_sorted.get(),
                                                                  poff.get(), pkey.get(), pval.get()); ::gb::note_launch();
     GB_CUDA(cudaGetLastError());
-    sort_pairs(pkey.get(), pkey_sorted.get(), pval.get(), p.grid_list.get(), npairs, bits_for(nkeys), p.pp_cub, st);
+    sort_pairs(pkey.get(), pkey_sorted.get(), pval.get(), p.grid_list.get(), npairs, bits_for(nkeys), p.pp_sort, st);
     p.grid_off.ensure(nkeys + 1);
     k_sorted_offsets<<<(unsigned)(((int64_t)npairs + TB) / TB), TB, 0, st>>>(pkey_sorted.get(), npairs,
                                                                             (uint32_t)nkeys, p.grid_off.get()); ::gb::note_launch();
