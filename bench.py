@@ -254,14 +254,25 @@ def run_ours(args, rank, world, local_rank):
     cg2.set_tc_tolerance(0.0)
     cg2.set_use_graph(True)
 
+    # The trajectory goes first on the solve's stream; the data, weights and
+    # coil maps (21 MB) cross on a second stream while the trajectory is
+    # preprocessed (preprocess reads only the trajectory), and the solve
+    # waits for them.
+    side = torch.cuda.Stream(device=dev)
+    copied = torch.cuda.Event()
+
     def e2e_step():
-        g_d.copy_(h_d, non_blocking=True)
         g_traj.copy_(h_traj, non_blocking=True)
-        g_sq.copy_(h_sq, non_blocking=True)
-        g_csm.copy_(h_csm, non_blocking=True)
+        side.wait_stream(stream)
+        with torch.cuda.stream(side):
+            g_d.copy_(h_d, non_blocking=True)
+            g_sq.copy_(h_sq, non_blocking=True)
+            g_csm.copy_(h_csm, non_blocking=True)
+            copied.record(side)
         E2.set_csm(g_csm)
         E2.set_dcw(g_sq)
         E2.preprocess(g_traj)
+        stream.wait_event(copied)
         cg2.set_encoding_operator(E2)
         cg2.solve(g_d, x_out)
         h_x.copy_(x_out, non_blocking=True)
@@ -353,7 +364,8 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas%d" % world},
         "e2e": {"value": round(e2e_ms / args.steps / world, 4), "unit": UNIT,
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "includes": "H2D (pinned) of data/trajectory/dcw/csm, preprocess, CG solve, D2H image"},
+                "includes": "H2D (pinned) of data/trajectory/dcw/csm (data, dcw and csm on a second stream, "
+                            "overlapping the preprocess), preprocess, CG solve, D2H image"},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": hbm_peak,
                      "unit": "GB/s", "frac": round(achieved / hbm_peak, 4), "peak_source": peak_src,
                      "traffic": traffic_for(kname), "algorithmic_bytes": int(kbytes), "ms_per_launch": round(kms, 5),

@@ -54,6 +54,7 @@ struct ConvArgs {
     int F;
     int nb;
     int layout;               // SampleLayout
+    int il_stride;            // SORTED_IL: float2 per sample row (nb rounded up to even)
     const float *dcw;         // original order, may be null
     int dcw_pow;
     int sign_fold;
@@ -476,11 +477,13 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
         qz[c] = q / (nrx * nry);
     }
 
-    float acc[RPW][RW][4];
+    // acc[c][j][h]: (re, im) of coil 2 cp + h at cell j of region c, updated
+    // with packed FP32x2 multiply-adds (each component rounds as fmaf).
+    float2 acc[RPW][RW][2];
 #pragma unroll
     for (int c = 0; c < RPW; c++)
 #pragma unroll
-        for (int j = 0; j < RW; j++) acc[c][j][0] = acc[c][j][1] = acc[c][j][2] = acc[c][j][3] = 0.f;
+        for (int j = 0; j < RW; j++) acc[c][j][0] = acc[c][j][1] = make_float2(0.f, 0.f);
 
     // A tile no sample touches: its cells are zero (nothing to add when
     // accumulating) -- one pass of coalesced stores, no staging.
@@ -534,7 +537,7 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
             pd[q] = 1.f;
             if (e < kChunkR * CG && i < cnt && b0 + c < a.nb) {
                 const uint32_t si = a.list[base + i];
-                const bool need_j = a.layout != LAYOUT_SORTED || a.dcw;
+                const bool need_j = a.layout == LAYOUT_ORIGINAL || a.dcw;
                 const uint32_t j = need_j ? a.perm[si] : si;
                 const int64_t idx = (a.layout == LAYOUT_SORTED) ? (int64_t)si : (int64_t)j;
                 pv[q] = samples[(int64_t)(b0 + c) * a.Mtot + idx];
@@ -596,20 +599,23 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
                     const int i = half * 32 + __ffs(bits) - 1;
                     bits &= bits - 1;
                     const float4 v = sv4[i * (SVS / 2) + cp];
+                    const float2 v0 = make_float2(v.x, v.y), v1 = make_float2(v.z, v.w);
                     const float *wr = wt + i * PRF;
                     float wyz = wr[T0 + ry];
                     if (D3) wyz *= wr[T0 + T1 + qz[c]];
+                    const float2 wyz2 = make_float2(wyz, wyz);
 #pragma unroll
                     for (int jj = 0; jj < RW / 4; jj++) {
                         const float4 w4 = *reinterpret_cast<const float4 *>(wr + qx0[c] + 4 * jj);
-                        const float wj[4] = {w4.x * wyz, w4.y * wyz, w4.z * wyz, w4.w * wyz};
+                        const float2 w01 = __fmul2_rn(make_float2(w4.x, w4.y), wyz2);
+                        const float2 w23 = __fmul2_rn(make_float2(w4.z, w4.w), wyz2);
+                        const float wj[4] = {w01.x, w01.y, w23.x, w23.y};
 #pragma unroll
                         for (int m = 0; m < 4; m++) {
-                            float *ac = acc[c][4 * jj + m];
-                            ac[0] = fmaf(wj[m], v.x, ac[0]);
-                            ac[1] = fmaf(wj[m], v.y, ac[1]);
-                            ac[2] = fmaf(wj[m], v.z, ac[2]);
-                            ac[3] = fmaf(wj[m], v.w, ac[3]);
+                            const float2 wm = make_float2(wj[m], wj[m]);
+                            float2 *ac = acc[c][4 * jj + m];
+                            ac[0] = __ffma2_rn(wm, v0, ac[0]);
+                            ac[1] = __ffma2_rn(wm, v1, ac[1]);
                         }
                     }
                 }
@@ -651,7 +657,7 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
             for (int c = 0; c < RPW; c++)
 #pragma unroll
                 for (int j = 0; j < RW; j++)
-                    store(c, j, make_float4(acc[c][j][0], acc[c][j][1], acc[c][j][2], acc[c][j][3]));
+                    store(c, j, make_float4(acc[c][j][0].x, acc[c][j][0].y, acc[c][j][1].x, acc[c][j][1].y));
             return;
         }
         float2 *tl = reinterpret_cast<float2 *>(g_rows_smem);
@@ -660,8 +666,8 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
 #pragma unroll
             for (int j = 0; j < RW; j++) {
                 const int o = qz[c] * ZS + (qy0[c] + row) * RS + qx0[c] + j;
-                tl[(2 * cp) * PS + o] = make_float2(acc[c][j][0], acc[c][j][1]);
-                tl[(2 * cp + 1) * PS + o] = make_float2(acc[c][j][2], acc[c][j][3]);
+                tl[(2 * cp) * PS + o] = acc[c][j][0];
+                tl[(2 * cp + 1) * PS + o] = acc[c][j][1];
             }
         __syncthreads();
         const int x = threadIdx.x % T0, r0 = threadIdx.x / T0, rpp = kThreads / T0;
@@ -703,7 +709,7 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
 #pragma unroll
             for (int j = 0; j < RW; j++)
                 pp[(c * RW + j) * kThreads + threadIdx.x] =
-                    make_float4(acc[c][j][0], acc[c][j][1], acc[c][j][2], acc[c][j][3]);
+                    make_float4(acc[c][j][0].x, acc[c][j][0].y, acc[c][j][1].x, acc[c][j][1].y);
     }
     __threadfence();
     __syncthreads();
@@ -728,11 +734,306 @@ k_grid_rows(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__
                 s.z += v.z;
                 s.w += v.w;
             }
-            acc[c][j][0] = s.x;
-            acc[c][j][1] = s.y;
-            acc[c][j][2] = s.z;
-            acc[c][j][3] = s.w;
+            acc[c][j][0] = make_float2(s.x, s.y);
+            acc[c][j][1] = make_float2(s.z, s.w);
         }
+    epilogue();
+}
+
+// ------------------------------------- NC2C, row variant, warp-specialized --
+//
+// The row variant for SORTED_IL samples (the E^H E workspace, where every
+// sample's coils are one contiguous row).  Nothing is staged through
+// registers: a producer warp (warp 8) streams each chunk's pair rows and
+// sample rows into a ring of kWsStages shared-memory stages with bulk copies
+// (cp.async.bulk), announcing the bytes on the stage's "full" mbarrier; the
+// eight consumer warps run the same region visits as k_grid_rows and release
+// a stage on its "empty" mbarrier (one arrival per warp) when done with it.
+// Warps never wait for each other inside the chunk loop, and the copies of
+// the next kWsStages - 1 chunks are in flight while a chunk is summed.  All
+// waits are bounded (err bit 0).  Same per-cell summation order as
+// k_grid_rows, so the result is bit-identical.
+
+constexpr int kWsStages = 4;
+constexpr int kWsThreads = kThreads + 32;   // 8 consumer warps + 1 producer warp
+constexpr int kWsMinBlocks = 2;             // resident CTAs per SM (96 registers a thread)
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+
+__host__ __device__ __forceinline__ int ws_stage_bytes(const KParams &k, int cg) {
+    return kChunkR * (pair_row_floats(k) * 4 + cg * 8);
+}
+
+template <int CG, int RW, int RPW, bool D3>
+__global__ void __launch_bounds__(kWsThreads, kWsMinBlocks)
+k_grid_rows_ws(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__ grid) {
+    constexpr int CP = CG / 2;      // lanes per row: one per coil pair
+    constexpr int ROWS = 32 / CP;   // rows per region
+    extern __shared__ __align__(128) unsigned char g_ws_smem[];
+    __shared__ int s_last;
+    __shared__ __align__(8) unsigned long long s_full[kWsStages], s_empty[kWsStages];
+
+    const KParams &k = a.k;
+    const int grp = blockIdx.y;
+    const int b0 = grp * CG;
+    const WorkItem it = a.items[blockIdx.x];
+    const int f = it.ft / k.ntiles_total;
+    const int tile = it.ft - f * k.ntiles_total;
+    const int tx = tile % k.ntiles[0];
+    const int ty = (tile / k.ntiles[0]) % k.ntiles[1];
+    const int tz = tile / (k.ntiles[0] * k.ntiles[1]);
+    const int org0 = tx * k.tile[0], org1 = ty * k.tile[1], org2 = tz * k.tile[2];
+    const int T0 = k.tile[0], T1 = k.tile[1];
+    const int PRF = a.prow_floats;   // floats per pair row
+    const int PRW = PRF - 4;         // weight part; the last 4 words are the footprint ranges
+    const int stage_bytes = ws_stage_bytes(k, CG);
+    auto stage_wt = [&](int s) { return reinterpret_cast<float *>(g_ws_smem + s * stage_bytes); };
+    auto stage_v = [&](int s) {
+        return reinterpret_cast<float2 *>(g_ws_smem + s * stage_bytes + kChunkR * PRF * 4);
+    };
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool consumer = warp < 8;
+
+    // A tile no sample touches: zero stores, no staging.
+    if (it.begin == it.end && it.split < 0) {
+        if (a.accumulate) return;
+        const int cells = T0 * T1 * k.tile[2];
+        const int64_t ostep = (int64_t)a.F * a.kl.s_bf;
+        float2 *gbase = grid + ((int64_t)b0 * a.F + f) * a.kl.s_bf;
+        for (int e = threadIdx.x; e < cells; e += blockDim.x) {
+            const int x = e % T0, yz = e / T0, y = yz % T1, z = yz / T1;
+            float2 *o = gbase + (int64_t)(org2 + z) * a.kl.s_z + (int64_t)(org1 + y) * a.kl.s_y + org0 + x;
+            for (int c = 0; c < CG && b0 + c < a.nb; c++) {
+                *o = make_float2(0.f, 0.f);
+                o += ostep;
+            }
+        }
+        return;
+    }
+
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < kWsStages; st++) {
+            mbar_init(smem_u32(&s_full[st]), 1);
+            mbar_init(smem_u32(&s_empty[st]), 8);
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const int nchunks = (it.end - it.begin + kChunkR - 1) / kChunkR;
+
+    const int cp = lane % CP, row = lane / CP;
+    const int nrx = T0 / RW, nry = T1 / ROWS;
+    int qx0[RPW], qy0[RPW], qz[RPW];
+#pragma unroll
+    for (int c = 0; c < RPW; c++) {
+        const int q = (consumer ? warp : 0) + 8 * c;
+        qx0[c] = (q % nrx) * RW;
+        qy0[c] = ((q / nrx) % nry) * ROWS;
+        qz[c] = q / (nrx * nry);
+    }
+    float2 acc[RPW][RW][2];
+#pragma unroll
+    for (int c = 0; c < RPW; c++)
+#pragma unroll
+        for (int j = 0; j < RW; j++) acc[c][j][0] = acc[c][j][1] = make_float2(0.f, 0.f);
+
+    if (!consumer) {
+        // Producer: for chunk ch, stage ch % kWsStages once the consumers
+        // released its previous use; lane 0 announces all bytes (arrival +
+        // transaction count) and copies the pair rows, then every lane copies
+        // up to two sample rows (this coil group's columns).
+        const uint32_t vbytes = (uint32_t)min(CG, a.il_stride - b0) * 8u;
+        for (int ch = 0; ch < nchunks; ch++) {
+            const int st = ch % kWsStages;
+            const int use = ch / kWsStages;
+            const int base = it.begin + ch * kChunkR;
+            const int cnt = min(kChunkR, it.end - base);
+            const uint32_t si0 = lane < cnt ? a.list[base + lane] : 0u;
+            const uint32_t si1 = lane + 32 < cnt ? a.list[base + lane + 32] : 0u;
+            if (use > 0) mbar_wait_bounded(smem_u32(&s_empty[st]), (uint32_t)(use - 1) & 1u, a.err);
+            fence_proxy_async_smem();
+            const uint32_t full = smem_u32(&s_full[st]);
+            if (lane == 0) {
+                const uint32_t rbytes = (uint32_t)cnt * (uint32_t)PRF * 4u;
+                mbar_expect_tx(full, rbytes + (uint32_t)cnt * vbytes);
+                bulk_copy_g2s(smem_u32(stage_wt(st)), a.prows + (int64_t)base * PRF, rbytes, full);
+            }
+            __syncwarp();
+            float2 *sv = stage_v(st);
+            if (lane < cnt)
+                bulk_copy_g2s(smem_u32(sv + lane * CG), samples + (int64_t)si0 * a.il_stride + b0, vbytes, full);
+            if (lane + 32 < cnt)
+                bulk_copy_g2s(smem_u32(sv + (lane + 32) * CG), samples + (int64_t)si1 * a.il_stride + b0, vbytes,
+                              full);
+        }
+    } else {
+        for (int ch = 0; ch < nchunks; ch++) {
+            const int st = ch % kWsStages;
+            const int base = it.begin + ch * kChunkR;
+            const int cnt = min(kChunkR, it.end - base);
+            mbar_wait_bounded(smem_u32(&s_full[st]), (uint32_t)(ch / kWsStages) & 1u, a.err);
+            const float *wt = stage_wt(st);
+            const float4 *sv4 = reinterpret_cast<const float4 *>(stage_v(st));
+#pragma unroll
+            for (int c = 0; c < RPW; c++) {
+                const int ry = qy0[c] + row;
+#pragma unroll
+                for (int half = 0; half < kChunkR / 32; half++) {
+                    const int il = half * 32 + lane;
+                    bool hit = false;
+                    if (il < cnt) {
+                        const uint4 r = *reinterpret_cast<const uint4 *>(wt + il * PRF + PRW);
+                        hit = (int)(r.x & 0xffffu) <= qx0[c] + RW - 1 && (int)(r.x >> 16) >= qx0[c] &&
+                              (int)(r.y & 0xffffu) <= qy0[c] + ROWS - 1 && (int)(r.y >> 16) >= qy0[c];
+                        if (D3) hit = hit && (int)(r.z & 0xffffu) <= qz[c] && (int)(r.z >> 16) >= qz[c];
+                    }
+                    uint32_t bits = __ballot_sync(0xffffffffu, hit);
+                    while (bits) {
+                        const int i = half * 32 + __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        const float4 v = sv4[i * (CG / 2) + cp];
+                        const float2 v0 = make_float2(v.x, v.y), v1 = make_float2(v.z, v.w);
+                        const float *wr = wt + i * PRF;
+                        float wyz = wr[T0 + ry];
+                        if (D3) wyz *= wr[T0 + T1 + qz[c]];
+                        const float2 wyz2 = make_float2(wyz, wyz);
+#pragma unroll
+                        for (int jj = 0; jj < RW / 4; jj++) {
+                            const float4 w4 = *reinterpret_cast<const float4 *>(wr + qx0[c] + 4 * jj);
+                            const float2 w01 = __fmul2_rn(make_float2(w4.x, w4.y), wyz2);
+                            const float2 w23 = __fmul2_rn(make_float2(w4.z, w4.w), wyz2);
+                            const float wj[4] = {w01.x, w01.y, w23.x, w23.y};
+#pragma unroll
+                            for (int m = 0; m < 4; m++) {
+                                const float2 wm = make_float2(wj[m], wj[m]);
+                                float2 *ac = acc[c][4 * jj + m];
+                                ac[0] = __ffma2_rn(wm, v0, ac[0]);
+                                ac[1] = __ffma2_rn(wm, v1, ac[1]);
+                            }
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&s_empty[st]));
+        }
+    }
+    __syncthreads();   // every stage consumed; every copy landed
+
+    auto store = [&](int c, int j, float4 v) {
+        const int gx = org0 + qx0[c] + j, gy = org1 + qy0[c] + row, gz = org2 + qz[c];
+        const int64_t g = (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y + gx;
+        const float sgn = (a.sign_fold && ((gx + gy + gz) & 1)) ? -1.f : 1.f;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int q = 2 * cp + h;
+            if (b0 + q >= a.nb) break;
+            float2 *o = grid + ((int64_t)(b0 + q) * a.F + f) * a.kl.s_bf + g;
+            float2 w = h ? make_float2(sgn * v.z, sgn * v.w) : make_float2(sgn * v.x, sgn * v.y);
+            if (a.accumulate) { const float2 old = *o; w.x += old.x; w.y += old.y; }
+            *o = w;
+        }
+    };
+    // Tile out through shared memory (as k_grid_rows), the stage ring as the
+    // staging area.  Every thread calls it (it has a barrier).
+    auto epilogue = [&]() {
+        const int T2 = k.tile[2];
+        const int RS = T0 + 1, ZS = T1 * RS;
+        int PS = T2 * ZS;
+        PS += (10 - PS % 8) % 8;   // PS = 2 (mod 8)
+        if ((int64_t)CG * PS * 8 > (int64_t)kWsStages * stage_bytes) {
+            if (consumer) {
+#pragma unroll
+                for (int c = 0; c < RPW; c++)
+#pragma unroll
+                    for (int j = 0; j < RW; j++)
+                        store(c, j, make_float4(acc[c][j][0].x, acc[c][j][0].y, acc[c][j][1].x, acc[c][j][1].y));
+            }
+            return;
+        }
+        float2 *tl = reinterpret_cast<float2 *>(g_ws_smem);
+        if (consumer) {
+#pragma unroll
+            for (int c = 0; c < RPW; c++)
+#pragma unroll
+                for (int j = 0; j < RW; j++) {
+                    const int o = qz[c] * ZS + (qy0[c] + row) * RS + qx0[c] + j;
+                    tl[(2 * cp) * PS + o] = acc[c][j][0];
+                    tl[(2 * cp + 1) * PS + o] = acc[c][j][1];
+                }
+        }
+        __syncthreads();
+        const int x = threadIdx.x % T0, r0 = threadIdx.x / T0, rpp = kThreads / T0;
+        if (r0 >= rpp) return;
+        const int rows_c = T2 * T1;
+        const int gx = org0 + x;
+        for (int r = r0; r < rows_c; r += rpp) {
+            const int z = r / T1, y = r - z * T1;
+            const int gy = org1 + y, gz = org2 + z;
+            const float sgn = (a.sign_fold && ((gx + gy + gz) & 1)) ? -1.f : 1.f;
+            const int64_t cell = (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y + gx;
+            const float2 *src = tl + z * ZS + y * RS + x;
+            float2 *o = grid + ((int64_t)b0 * a.F + f) * a.kl.s_bf + cell;
+            const int64_t ostep = (int64_t)a.F * a.kl.s_bf;
+            for (int c = 0; c < CG && b0 + c < a.nb; c++) {
+                float2 v = src[c * PS];
+                v.x *= sgn;
+                v.y *= sgn;
+                if (a.accumulate) { const float2 old = *o; v.x += old.x; v.y += old.y; }
+                *o = v;
+                o += ostep;
+            }
+        }
+    };
+    if (it.split < 0) {
+        epilogue();
+        return;
+    }
+    // Split tile: write this chunk's partial tile, the last CTA sums the
+    // partials in chunk order.
+    const SplitInfo si = a.splits[it.split];
+    auto part = [&](int slot) -> float4 * {
+        return reinterpret_cast<float4 *>(a.partials + ((int64_t)slot * a.ncg + grp) * a.part_elems);
+    };
+    if (consumer) {
+        float4 *pp = part(si.first_slot + it.chunk);
+#pragma unroll
+        for (int c = 0; c < RPW; c++)
+#pragma unroll
+            for (int j = 0; j < RW; j++)
+                pp[(c * RW + j) * kThreads + threadIdx.x] =
+                    make_float4(acc[c][j][0].x, acc[c][j][0].y, acc[c][j][1].x, acc[c][j][1].y);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int *ctr = a.counters + (int64_t)it.split * a.ncg + grp;
+        const unsigned int old = atomicAdd(ctr, 1u);
+        s_last = (old == (unsigned int)(si.nchunks - 1));
+        if (s_last) *ctr = 0u;   // ready for the next launch
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (consumer) {
+#pragma unroll
+        for (int c = 0; c < RPW; c++)
+#pragma unroll
+            for (int j = 0; j < RW; j++) {
+                float4 sm = make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int ch = 0; ch < si.nchunks; ch++) {
+                    const float4 v = __ldcg(&part(si.first_slot + ch)[(c * RW + j) * kThreads + threadIdx.x]);
+                    sm.x += v.x;
+                    sm.y += v.y;
+                    sm.z += v.z;
+                    sm.w += v.w;
+                }
+                acc[c][j][0] = make_float2(sm.x, sm.y);
+                acc[c][j][1] = make_float2(sm.z, sm.w);
+            }
+    }
     epilogue();
 }
 
@@ -954,7 +1255,7 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
         }
         const bool valid = i < it.end;
         const uint32_t j = valid ? a.perm[i] : 0u;
-        const int64_t idx = (a.layout == LAYOUT_SORTED) ? (int64_t)i : (int64_t)j;
+        const int64_t idx = (a.layout != LAYOUT_ORIGINAL) ? (int64_t)i : (int64_t)j;
         if (!GRAD) {
             if (valid) {
                 float scale = 1.f;
@@ -977,7 +1278,8 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
                             val.y *= scale;
                         }
                     }
-                    float2 *o = out + (int64_t)coil * a.Mtot + idx;
+                    float2 *o = (a.layout == LAYOUT_SORTED_IL) ? out + idx * a.il_stride + coil
+                                                            : out + (int64_t)coil * a.Mtot + idx;
                     if (a.accumulate) { const float2 ov = *o; val.x += ov.x; val.y += ov.y; }
                     *o = val;
                 }
@@ -1065,7 +1367,7 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
             r.t0[d] = __ldg(trow);
             r.t1[d] = NT > 4 ? __ldg(trow + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        const bool need_j = a.layout != LAYOUT_SORTED || a.dcw;
+        const bool need_j = a.layout == LAYOUT_ORIGINAL || a.dcw;
         r.j = need_j ? a.perm[ic] : (uint32_t)ic;
         r.dw = a.dcw ? a.dcw[r.j] : 1.f;
     };
@@ -1152,9 +1454,10 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
 #pragma unroll
             for (int t = 0; t < NT; t++) w[d][t] = (a.sign_fold && (t & 1)) ? -s0 * tv[t] : s0 * tv[t];
         }
-        float acc[CPL][2];
+        // (re, im) of each of the lane's coils, packed FP32x2 multiply-adds
+        float2 acc[CPL];
 #pragma unroll
-        for (int c = 0; c < CPL; c++) acc[c][0] = acc[c][1] = 0.f;
+        for (int c = 0; c < CPL; c++) acc[c] = make_float2(0.f, 0.f);
         const float2 *base_s = tile_s + (((size_t)rs[2] * R1 + rs[1]) * R0 + rs[0]) * CS + ll * CPL;
         // Tap nest, unrolled to NTT taps per dimension, with no per-tap
         // predicates in x and y: the table weights beyond a footprint are zero
@@ -1178,16 +1481,13 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
                             for (int t = 0; t < NTT; t++) {
                                 {
                                     const float wv = w[0][t] * wyz;
+                                    const float2 wv2 = make_float2(wv, wv);
                                     if (CPL == 2) {
                                         const float4 q = *reinterpret_cast<const float4 *>(row + t * CS);
-                                        acc[0][0] = fmaf(wv, q.x, acc[0][0]);
-                                        acc[0][1] = fmaf(wv, q.y, acc[0][1]);
-                                        acc[CPL - 1][0] = fmaf(wv, q.z, acc[CPL - 1][0]);
-                                        acc[CPL - 1][1] = fmaf(wv, q.w, acc[CPL - 1][1]);
+                                        acc[0] = __ffma2_rn(wv2, make_float2(q.x, q.y), acc[0]);
+                                        acc[CPL - 1] = __ffma2_rn(wv2, make_float2(q.z, q.w), acc[CPL - 1]);
                                     } else {
-                                        const float2 q = row[t * CS];
-                                        acc[0][0] = fmaf(wv, q.x, acc[0][0]);
-                                        acc[0][1] = fmaf(wv, q.y, acc[0][1]);
+                                        acc[0] = __ffma2_rn(wv2, row[t * CS], acc[0]);
                                     }
                                 }
                             }
@@ -1206,13 +1506,13 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
             nest(std::integral_constant<int, NT>{});
         if (valid) {
             const uint32_t j = cur.j;
-            const int64_t idx = (a.layout == LAYOUT_SORTED) ? (int64_t)i : (int64_t)j;
+            const int64_t idx = (a.layout != LAYOUT_ORIGINAL) ? (int64_t)i : (int64_t)j;
             const float dw = cur.dw;
 #pragma unroll
             for (int c = 0; c < CPL; c++) {
                 const int coil = b0 + ll * CPL + c;
                 if (coil >= a.nb) break;
-                float2 val = make_float2(acc[c][0], acc[c][1]);
+                float2 val = acc[c];
                 if (a.dcw) {
                     if (a.dcw_pow == 2) {
                         val.x = (val.x * dw) * dw;
@@ -1222,7 +1522,8 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
                         val.y *= dw;
                     }
                 }
-                float2 *o = out + (int64_t)coil * a.Mtot + idx;
+                float2 *o = (a.layout == LAYOUT_SORTED_IL) ? out + idx * a.il_stride + coil
+                                                            : out + (int64_t)coil * a.Mtot + idx;
                 if (a.accumulate) { const float2 ov = *o; val.x += ov.x; val.y += ov.y; }
                 *o = val;
             }
@@ -1257,6 +1558,7 @@ static ConvArgs make_args(NufftPlan &p, int nb, SampleLayout layout, const float
     a.F = (int)p.F;
     a.nb = nb;
     a.layout = layout;
+    a.il_stride = il_stride_for(nb);
     a.dcw = dcw;
     a.dcw_pow = dcw_pow;
     a.sign_fold = sign_fold ? 1 : 0;
@@ -1340,6 +1642,26 @@ static void grid_rows_launch(const ConvArgs &a, dim3 g, int smem, const float2 *
     kern<<<g, kThreads, smem, st>>>(a, s, o); ::gb::note_launch();
 }
 
+template <int CG, int RW, int RPW, bool D3>
+static void grid_rows_ws_launch(const ConvArgs &a, dim3 g, const float2 *s, float2 *o, cudaStream_t st) {
+    auto kern = k_grid_rows_ws<CG, RW, RPW, D3>;
+    const int smem = kWsStages * ws_stage_bytes(a.k, CG);
+    if (smem > 48 * 1024)
+        GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    kern<<<g, kWsThreads, smem, st>>>(a, s, o); ::gb::note_launch();
+}
+
+template <int CG, bool D3>
+static void grid_rows_ws_shape(const GridCfg &c, const ConvArgs &a, dim3 g, const float2 *s, float2 *o,
+                               cudaStream_t st) {
+    if (c.rw == 4 && c.rpw == 1) grid_rows_ws_launch<CG, 4, 1, D3>(a, g, s, o, st);
+    else if (c.rw == 4 && c.rpw == 2) grid_rows_ws_launch<CG, 4, 2, D3>(a, g, s, o, st);
+    else if (c.rw == 4 && c.rpw == 4) grid_rows_ws_launch<CG, 4, 4, D3>(a, g, s, o, st);
+    else if (c.rw == 8 && c.rpw == 1) grid_rows_ws_launch<CG, 8, 1, D3>(a, g, s, o, st);
+    else if (c.rw == 8 && c.rpw == 2) grid_rows_ws_launch<CG, 8, 2, D3>(a, g, s, o, st);
+    else fail(GB_ERR_INTERNAL, "unsupported gridding region shape");
+}
+
 template <int CG, bool D3>
 static void grid_rows_shape(const GridCfg &c, const ConvArgs &a, dim3 g, const float2 *s, float2 *o,
                             cudaStream_t st) {
@@ -1355,7 +1677,16 @@ static void grid_rows_shape(const GridCfg &c, const ConvArgs &a, dim3 g, const f
 static void grid_dispatch_cfg(const GridCfg &c, const NufftPlan &p, const ConvArgs &a, const float2 *samples,
                               float2 *grid, cudaStream_t st) {
     dim3 g(p.n_grd_items, c.ncg);
-    if (c.rows) {
+    if (c.rows && a.layout == LAYOUT_SORTED_IL) {
+        const bool d3 = p.kp.D == 3;
+        if (c.cg == 16) {
+            if (d3) grid_rows_ws_shape<16, true>(c, a, g, samples, grid, st);
+            else grid_rows_ws_shape<16, false>(c, a, g, samples, grid, st);
+        } else {
+            if (d3) grid_rows_ws_shape<8, true>(c, a, g, samples, grid, st);
+            else grid_rows_ws_shape<8, false>(c, a, g, samples, grid, st);
+        }
+    } else if (c.rows) {
         const bool d3 = p.kp.D == 3;
         if (c.cg == 16) {
             if (d3) grid_rows_shape<16, true>(c, a, g, samples, grid, st);
@@ -1403,6 +1734,8 @@ void launch_grid(NufftPlan &p, const float2 *samples, float2 *grid, int nb, Samp
                  const float *dcw, bool sign_fold, bool accumulate, cudaStream_t st, const KLayout *kl) {
     if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
     const GridCfg c = grid_config(p, nb);
+    if (layout == LAYOUT_SORTED_IL && (!c.rows || dcw))
+        fail(GB_ERR_INTERNAL, "interleaved samples need the row-variant gridding kernel and no density weights");
     ConvArgs a = make_args(p, nb, layout, dcw, 1, sign_fold, accumulate);
     if (kl) a.kl = *kl;
     a.list = p.grid_list.get();
@@ -1418,6 +1751,24 @@ void launch_grid(NufftPlan &p, const float2 *samples, float2 *grid, int nb, Samp
     }
     if (p.n_grd_items == 0) return;
     grid_dispatch_cfg(c, p, a, samples, grid, st);
+}
+
+// The warp-specialized gridding (and so the interleaved workspace) wins when
+// the launch is a few waves deep: its 4-stage copy pipeline hides the
+// staging latency that dominates a short launch (CG-SENSE 256^2 x 16 coils:
+// 1082 CTAs, 1.25 -> 1.19 ms per recon).  On launches many waves deep the
+// register-staged kernel's higher occupancy (3 CTAs of 8 warps per SM against
+// 2 of 8 + 1) wins instead (64 uneven frames x 12 coils: 42.0 against 45.5 ms
+// per batch), so past kWsMaxWaves resident waves E^H E keeps SORTED.
+constexpr int kWsMaxWaves = 8;
+
+SampleLayout normal_op_layout(const NufftPlan &p, int nb) {
+    const GridCfg c = grid_config(p, nb);
+    if (!c.rows) return LAYOUT_SORTED;
+    int sms = 0;
+    GB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device));
+    const int64_t ctas = (int64_t)p.n_grd_items * c.ncg;
+    return ctas <= (int64_t)kWsMaxWaves * kWsMinBlocks * sms ? LAYOUT_SORTED_IL : LAYOUT_SORTED;
 }
 
 // Scratch (split-tile partial tiles and their counters) that launch_grid

@@ -332,7 +332,19 @@ uint64_t plan_layout_signature(const NufftPlan &p, int nbf);
 void plan_autotune(NufftPlan &p, int nb, cudaStream_t st);
 
 // Sample-array layout flags for the convolution kernels.
-enum SampleLayout { LAYOUT_ORIGINAL = 0, LAYOUT_SORTED = 1 };
+//   ORIGINAL   [nb][Mtot], the caller's sample order
+//   SORTED     [nb][Mtot], the plan's sorted (home tile) order
+//   SORTED_IL  [Mtot][il] sorted order with the coils of a sample adjacent
+//              (il = nb rounded up to even, so a sample's coil group is a
+//              16-byte multiple): the plan's own workspace between
+//              degridding and gridding inside E^H E, which the gridding
+//              kernel stages by bulk copies (no gather through registers).
+enum SampleLayout { LAYOUT_ORIGINAL = 0, LAYOUT_SORTED = 1, LAYOUT_SORTED_IL = 2 };
+__host__ __device__ inline int il_stride_for(int nb) { return (nb + 1) & ~1; }
+// The layout that E^H E hands from degridding to gridding for nb batches:
+// SORTED_IL when the gridding runs the row variant (bulk-copied values),
+// else SORTED.
+SampleLayout normal_op_layout(const NufftPlan &p, int nb);
 
 // Degridding: grid [nb][F][G] -> samples.  sign_fold multiplies the weight of
 // grid cell g by (-1)^(sum g) (the centring checkerboard after the FFT).

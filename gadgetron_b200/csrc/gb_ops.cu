@@ -44,7 +44,8 @@ float2 *ensure_kgrid(NufftPlan &p, int64_t nbf) {
 }
 
 float2 *ensure_samp(NufftPlan &p, int nb) {
-    p.samp_ws.ensure((size_t)nb * p.Mtot);
+    // room for either sorted layout ([nb][M] or [M][il])
+    p.samp_ws.ensure((size_t)il_stride_for(nb) * p.Mtot);
     return p.samp_ws.get();
 }
 
@@ -195,8 +196,9 @@ void nufft_adjoint(NufftPlan &p, const float2 *samples, SampleLayout layout, con
 void nufft_normal(NufftPlan &p, const float2 *img, const float2 *csm, int nb, const float *dcw,
                   float2 *out, bool accumulate, float weight, cudaStream_t st) {
     float2 *samp = ensure_samp(p, nb);
-    nufft_forward(p, img, csm, nb, false, samp, LAYOUT_SORTED, dcw, 2, false, st);
-    nufft_adjoint(p, samp, LAYOUT_SORTED, nullptr, csm, nb, out, false, accumulate, weight, CUFFT_INVERSE, st);
+    const SampleLayout lay = normal_op_layout(p, nb);
+    nufft_forward(p, img, csm, nb, false, samp, lay, dcw, 2, false, st);
+    nufft_adjoint(p, samp, lay, nullptr, csm, nb, out, false, accumulate, weight, CUFFT_INVERSE, st);
 }
 
 void nufft_compute(NufftPlan &p, const void *in, void *out, const float *dcw, gb_comp_mode mode,
@@ -867,11 +869,12 @@ static void cg_normal_dot(CgSolver &cg, cudaStream_t st, bool update_p) {
     const int64_t nbf = (int64_t)nb * p.F;
     float2 *samp = ensure_samp(p, nb);
     PUpdate pu{cg.p.get(), cg.r.get(), cg.precond, cg.segs.get(), cg.nseg > 1 ? 1 : 0};
-    nufft_forward(p, cg.p.get(), s.csm, nb, false, samp, LAYOUT_SORTED, s.dcw, 2, false, st,
+    const SampleLayout lay = normal_op_layout(p, nb);
+    nufft_forward(p, cg.p.get(), s.csm, nb, false, samp, lay, s.dcw, 2, false, st,
                   update_p ? &pu : nullptr);
     float2 *kg = ensure_kgrid(p, nbf);
     const KLayout kl = ws_layout(p, nbf);
-    launch_grid(p, samp, kg, nb, LAYOUT_SORTED, nullptr, true, false, st, &kl);
+    launch_grid(p, samp, kg, nb, lay, nullptr, true, false, st, &kl);
     fft_adjoint_ws(p, kg, (int)nbf, CUFFT_INVERSE, true, st);
     k_cg_crop_dot<<<seg_grid(cg), 256, 0, st>>>(p.kp, kl, p.deap_img.get(), p.maxN,
                                                 (float)(1.0 / std::sqrt((double)p.kp.G)), kg, s.csm, nb,
@@ -904,8 +907,9 @@ static void cg_iteration_fused(CgSolver &cg, cudaStream_t st, double *hist, bool
     float2 *kg = ensure_kgrid(p, nbf);
     float2 *samp = ensure_samp(p, nb);
     fft_forward_ws(p, pad, kg, (int)nbf, CUFFT_FORWARD, true, st);
-    launch_degrid(p, kg, samp, nb, LAYOUT_SORTED, s.dcw, 2, true, false, st, &kl);
-    launch_grid(p, samp, kg, nb, LAYOUT_SORTED, nullptr, true, false, st, &kl);
+    const SampleLayout lay = normal_op_layout(p, nb);
+    launch_degrid(p, kg, samp, nb, lay, s.dcw, 2, true, false, st, &kl);
+    launch_grid(p, samp, kg, nb, lay, nullptr, true, false, st, &kl);
     fft_adjoint_ws(p, kg, (int)nbf, CUFFT_INVERSE, true, st);
     TailArgs ta{};
     ta.k = p.kp;

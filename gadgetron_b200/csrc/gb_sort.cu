@@ -9,9 +9,10 @@
 // per-cell summation order a function of the trajectory alone, so results
 // are bit-reproducible.
 //
-// Radix sort: 8-bit digits, ceil(end_bit / 8) passes, each pass three
-// launches over tiles of kSortTile elements (256 threads, 8 warps; a warp
-// owns a contiguous run of kSortTile / 8 elements):
+// Radix sort: ceil(end_bit / 11) passes of equal digits of at most 11 bits
+// (a 10-bit key sorts in one pass), each pass three launches over tiles of
+// kSortTile elements (256 threads, 8 warps; a warp owns a contiguous run of
+// kSortTile / 8 elements):
 //   upsweep    per-tile digit histogram (shared-memory atomics), written
 //              digit-major: hist[digit * ntiles + tile];
 //   scan       exclusive scan of hist (the global position of every
@@ -30,40 +31,48 @@
 
 namespace gb {
 
+void exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *tile_scratch, cudaStream_t st);
+
 namespace {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortPerWarp = 512;                        // 16 rounds of 32
 constexpr int kSortTile = kSortWarps * kSortPerWarp;     // 4096 elements
-constexpr int kRadix = 256;
+constexpr int kMaxRadixBits = 11;
 
 constexpr int kScanThreads = 256;
 constexpr int kScanPerThread = 16;
 constexpr int kScanTile = kScanThreads * kScanPerThread;  // 4096 counts
 
+template <int RB>
 __global__ void __launch_bounds__(kSortThreads) k_radix_upsweep(const uint32_t *__restrict__ keys, int64_t n,
                                                                 int shift, int64_t ntiles,
                                                                 uint32_t *__restrict__ hist) {
-    __shared__ uint32_t h[kRadix];
-    h[threadIdx.x] = 0u;
+    constexpr int R = 1 << RB;
+    __shared__ uint32_t h[R];
+    for (int d = threadIdx.x; d < R; d += kSortThreads) h[d] = 0u;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kSortTile;
     for (int i = threadIdx.x; i < kSortTile; i += kSortThreads) {
         const int64_t e = base + i;
-        if (e < n) atomicAdd(&h[(keys[e] >> shift) & (kRadix - 1)], 1u);
+        if (e < n) atomicAdd(&h[(keys[e] >> shift) & (R - 1)], 1u);
     }
     __syncthreads();
-    hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+    for (int d = threadIdx.x; d < R; d += kSortThreads) hist[(int64_t)d * ntiles + blockIdx.x] = h[d];
 }
 
+// Shared memory: kSortWarps x 2^RB counters (dynamic, up to 64 KB).
+template <int RB>
 __global__ void __launch_bounds__(kSortThreads)
 k_radix_downsweep(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                   uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, int64_t n, int shift,
                   int64_t ntiles, const uint32_t *__restrict__ offs) {
-    __shared__ uint32_t cnt[kSortWarps][kRadix];
+    constexpr int R = 1 << RB;
+    extern __shared__ uint32_t g_sort_cnt[];
+    auto cnt = [&](int w, uint32_t d) -> uint32_t & { return g_sort_cnt[w * R + d]; };
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&cnt[0][0])[i] = 0u;
+    for (int i = threadIdx.x; i < kSortWarps * R; i += kSortThreads) g_sort_cnt[i] = 0u;
     __syncthreads();
     const int64_t wbase = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * kSortPerWarp;
     const uint32_t lt = (1u << lane) - 1u;
@@ -71,18 +80,17 @@ k_radix_downsweep(const uint32_t *__restrict__ keys_in, const uint32_t *__restri
     for (int r = 0; r < kSortPerWarp; r += 32) {
         const int64_t e = wbase + r + lane;
         const bool ok = e < n;
-        const uint32_t d = ok ? (keys_in[e] >> shift) & (kRadix - 1) : (uint32_t)kRadix;
+        const uint32_t d = ok ? (keys_in[e] >> shift) & (R - 1) : (uint32_t)R;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        if (ok && (peers & lt) == 0u) cnt[warp][d] += (uint32_t)__popc(peers);
+        if (ok && (peers & lt) == 0u) cnt(warp, d) += (uint32_t)__popc(peers);
     }
     __syncthreads();
     // global start of every (warp, digit) run of this tile
-    {
-        const int d = threadIdx.x;
+    for (int d = threadIdx.x; d < R; d += kSortThreads) {
         uint32_t run = offs[(int64_t)d * ntiles + blockIdx.x];
         for (int w = 0; w < kSortWarps; w++) {
-            const uint32_t c = cnt[w][d];
-            cnt[w][d] = run;
+            const uint32_t c = cnt(w, d);
+            cnt(w, d) = run;
             run += c;
         }
     }
@@ -95,17 +103,33 @@ k_radix_downsweep(const uint32_t *__restrict__ keys_in, const uint32_t *__restri
             key = keys_in[e];
             val = vals_in[e];
         }
-        const uint32_t d = ok ? (key >> shift) & (kRadix - 1) : (uint32_t)kRadix;
+        const uint32_t d = ok ? (key >> shift) & (R - 1) : (uint32_t)R;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         if (ok) {
-            const uint32_t pos = cnt[warp][d] + (uint32_t)__popc(peers & lt);
+            const uint32_t pos = cnt(warp, d) + (uint32_t)__popc(peers & lt);
             keys_out[pos] = key;
             vals_out[pos] = val;
         }
         __syncwarp();
-        if (ok && (peers & lt) == 0u) cnt[warp][d] += (uint32_t)__popc(peers);
+        if (ok && (peers & lt) == 0u) cnt(warp, d) += (uint32_t)__popc(peers);
         __syncwarp();
     }
+}
+
+template <int RB>
+void radix_pass(const uint32_t *ki, const uint32_t *vi, uint32_t *ko, uint32_t *vo, int64_t n, int shift,
+                int64_t ntiles, uint32_t *hist, uint32_t *scan_tmp, cudaStream_t st) {
+    constexpr int R = 1 << RB;
+    const size_t smem = (size_t)kSortWarps * R * sizeof(uint32_t);
+    if (smem > 48 * 1024)   // set on every call: the attribute belongs to the current device's context
+        GB_CUDA(cudaFuncSetAttribute(k_radix_downsweep<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    k_radix_upsweep<RB><<<(unsigned)ntiles, kSortThreads, 0, st>>>(ki, n, shift, ntiles, hist); note_launch();
+    GB_CUDA(cudaGetLastError());
+    exclusive_scan_u32(hist, hist, (int64_t)R * ntiles, scan_tmp, st);
+    k_radix_downsweep<RB><<<(unsigned)ntiles, kSortThreads, smem, st>>>(ki, vi, ko, vo, n, shift, ntiles, hist);
+    note_launch();
+    GB_CUDA(cudaGetLastError());
 }
 
 // Exclusive scan of the kScanTile counts of each tile in shared memory,
@@ -212,9 +236,11 @@ void sort_pairs(const uint32_t *keys_in, uint32_t *keys_out, const uint32_t *val
                 int end_bit, DevBuf<unsigned char> &tmp, cudaStream_t st) {
     if (n <= 0) return;
     if (n >= (1ll << 31)) fail(GB_ERR_INVALID_ARGUMENT, "sort of 2^31 or more elements");
-    const int passes = std::max(1, (end_bit + 7) / 8);
+    end_bit = std::max(1, std::min(end_bit, 32));
+    const int passes = (end_bit + kMaxRadixBits - 1) / kMaxRadixBits;
+    const int rb = std::max(4, (end_bit + passes - 1) / passes);   // digit bits, 4..11
     const int64_t ntiles = (n + kSortTile - 1) / kSortTile;
-    const int64_t nhist = ntiles * kRadix;
+    const int64_t nhist = ntiles << rb;
     size_t scan_bytes = 0;
     scan_scratch_need(nhist, &scan_bytes);
     // layout: hist [nhist] | scan scratch | two ping-pong (key, value) arrays
@@ -233,7 +259,7 @@ void sort_pairs(const uint32_t *keys_in, uint32_t *keys_out, const uint32_t *val
     }
     const uint32_t *ki = keys_in, *vi = vals_in;
     for (int p = 0; p < passes; p++) {
-        const int shift = 8 * p;
+        const int shift = rb * p;
         uint32_t *ko, *vo;
         if (p == passes - 1) {
             ko = keys_out;
@@ -242,12 +268,16 @@ void sort_pairs(const uint32_t *keys_in, uint32_t *keys_out, const uint32_t *val
             ko = pk[p & 1];
             vo = pv[p & 1];
         }
-        k_radix_upsweep<<<(unsigned)ntiles, kSortThreads, 0, st>>>(ki, n, shift, ntiles, hist); note_launch();
-        GB_CUDA(cudaGetLastError());
-        exclusive_scan_u32(hist, hist, nhist, scan_tmp, st);
-        k_radix_downsweep<<<(unsigned)ntiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n, shift, ntiles, hist);
-        note_launch();
-        GB_CUDA(cudaGetLastError());
+        switch (rb) {
+        case 4: radix_pass<4>(ki, vi, ko, vo, n, shift, ntiles, hist, scan_tmp, st); break;
+        case 5: radix_pass<5>(ki, vi, ko, vo, n, shift, ntiles, hist, scan_tmp, st); break;
+        case 6: radix_pass<6>(ki, vi, ko, vo, n, shift, ntiles, hist, scan_tmp, st); break;
+        case 7: radix_pass<7>(ki, vi, ko, vo, n, shift, ntiles, hist, scan_tmp, st); break;
+        case 8: radix_pass<8>(ki, vi, ko, vo, n, shift, ntiles, hist, scan_tmp, st); break;
+        case 9: radix_pass<9>(ki, vi, ko, vo, n, shift, ntiles, hist, scan_tmp, st); break;
+        case 10: radix_pass<10>(ki, vi, ko, vo, n, shift, ntiles, hist, scan_tmp, st); break;
+        default: radix_pass<11>(ki, vi, ko, vo, n, shift, ntiles, hist, scan_tmp, st); break;
+        }
         ki = ko;
         vi = vo;
     }

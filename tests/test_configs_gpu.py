@@ -169,3 +169,49 @@ def test_traj_grad_fd_3d_alpha_1_5_w4():
     err, frac = _fd_check(traj, (64, 64, 64), (96, 96, 96), 4.0, nb=2, seed=29)
     assert frac > 0.5
     assert err <= FD_TOL, err
+
+
+def test_batched_many_frames_register_staged_path():
+    """48 uneven frames of 64^2 (mos 128, 64 tiles a frame): the gridding
+    launch of E^H E is more than 8 resident waves deep, which selects the
+    register-staged gridding over the plan's sorted sample layout (small
+    launches take the warp-specialized kernel over the interleaved layout,
+    covered by every other CG test).  Frame-independent CG against one
+    oracle solve per frame."""
+    dev = torch.device("cuda:0")
+    N, mos, W, C, F, iters = 64, 128, 5.5, 8, 48, 6
+    spokes = [4 + (f * 5) % 9 for f in range(F)]
+    trajs = [S.radial_golden_angle_2d(s, 64, profile_offset=sum(spokes[:f])) for f, s in enumerate(spokes)]
+    offs = np.cumsum([0] + [t.shape[0] for t in trajs]).tolist()
+    traj = np.concatenate(trajs, 0)
+    sq = np.concatenate([np.sqrt(S.ramp_dcw(t)) for t in trajs]).astype(np.float32)
+    csm = S.gaussian_bump_csm((N, N), C)
+    base = S.ellipse_phantom((N, N), 8, 41)
+    rng = np.random.default_rng(42)
+    ph = np.stack([base * rng.uniform(0.9, 1.1) for _ in range(F)], 0).astype(np.complex64)
+    d = np.zeros((C, offs[-1]), np.complex64)
+    ops = []
+    for f in range(F):
+        P = O.OraclePlan((N, N), (mos, mos), W)
+        P.preprocess(trajs[f][None])
+        Ef = O.OracleSense(P, csm, sq[offs[f]:offs[f + 1]][None])
+        d[:, offs[f]:offs[f + 1]] = Ef.mult_M(ph[f:f + 1]).reshape(C, -1)
+        ops.append(Ef)
+    E = gb.cuNonCartesianSenseOperator(2)
+    E.setup((N, N), (mos, mos), W)
+    E.set_csm(torch.from_numpy(csm).to(dev))
+    E.set_dcw(torch.from_numpy(sq).to(dev))
+    E.preprocess(torch.from_numpy(traj).to(dev), frame_offsets=offs)
+    E.get_plan().set_tiling((16, 16), 8)
+    cg = gb.cuCgSolver()
+    cg.set_encoding_operator(E)
+    cg.set_max_iterations(iters)
+    cg.set_tc_tolerance(0.0)
+    cg.set_frame_independent(True)
+    for use_graph in (False, True):
+        cg.set_use_graph(use_graph)
+        xb = cg.solve(torch.from_numpy(d).to(dev)).cpu().numpy()
+        for f in range(0, F, 7):
+            xr = O.cg_solve(ops[f], d[:, offs[f]:offs[f + 1]][:, None, :], iterations=iters, tc_tolerance=0.0)
+            assert rel_l2(xb[f], xr[0]) <= CG_TOL, (use_graph, f)
+    assert E.get_plan().device_errors() == 0
