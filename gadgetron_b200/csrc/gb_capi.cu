@@ -275,6 +275,18 @@ GB_API gb_status gb_nufft_autotune(gb_nufft_plan plan, uint32_t num_batches, voi
     });
 }
 
+GB_API gb_status gb_nufft_time_normal_convolutions(gb_nufft_plan plan, uint32_t num_batches, const float *dcw,
+                                                   uint32_t reps, void *flush, uint64_t flush_bytes,
+                                                   float *ms_grid, float *ms_degrid, void *stream) {
+    return guarded([&] {
+        if (!plan || !ms_grid || !ms_degrid) fail(GB_ERR_INVALID_ARGUMENT, "NULL argument");
+        DeviceGuard g((*plan->p).device);
+        nufft_time_normal_convolutions(*plan->p, count_arg(num_batches, "number of batches"), dcw,
+                                       count_arg(reps, "repetitions"), flush, (size_t)flush_bytes, ms_grid,
+                                       ms_degrid, S(stream));
+    });
+}
+
 GB_API gb_status gb_nufft_get_tiling(gb_nufft_plan plan, int *tile, int *coil_group) {
     return guarded([&] {
         if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");

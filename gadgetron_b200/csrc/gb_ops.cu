@@ -201,6 +201,48 @@ void nufft_normal(NufftPlan &p, const float2 *img, const float2 *csm, int nb, co
     nufft_adjoint(p, samp, lay, nullptr, csm, nb, out, false, accumulate, weight, CUFFT_INVERSE, st);
 }
 
+// Device time of the two convolutions of E^H E (degridding with dcw^2 into
+// the plan's sample workspace, gridding back into the k-space workspace),
+// each launched `reps` times exactly as the normal operator launches them,
+// on the plan's own workspaces.  Before every launch `flush_bytes` of
+// `flush` are overwritten (cudaMemsetAsync) so that each one starts with a
+// cold L2.  Averages in milliseconds.
+void nufft_time_normal_convolutions(NufftPlan &p, int nb, const float *dcw, int reps, void *flush,
+                                    size_t flush_bytes, float *ms_grid, float *ms_degrid, cudaStream_t st) {
+    if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "preprocess has not been called");
+    if (reps <= 0) fail(GB_ERR_INVALID_ARGUMENT, "reps must be positive");
+    const int64_t nbf = (int64_t)nb * p.F;
+    float2 *kg = ensure_kgrid(p, nbf);
+    float2 *samp = ensure_samp(p, nb);
+    launch_grid_prepare(p, nb, st);
+    const KLayout kl = ws_layout(p, nbf);
+    const SampleLayout lay = normal_op_layout(p, nb);
+    GB_CUDA(cudaMemsetAsync(kg, 0, (size_t)nbf * p.kp.G * sizeof(float2), st));
+    cudaEvent_t e0, e1;
+    GB_CUDA(cudaEventCreate(&e0));
+    GB_CUDA(cudaEventCreate(&e1));
+    double tg = 0.0, td = 0.0;
+    for (int r = 0; r < reps + 1; r++) {   // the first round warms up, untimed
+        for (int which = 0; which < 2; which++) {
+            if (flush && flush_bytes) GB_CUDA(cudaMemsetAsync(flush, r & 0xff, flush_bytes, st));
+            GB_CUDA(cudaEventRecord(e0, st));
+            if (which == 0)
+                launch_degrid(p, kg, samp, nb, lay, dcw, 2, true, false, st, &kl);
+            else
+                launch_grid(p, samp, kg, nb, lay, nullptr, true, false, st, &kl);
+            GB_CUDA(cudaEventRecord(e1, st));
+            GB_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            GB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (r > 0) (which == 0 ? td : tg) += ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms_grid = (float)(tg / reps);
+    *ms_degrid = (float)(td / reps);
+}
+
 void nufft_compute(NufftPlan &p, const void *in, void *out, const float *dcw, gb_comp_mode mode,
                    int nb, bool image_os, cudaStream_t st) {
     if (!p.prepped) fail(GB_ERR_NOT_PREPROCESSED, "NFFT_plan::compute: preprocess has not been called");

@@ -88,6 +88,8 @@ void nufft_normal(NufftPlan &p, const float2 *img, const float2 *csm, int nb, co
 void nufft_compute(NufftPlan &p, const void *in, void *out, const float *dcw, gb_comp_mode mode, int nb,
                    bool image_os, cudaStream_t st);
 void nufft_mult_MH_M(NufftPlan &p, const void *in, void *out, const float *dcw, int nb, cudaStream_t st);
+void nufft_time_normal_convolutions(NufftPlan &p, int nb, const float *dcw, int reps, void *flush,
+                                    size_t flush_bytes, float *ms_grid, float *ms_degrid, cudaStream_t st);
 void nufft_convolve(NufftPlan &p, const void *in, void *out, gb_conv_mode mode, bool accumulate, int nb,
                     cudaStream_t st);
 void nufft_fft(NufftPlan &p, void *data, gb_fft_mode mode, bool do_scale, int nbf, cudaStream_t st);

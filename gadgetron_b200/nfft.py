@@ -145,6 +145,17 @@ class cuNFFT_plan:
         """Time candidate tilings on this trajectory and keep the fastest."""
         check(lib.gb_nufft_autotune(self._h, int(num_batches), _stream()))
 
+    def time_normal_convolutions(self, num_batches: int, dcw: Optional[torch.Tensor] = None, reps: int = 20,
+                                 flush: Optional[torch.Tensor] = None):
+        """Diagnostic: ms per launch of the gridding and the degridding that
+        E^H E runs for num_batches batches (cold L2 when a flush buffer is
+        given).  Returns (ms_grid, ms_degrid)."""
+        g, d = ctypes.c_float(), ctypes.c_float()
+        fb = 0 if flush is None else flush.numel() * flush.element_size()
+        check(lib.gb_nufft_time_normal_convolutions(self._h, int(num_batches), _ptr(dcw), int(reps), _ptr(flush),
+                                                    int(fb), ctypes.byref(g), ctypes.byref(d), _stream()))
+        return float(g.value), float(d.value)
+
     def set_tiling(self, tile: Sequence[int], coil_group: int):
         t = (ctypes.c_int * 3)(*(list(tile) + [1] * (3 - len(tile))))
         check(lib.gb_nufft_set_tiling(self._h, t, int(coil_group)))

@@ -211,6 +211,19 @@ GB_API gb_status gb_nufft_device_errors(gb_nufft_plan plan, uint32_t *error_bits
  * Synchronises the stream.  No reference counterpart. */
 GB_API gb_status gb_nufft_autotune(gb_nufft_plan plan, uint32_t num_batches, void *stream);
 
+/* Diagnostic: device time (CUDA events on `stream`) of the two convolutions
+ * inside the normal operator E^H E for `num_batches` batches -- degridding
+ * into the plan's sample workspace with dcw applied twice (dcw may be NULL),
+ * then gridding back into its k-space workspace -- launched `reps` times
+ * each after one untimed round, exactly as E^H E launches them (same
+ * kernels, same workspace layouts).  When flush is not NULL, flush_bytes of
+ * it are overwritten before every launch so each one starts with a cold L2.
+ * Averages in milliseconds; the workspaces' contents are overwritten.
+ * Synchronises the stream.  No reference counterpart. */
+GB_API gb_status gb_nufft_time_normal_convolutions(gb_nufft_plan plan, uint32_t num_batches, const float *dcw,
+                                                   uint32_t reps, void *flush, uint64_t flush_bytes,
+                                                   float *ms_grid, float *ms_degrid, void *stream);
+
 /* Tile configuration used by the gridding kernels (chosen by the autotuner
  * when GB_FLAG_AUTOTUNE is set, else defaults), for inspection. */
 GB_API gb_status gb_nufft_get_tiling(gb_nufft_plan plan, int *tile, int *coil_group);

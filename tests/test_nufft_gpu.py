@@ -290,3 +290,18 @@ def test_autotune_keeps_parity(cuda):
     plan.compute(x, y, None, gb.NFFT_comp_mode.FORWARDS_C2NC)
     assert rel_l2(y.cpu().numpy(), ref) <= PARITY_TOL
     del before
+
+
+def test_time_normal_convolutions_diagnostic(cuda):
+    """The diagnostic timing of E^H E's two convolutions returns positive
+    times and leaves the plan usable (its workspaces are scratch)."""
+    case = radial_case(N=64, spokes=32, samples=128, batches=8, seed=19)
+    plan, orc, _ = _plan_and_oracle(case)
+    dcw = torch.from_numpy(case["dcw"]).to(cuda)
+    flush = torch.empty(64 * 1024 * 1024 // 4, dtype=torch.float32, device=cuda)
+    tg, td = plan.time_normal_convolutions(8, dcw, reps=3, flush=flush)
+    assert 0.0 < tg < 100.0 and 0.0 < td < 100.0
+    x = torch.from_numpy(case["img"]).to(cuda)
+    out = torch.empty_like(x)
+    plan.mult_MH_M(x, out, dcw)
+    assert rel_l2(out.cpu().numpy(), orc.mult_MH_M(case["img"], case["dcw"].reshape(1, -1))) <= PARITY_TOL
