@@ -19,7 +19,7 @@ _EXPORTS = {
     "lib": "._lib",
     "NFFT": ".nfft", "ConvolutionType": ".nfft", "NFFT_comp_mode": ".nfft", "NFFT_conv_mode": ".nfft",
     "NFFT_fft_mode": ".nfft", "NFFT_prep_mode": ".nfft", "cuNFFT_plan": ".nfft", "FLAG_AUTOTUNE": ".nfft",
-    "FLAG_COMPENSATED": ".nfft",
+    "FLAG_COMPENSATED": ".nfft", "FLAG_REFERENCE_FOLD": ".nfft",
     "cuNonCartesianSenseOperator": ".sense",
     "cuCgSolver": ".solvers",
     "cuCgPreconditioner": ".operators", "cuImageOperator": ".operators", "sense_precond_weights": ".operators",

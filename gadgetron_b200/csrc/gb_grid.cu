@@ -55,6 +55,7 @@ struct ConvArgs {
     int nb;
     int layout;               // SampleLayout
     int il_stride;            // SORTED_IL: float2 per sample row (nb rounded up to even)
+    const uint32_t *home_key; // sorted home keys (frame * ntiles_total + tile)
     const float *dcw;         // original order, may be null
     int dcw_pow;
     int sign_fold;
@@ -1037,6 +1038,113 @@ k_grid_rows_ws(ConvArgs a, const float2 *__restrict__ samples, float2 *__restric
     epilogue();
 }
 
+// ------------------------------------------ reference fold (3D, opt-in) --
+//
+// GB_FLAG_REFERENCE_FOLD.  The reference grids onto a padded grid and folds
+// the ring back in wrap_image_kernel (ConvolverNC2C_standard.cuh:394-437):
+// for each nonempty combination of dimensions it tries the 2^d wrap
+// directions and adds the first periodic image whose dimensions all wrap.
+// It tests whether dimension i (1-based) belongs to a combination with
+// `i & combination` (:411-413), which for i = 3 looks at bits 0|1 instead of
+// bit 2.  ref_fold_mult() restates that loop: how many times the periodic
+// image at shift sigma (per dimension -1, 0, +1) is added to a cell in state
+// st (per dimension 0 inside, 1 within the ring width of the low face, 2 of
+// the high face).  It is 1 everywhere in 1D and 2D, and in 3D differs from 1
+// only on cells within the ring width of a z face.  The periodic gridding
+// counts every image once, so after it k_ref_fold_fix adds (mult - 1) times
+// each wrapped tap's contribution (float atomics: few taps -- only samples
+// whose footprint crosses the grid's edge have wrapped taps).
+__device__ int ref_fold_mult(int D, const int *st, const int *sigma) {
+    bool zero = true;
+    for (int d = 0; d < D; d++) zero &= sigma[d] == 0;
+    if (zero) return 1;
+    int count = 0;
+    for (int comb = 1; comb < (1 << D); comb++) {
+        int nd = 0;
+        for (int i = 0; i < D; i++) nd += (comb & (1 << i)) != 0;
+        for (int sel = 0; sel < (1 << nd); sel++) {
+            int stride[kMaxD] = {0, 0, 0}, wraps = 0, skipped = 0;
+            for (int i = 1; i <= D; i++) {
+                if (i & comb) {
+                    if (i & (sel << skipped)) {
+                        if (st[i - 1] == 2) { stride[i - 1] = -1; wraps++; }
+                    } else {
+                        if (st[i - 1] == 1) { stride[i - 1] = 1; wraps++; }
+                    }
+                } else {
+                    skipped++;
+                }
+            }
+            if (wraps == nd) {
+                bool same = true;
+                for (int d = 0; d < D; d++) same &= stride[d] == sigma[d];
+                count += same ? 1 : 0;
+                break;
+            }
+        }
+    }
+    return count;
+}
+
+// One thread per sorted sample; samples whose footprint stays inside the
+// grid return at once.
+__global__ void k_ref_fold_fix(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__ grid) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const KParams &k = a.k;
+    if (j >= a.Mtot) return;
+    int lo[3], n[3];
+    bool crosses = false;
+    for (int d = 0; d < 3; d++) {
+        const float s = a.pos[(int64_t)d * a.Mtot + j];
+        lo[d] = (int)ceilf(s - k.radius);
+        n[d] = min((int)floorf(s + k.radius) - lo[d] + 1, kWMax);
+        const int u0 = lo[d] - k.hw, u1 = u0 + n[d] - 1;
+        crosses |= u0 < 0 || u1 >= k.mos[d];
+    }
+    if (!crosses) return;
+    const int f = (int)(a.home_key[j] / (uint32_t)k.ntiles_total);
+    const uint32_t jo = a.perm[j];
+    const float dw = a.dcw ? a.dcw[jo] : 1.f;
+    const float *wt = a.wtab + j * 3 * kWMax;
+    for (int tz = 0; tz < n[2]; tz++)
+        for (int ty = 0; ty < n[1]; ty++)
+            for (int tx = 0; tx < n[0]; tx++) {
+                const int t[3] = {tx, ty, tz};
+                int sigma[3], st[3], co[3];
+                bool wrapped = false;
+                for (int d = 0; d < 3; d++) {
+                    const int u = lo[d] + t[d] - k.hw;
+                    sigma[d] = u < 0 ? -1 : (u >= k.mos[d] ? 1 : 0);
+                    co[d] = u - sigma[d] * k.mos[d];
+                    st[d] = co[d] < k.hw ? 1 : (co[d] >= k.mos[d] - k.hw ? 2 : 0);
+                    wrapped |= sigma[d] != 0;
+                }
+                if (!wrapped) continue;
+                const int m = ref_fold_mult(3, st, sigma) - 1;
+                if (m == 0) continue;
+                float w = wt[tx] * (wt[kWMax + ty] * wt[2 * kWMax + tz]);
+                if (a.sign_fold && ((co[0] + co[1] + co[2]) & 1)) w = -w;
+                w *= (float)m * dw;
+                const int64_t cell = (int64_t)co[2] * a.kl.s_z + (int64_t)co[1] * a.kl.s_y + co[0];
+                for (int b = 0; b < a.nb; b++) {
+                    float2 v;
+                    if (a.layout == LAYOUT_SORTED_IL) v = samples[j * a.il_stride + b];
+                    else if (a.layout == LAYOUT_SORTED) v = samples[(int64_t)b * a.Mtot + j];
+                    else v = samples[(int64_t)b * a.Mtot + jo];
+                    float *o = reinterpret_cast<float *>(grid + ((int64_t)b * a.F + f) * a.kl.s_bf + cell);
+                    atomicAdd(o, w * v.x);
+                    atomicAdd(o + 1, w * v.y);
+                }
+            }
+}
+
+static void launch_ref_fold_fix(const NufftPlan &p, const ConvArgs &a, const float2 *samples, float2 *grid,
+                                cudaStream_t st) {
+    if (!(p.flags & GB_FLAG_REFERENCE_FOLD) || p.D != 3 || p.Mtot == 0) return;
+    k_ref_fold_fix<<<(unsigned)((p.Mtot + 255) / 256), 256, 0, st>>>(a, samples, grid); ::gb::note_launch();
+    GB_CUDA(cudaGetLastError());
+}
+
 // --------------------------------------------------------------- C2NC -----
 
 // Staged region of a home tile: tile + pad/2 cells on each side.
@@ -1559,6 +1667,7 @@ static ConvArgs make_args(NufftPlan &p, int nb, SampleLayout layout, const float
     a.nb = nb;
     a.layout = layout;
     a.il_stride = il_stride_for(nb);
+    a.home_key = p.pp_key_sorted.get();
     a.dcw = dcw;
     a.dcw_pow = dcw_pow;
     a.sign_fold = sign_fold ? 1 : 0;
@@ -1751,6 +1860,7 @@ void launch_grid(NufftPlan &p, const float2 *samples, float2 *grid, int nb, Samp
     }
     if (p.n_grd_items == 0) return;
     grid_dispatch_cfg(c, p, a, samples, grid, st);
+    launch_ref_fold_fix(p, a, samples, grid, st);
 }
 
 // The warp-specialized gridding (and so the interleaved workspace) wins when
@@ -1797,6 +1907,7 @@ void launch_grid_external_scratch(NufftPlan &p, const float2 *samples, float2 *g
     a.counters = counters;
     if (p.n_grd_items == 0) return;
     grid_dispatch_cfg(c, p, a, samples, grid, st);
+    launch_ref_fold_fix(p, a, samples, grid, st);
 }
 
 template <int CG, bool GRAD>

@@ -58,6 +58,7 @@ class ConvolutionType(enum.IntEnum):
 
 FLAG_COMPENSATED = 0x1
 FLAG_AUTOTUNE = 0x2
+FLAG_REFERENCE_FOLD = 0x4
 
 
 def _u64(vals):

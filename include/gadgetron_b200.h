@@ -75,6 +75,15 @@ typedef enum gb_fft_mode { GB_FFT_FORWARDS = 0, GB_FFT_BACKWARDS = 1 } gb_fft_mo
 /* Plan flags. */
 #define GB_FLAG_COMPENSATED 0x1u   /* compensated (TwoSum) in-tile accumulation */
 #define GB_FLAG_AUTOTUNE    0x2u   /* autotune at preprocess (plans: 1 batch; SENSE: its coils) */
+/* 3D gridding (NC2C) folds the padding ring as the reference's wrap_image_kernel
+ * does (toolboxes/nfft/gpu/ConvolverNC2C_standard.cuh:394-437) instead of
+ * periodically: on cells within the ring width of a z face it adds some
+ * periodic images twice and others not at all (its dimension test
+ * `i & combination`, :411-413).  For callers that need the reference's 3D
+ * adjoint bit for bit in the math (not in the rounding: the extra terms are
+ * added with float atomics, so such results are not bitwise repeatable).
+ * No effect in 1D and 2D, where the reference's fold is the periodic one. */
+#define GB_FLAG_REFERENCE_FOLD 0x4u
 
 typedef struct gb_nufft_plan_s *gb_nufft_plan;
 typedef struct gb_sense_op_s *gb_sense_op;

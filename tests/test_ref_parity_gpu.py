@@ -313,3 +313,64 @@ def test_ref_cg_oracle_pinned():
     x_ref = R.cg_sense(N, mos, W, traj, 1, csm, sq, d.reshape(C, -1), 8, 0.0)
     x_orc = O.cg_solve(orc, d, iterations=8, tc_tolerance=0.0)
     assert rel_l2(x_orc, x_ref) <= CG_TOL
+
+
+def test_ref_3d_adjoint_with_reference_fold_flag():
+    """GB_FLAG_REFERENCE_FOLD reproduces the reference's 3D fold: adjoint
+    compute, standalone NC2C convolve (plus accumulate) and the plan's
+    mult_MH_M (E^H E's own gridding path) against the reference, <= 1e-5.
+    Without the flag 2D plans are bitwise unaffected (the fold is periodic
+    there)."""
+    dev = torch.device("cuda:0")
+    N, mos, W = (64, 64, 64), (96, 96, 96), 4.0
+    traj = S.kooshball_golden_means_3d(1500, 96)
+    dcw = S.ramp_dcw(traj)
+    plan = _plan(N, mos, W, traj, flags=gb.FLAG_REFERENCE_FOLD)
+    rng = np.random.default_rng(40)
+    M = traj.shape[0]
+    y = (rng.standard_normal((2, M)) + 1j * rng.standard_normal((2, M))).astype(np.complex64)
+    x = torch.empty((2, 1, 64, 64, 64), dtype=torch.complex64, device=dev)
+    plan.compute(_t(y, dev), x, _t(dcw, dev), gb.NFFT_comp_mode.BACKWARDS_NC2C)
+    x_ref = R.nfft_compute(N, mos, W, traj, 1, y, dcw, "BACKWARDS_NC2C", 2)
+    e = rel_l2(x.cpu().numpy(), x_ref)
+    print("3D adjoint with the reference fold vs reference: %.2e" % e)
+    assert e <= PARITY_TOL, e
+    g = torch.empty((2, 1, 96, 96, 96), dtype=torch.complex64, device=dev)
+    plan.convolve(_t(y, dev), g, gb.NFFT_conv_mode.NC2C)
+    g_ref = R.nfft_convolve(N, mos, W, traj, 1, y, "NC2C", 2)
+    assert rel_l2(g.cpu().numpy(), g_ref) <= PARITY_TOL
+    plan.convolve(_t(y, dev), g, gb.NFFT_conv_mode.NC2C, accumulate=True)
+    assert rel_l2(g.cpu().numpy(), 2 * g_ref) <= PARITY_TOL
+    img = S.gaussian_image((2, 1, 64, 64, 64), 41)
+    out = torch.empty_like(_t(img, dev))
+    plan.mult_MH_M(_t(img, dev), out, _t(dcw, dev))
+    assert rel_l2(out.cpu().numpy(), R.nfft_mult_MH_M(N, mos, W, traj, 1, img, dcw, 2)) <= PARITY_TOL
+    # 2D: the flag changes nothing
+    N2, mos2 = (64, 64), (128, 128)
+    t2 = S.radial_golden_angle_2d(32, 128)
+    y2 = (rng.standard_normal((2, t2.shape[0])) + 1j * rng.standard_normal((2, t2.shape[0]))).astype(np.complex64)
+    outs = []
+    for flags in (0, gb.FLAG_REFERENCE_FOLD):
+        p2 = _plan(N2, mos2, 5.5, t2, flags=flags)
+        o = torch.empty((2, 1, 64, 64), dtype=torch.complex64, device=dev)
+        p2.compute(_t(y2, dev), o, None, gb.NFFT_comp_mode.BACKWARDS_NC2C)
+        outs.append(o)
+    assert torch.equal(outs[0], outs[1])
+
+
+def test_ref_3d_adjoint_reference_fold_full_sample_count():
+    """The 3D benchmark geometry (128^3 -> 192^3, 5.12M samples) with the
+    reference fold: within the reference's own FP32 drift at this size."""
+    dev = torch.device("cuda:0")
+    N, mos, W = (128, 128, 128), (192, 192, 192), 4.0
+    traj = S.kooshball_golden_means_3d(20000, 256)
+    dcw = S.ramp_dcw(traj)
+    plan = _plan(N, mos, W, traj, flags=gb.FLAG_REFERENCE_FOLD)
+    rng = np.random.default_rng(42)
+    y = (rng.standard_normal((1, traj.shape[0])) + 1j * rng.standard_normal((1, traj.shape[0]))).astype(np.complex64)
+    x = torch.empty((1, 1, 128, 128, 128), dtype=torch.complex64, device=dev)
+    plan.compute(_t(y, dev), x, _t(dcw, dev), gb.NFFT_comp_mode.BACKWARDS_NC2C)
+    x_ref = R.nfft_compute(N, mos, W, traj, 1, y, dcw, "BACKWARDS_NC2C", 1)
+    e = rel_l2(x.cpu().numpy(), x_ref)
+    print("3D full-size adjoint with the reference fold vs reference: %.2e" % e)
+    assert e <= 5e-5, e
