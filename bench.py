@@ -1011,6 +1011,9 @@ def headline_extras(args, wl, d_host, x_out):
                       against the reference's own cuNFFT and the FP64 NDFT;
     batched        -- 64 uneven frames (192^2, 12 coils, 15 iterations):
                       batched graph-captured solve vs the plain per-frame form;
+    nufft_3d       -- the 3D kooshball NUFFT (128^3 -> 192^3, 5.12M samples, 32
+                      coils, W 4): forward + adjoint throughput and the trajectory
+                      gradient against central finite differences (64 samples);
     reference_gpu  -- the reference's own GPU path (built from its sources)
                       on the same B200: cuCgSolver ms/recon on this workload
                       and cuNFFT on the 2D NUFFT case, and the product's
@@ -1103,6 +1106,16 @@ def headline_extras(args, wl, d_host, x_out):
     else:
         ref_gpu["unavailable"] = "oracle/_ref/libgbref.so not built"
     out["reference_gpu"] = ref_gpu
+
+    # --- 3D kooshball NUFFT with the trajectory gradient (128^3 -> 192^3,
+    # 20000 x 256 samples, 32 coils, W 4): throughput and the central
+    # finite-difference check of the gradient on 64 samples
+    try:
+        n3 = run_nufft(_copy_args(args, steps=3, warmup=3, size="full"), 3)
+        out["nufft_3d"] = {k: n3[k] for k in ("value", "unit", "ms_forward", "ms_adjoint", "config",
+                                              "forward_rel_l2_vs_fp64_ndft", "fd_gradient")}
+    except Exception as e:  # reported, never gates the headline
+        out["nufft_3d"] = {"error": str(e)}
     return out
 
 
