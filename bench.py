@@ -692,7 +692,10 @@ def run_batched(args):
         E.get_plan().set_tiling((tx, ty), cgr)
     else:
         E.autotune()   # tile shape and coil group for this trajectory set
+    if getattr(args, "schedule", None) is not None:
+        E.get_plan().set_grid_schedule(args.schedule)
     tiling = E.get_plan().get_tiling()
+    schedule = E.get_plan().get_grid_schedule()
     y = torch.empty((C, offs[-1]), dtype=torch.complex64, device=dev)
     E.mult_M(torch.from_numpy(ph).to(dev), y)
     rms = float(y.abs().pow(2).mean().sqrt())
@@ -746,6 +749,7 @@ def run_batched(args):
         "plain_per_frame_ms": round(ms_p, 3), "speedup_vs_plain": round(ms_p / ms_b, 2),
         "batched_vs_plain_rel_l2": err, "gpu_launches_per_batch": int(launches),
         "tiling_after_autotune": {"tile": list(tiling[0]), "coil_group": tiling[1]},
+        "grid_schedule": schedule,
     }
 
 
@@ -937,6 +941,9 @@ def main():
     ap.add_argument("--tiling", default=None,
                     help="batched workload: fixed tile and coil group 'tx,ty,cg' instead of the "
                          "autotuner's choice (profiling runs, whose launch timings the profiler skews)")
+    ap.add_argument("--schedule", type=int, default=None, choices=[0, 1, 2],
+                    help="batched workload: gridding schedule of the normal operator (0 by launch depth, "
+                         "1 one CTA per work item, 2 persistent work queue); default 0")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -1071,7 +1078,7 @@ def headline_extras(args, wl, d_host, x_out):
         b = run_batched(_copy_args(args, steps=5, warmup=3, size="full", tiling=None))
         out["batched"] = {k: b[k] for k in ("value", "unit", "plain_per_frame_ms", "speedup_vs_plain",
                                             "batched_vs_plain_rel_l2", "tiling_after_autotune",
-                                            "gpu_launches_per_batch")}
+                                            "grid_schedule", "gpu_launches_per_batch")}
         out["batched"]["config"] = b["config"]
     except Exception as e:  # reported, never gates the headline
         out["batched"] = {"error": str(e)}

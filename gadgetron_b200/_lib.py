@@ -71,6 +71,8 @@ def _load():
         "gb_nufft_autotune": (i32, [P, u32, P]),
         "gb_sense_autotune": (i32, [P, P]),
         "gb_nufft_set_tiling": (i32, [P, P, i32]),
+        "gb_nufft_set_grid_schedule": (i32, [P, i32]),
+        "gb_nufft_get_grid_schedule": (i32, [P, P]),
         "gb_sense_create": (i32, [i32, P, P, f32, u32, P]),
         "gb_sense_destroy": (i32, [P]),
         "gb_sense_preprocess": (i32, [P, P, u64, u32, P, P]),
@@ -127,7 +129,7 @@ EXPORTED = (
     "gb_nufft_compute gb_nufft_mult_MH_M gb_nufft_convolve gb_nufft_convolve_nc2c_noalloc gb_nufft_fft gb_nufft_deapodize "
     "gb_nufft_traj_grad gb_nufft_traj_grad_from_grid gb_nufft_get_info gb_nufft_device_errors gb_nufft_get_tiling gb_nufft_autotune "
     "gb_nufft_time_normal_convolutions "
-    "gb_nufft_set_tiling gb_sense_create gb_sense_destroy gb_sense_preprocess gb_sense_set_csm "
+    "gb_nufft_set_tiling gb_nufft_set_grid_schedule gb_nufft_get_grid_schedule gb_sense_create gb_sense_destroy gb_sense_preprocess gb_sense_set_csm "
     "gb_sense_set_dcw gb_sense_mult_M gb_sense_mult_MH gb_sense_mult_MH_M gb_sense_get_nufft_plan gb_sense_autotune "
     "gb_cg_create gb_cg_destroy gb_cg_set_encoding_operator gb_cg_set_max_iterations "
     "gb_cg_set_tc_tolerance gb_cg_set_x0 gb_cg_set_preconditioner gb_cg_set_identity_regularization "

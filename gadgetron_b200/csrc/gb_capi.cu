@@ -309,6 +309,21 @@ GB_API gb_status gb_nufft_set_tiling(gb_nufft_plan plan, const int *tile, int co
     });
 }
 
+GB_API gb_status gb_nufft_set_grid_schedule(gb_nufft_plan plan, int schedule) {
+    return guarded([&] {
+        if (!plan) fail(GB_ERR_INVALID_ARGUMENT, "NULL plan");
+        if (schedule < 0 || schedule > 2) fail(GB_ERR_INVALID_ARGUMENT, "schedule must be 0, 1 or 2");
+        (*plan->p).tiling.schedule = schedule;
+    });
+}
+
+GB_API gb_status gb_nufft_get_grid_schedule(gb_nufft_plan plan, int *schedule) {
+    return guarded([&] {
+        if (!plan || !schedule) fail(GB_ERR_INVALID_ARGUMENT, "NULL argument");
+        *schedule = (*plan->p).tiling.schedule;
+    });
+}
+
 // ---------------------------------------------------------------- SENSE ---
 
 GB_API gb_status gb_sense_create(int D, const uint64_t *matrix_size, const uint64_t *matrix_size_os, float W,

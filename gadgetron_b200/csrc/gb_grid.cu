@@ -70,6 +70,8 @@ struct ConvArgs {
     const float *prows;       // gridding pair rows (row variant)
     int prow_floats;
     unsigned int *err;        // bounded-wait failure flag
+    unsigned int *queue;      // persistent gridding: [0] next work unit, [1] CTAs finished
+    int n_work;               // persistent gridding: work units (items x coil groups)
 };
 
 __device__ __forceinline__ float sign_of(int g) { return (g & 1) ? -1.f : 1.f; }
@@ -1038,6 +1040,364 @@ k_grid_rows_ws(ConvArgs a, const float2 *__restrict__ samples, float2 *__restric
     epilogue();
 }
 
+// ---------------------- NC2C, row variant, warp-specialized, persistent --
+//
+// k_grid_rows_ws as one persistent launch over every work unit (gridding
+// item x coil group) of all frames: kWsMinBlocks CTAs per SM take units from
+// a global counter (units in list order: split chunks of heavy tiles first),
+// and the producer warp streams chunk after chunk across unit boundaries, so
+// the copy pipeline does not drain between tiles and no CTA pays a launch
+// ramp per tile.  Every stage carries a descriptor of its chunk (unit, sample
+// count, first/last flags); the consumer warps zero their accumulators on a
+// unit's first chunk and write the tile out after its last one, through a
+// tile buffer of their own (the producer keeps filling stages meanwhile),
+// synchronising only among themselves (an mbarrier of the 256 consumer
+// threads).  No CTA waits for another; the last CTA to finish resets the
+// counter for the next launch.  Every wait is bounded: a wait that runs out
+// sets err bit 0 and the CTA's bail flag, after which every wait of the CTA
+// returns at once, both loops end, and the producer waits (bounded) for its
+// copies still in flight before the CTA exits.  Per-cell summation order as
+// k_grid_rows: the result is bit-identical.
+
+struct WspDesc {
+    int ft, split, chunk, grp;
+    int cnt, flags, pad0, pad1;
+};
+constexpr int kWspFirst = 1, kWspLast = 2, kWspDone = 4, kWspEmpty = 8;
+
+// Bounded wait that reports whether the phase completed.  It gives up after
+// ~2 s (err bit 0 and *bail set) or as soon as *bail is set (bail may be null).
+__device__ __forceinline__ bool mbar_wait_ok(uint32_t bar, uint32_t parity, unsigned int *err, int *bail) {
+    for (int round = 0; round < 2; round++) {
+        for (uint32_t i = 0; i < (1u << 22); i++) {
+            if (mbar_try_wait(bar, parity)) return true;
+            if (bail && *reinterpret_cast<volatile int *>(bail)) return false;
+            if (i >= 16) __nanosleep(256);
+        }
+    }
+    if (err) atomicOr(err, 1u);
+    if (bail) *reinterpret_cast<volatile int *>(bail) = 1;
+    return false;
+}
+
+// Epilogue tile of the persistent kernel: [coil][z][y][x], rows padded by
+// one cell, coil planes at 2 (mod 8) cells (conflict-free transposition).
+__host__ __device__ __forceinline__ int wsp_plane_cells(const KParams &k) {
+    const int ps = k.tile[2] * k.tile[1] * (k.tile[0] + 1);
+    return ps + (10 - ps % 8) % 8;
+}
+__host__ __device__ __forceinline__ int wsp_smem_bytes(const KParams &k, int cg) {
+    return kWsStages * ws_stage_bytes(k, cg) + cg * wsp_plane_cells(k) * 8;
+}
+
+template <int CG, int RW, int RPW, bool D3>
+__global__ void __launch_bounds__(kWsThreads, kWsMinBlocks)
+k_grid_rows_wsp(ConvArgs a, const float2 *__restrict__ samples, float2 *__restrict__ grid) {
+    constexpr int CP = CG / 2;      // lanes per row: one per coil pair
+    constexpr int ROWS = 32 / CP;   // rows per region
+    extern __shared__ __align__(128) unsigned char g_wsp_smem[];
+    __shared__ int s_last, s_bail;
+    __shared__ __align__(8) unsigned long long s_full[kWsStages], s_empty[kWsStages], s_cons[2];
+    __shared__ WspDesc s_desc[kWsStages];
+
+    const KParams &k = a.k;
+    const int T0 = k.tile[0], T1 = k.tile[1], T2 = k.tile[2];
+    const int PRF = a.prow_floats;   // floats per pair row
+    const int PRW = PRF - 4;         // weight part; the last 4 words are the footprint ranges
+    const int stage_bytes = ws_stage_bytes(k, CG);
+    auto stage_wt = [&](int s) { return reinterpret_cast<float *>(g_wsp_smem + s * stage_bytes); };
+    auto stage_v = [&](int s) {
+        return reinterpret_cast<float2 *>(g_wsp_smem + s * stage_bytes + kChunkR * PRF * 4);
+    };
+    float2 *tl = reinterpret_cast<float2 *>(g_wsp_smem + kWsStages * stage_bytes);
+    const int PS = wsp_plane_cells(k);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool consumer = warp < 8;
+
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < kWsStages; st++) {
+            mbar_init(smem_u32(&s_full[st]), 1);
+            mbar_init(smem_u32(&s_empty[st]), 8);
+        }
+        mbar_init(smem_u32(&s_cons[0]), kThreads);
+        mbar_init(smem_u32(&s_cons[1]), kThreads);
+        mbar_fence_init();
+        s_bail = 0;
+    }
+    __syncthreads();
+
+    if (!consumer) {
+        // Producer: takes units from the counter (the next one is fetched
+        // while the current one's chunks are issued); for chunk g of the
+        // CTA's sequence, stage g % kWsStages once the consumers released its
+        // previous use: lane 0 writes the descriptor, announces the bytes
+        // (arrival + transaction count) and copies the pair rows, then every
+        // lane copies up to two sample rows (this coil group's columns).  A
+        // last descriptor flagged kWspDone ends the consumers' loop.
+        const int ncg = a.ncg;
+        uint32_t g = 0;
+        int w = 0;
+        if (lane == 0) w = (int)atomicAdd(&a.queue[0], 1u);
+        w = __shfl_sync(0xffffffffu, w, 0);
+        bool bail = false;
+        while (!bail) {
+            const bool done = w >= a.n_work;
+            int wn = w;
+            if (!done) {
+                if (lane == 0) wn = (int)atomicAdd(&a.queue[0], 1u);
+                wn = __shfl_sync(0xffffffffu, wn, 0);
+            }
+            WorkItem it{};
+            int grp = 0;
+            if (!done) {
+                it = a.items[w / ncg];
+                grp = w - (w / ncg) * ncg;
+            }
+            const int b0 = grp * CG;
+            const int n = done ? 0 : it.end - it.begin;
+            const uint32_t vbytes = n > 0 ? (uint32_t)min(CG, a.il_stride - b0) * 8u : 0u;
+            const int nch = n > 0 ? (n + kChunkR - 1) / kChunkR : 1;
+            for (int ch = 0; ch < nch; ch++, g++) {
+                const int st = (int)(g % kWsStages);
+                const uint32_t use = g / kWsStages;
+                const int base = it.begin + ch * kChunkR;
+                const int cnt = n > 0 ? min(kChunkR, it.end - base) : 0;
+                const uint32_t si0 = lane < cnt ? a.list[base + lane] : 0u;
+                const uint32_t si1 = lane + 32 < cnt ? a.list[base + lane + 32] : 0u;
+                if (use > 0 && !mbar_wait_ok(smem_u32(&s_empty[st]), (use - 1) & 1u, a.err, &s_bail)) bail = true;
+                if (*reinterpret_cast<volatile int *>(&s_bail)) bail = true;
+                if (bail) break;
+                const uint32_t full = smem_u32(&s_full[st]);
+                if (lane == 0) {
+                    WspDesc d;
+                    d.ft = it.ft;
+                    d.split = it.split;
+                    d.chunk = it.chunk;
+                    d.grp = grp;
+                    d.cnt = cnt;
+                    d.flags = (ch == 0 ? kWspFirst : 0) | (ch == nch - 1 ? kWspLast : 0) | (done ? kWspDone : 0) |
+                              (n == 0 ? kWspEmpty : 0);
+                    d.pad0 = d.pad1 = 0;
+                    s_desc[st] = d;
+                }
+                fence_proxy_async_smem();
+                if (lane == 0) {
+                    const uint32_t rbytes = (uint32_t)cnt * (uint32_t)PRF * 4u;
+                    if (cnt > 0) {
+                        mbar_expect_tx(full, rbytes + (uint32_t)cnt * vbytes);
+                        bulk_copy_g2s(smem_u32(stage_wt(st)), a.prows + (int64_t)base * PRF, rbytes, full);
+                    } else {
+                        mbar_arrive(full);
+                    }
+                }
+                __syncwarp();
+                float2 *sv = stage_v(st);
+                if (lane < cnt)
+                    bulk_copy_g2s(smem_u32(sv + lane * CG), samples + (int64_t)si0 * a.il_stride + b0, vbytes, full);
+                if (lane + 32 < cnt)
+                    bulk_copy_g2s(smem_u32(sv + (lane + 32) * CG), samples + (int64_t)si1 * a.il_stride + b0,
+                                  vbytes, full);
+            }
+            if (done) break;
+            w = wn;
+        }
+        if (bail) {
+            // the consumers stopped early: wait for the copies still in flight
+            for (uint32_t gi = g > kWsStages ? g - kWsStages : 0; gi < g; gi++)
+                mbar_wait_ok(smem_u32(&s_full[gi % kWsStages]), (gi / kWsStages) & 1u, nullptr, nullptr);
+        }
+    } else {
+        const int cp = lane % CP, row = lane / CP;
+        const int nrx = T0 / RW, nry = T1 / ROWS;
+        int qx0[RPW], qy0[RPW], qz[RPW];
+#pragma unroll
+        for (int c = 0; c < RPW; c++) {
+            const int q = warp + 8 * c;
+            qx0[c] = (q % nrx) * RW;
+            qy0[c] = ((q / nrx) % nry) * ROWS;
+            qz[c] = q / (nrx * nry);
+        }
+        float2 acc[RPW][RW][2];
+#pragma unroll
+        for (int c = 0; c < RPW; c++)
+#pragma unroll
+            for (int j = 0; j < RW; j++) acc[c][j][0] = acc[c][j][1] = make_float2(0.f, 0.f);
+
+        // Barrier of the 256 consumer threads (every thread arrives: its
+        // shared-memory writes are released to the others).
+        uint32_t ncs = 0;
+        auto consumer_bar = [&]() {
+            const uint32_t b = smem_u32(&s_cons[ncs & 1u]);
+            mbar_arrive(b);
+            mbar_wait_ok(b, (ncs >> 1) & 1u, a.err, &s_bail);
+            ncs++;
+        };
+        // Tile out through the tile buffer: lanes put their cells into the
+        // [coil][z][y][x] tile, then the 256 consumer threads store whole rows
+        // of one coil plane (coalesced).
+        auto epilogue = [&](int f, int org0, int org1, int org2, int b0) {
+            const int RS = T0 + 1, ZS = T1 * RS;
+            consumer_bar();   // the previous tile has left the buffer
+#pragma unroll
+            for (int c = 0; c < RPW; c++)
+#pragma unroll
+                for (int j = 0; j < RW; j++) {
+                    const int o = qz[c] * ZS + (qy0[c] + row) * RS + qx0[c] + j;
+                    tl[(2 * cp) * PS + o] = acc[c][j][0];
+                    tl[(2 * cp + 1) * PS + o] = acc[c][j][1];
+                }
+            consumer_bar();
+            const int x = threadIdx.x % T0, r0 = threadIdx.x / T0, rpp = kThreads / T0;
+            if (r0 >= rpp) return;
+            const int rows_c = T2 * T1;
+            const int gx = org0 + x;
+            const int64_t ostep = (int64_t)a.F * a.kl.s_bf;
+            for (int r = r0; r < rows_c; r += rpp) {
+                const int z = r / T1, y = r - z * T1;
+                const int gy = org1 + y, gz = org2 + z;
+                const float sgn = (a.sign_fold && ((gx + gy + gz) & 1)) ? -1.f : 1.f;
+                const int64_t cell = (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y + gx;
+                const float2 *src = tl + z * ZS + y * RS + x;
+                float2 *o = grid + ((int64_t)b0 * a.F + f) * a.kl.s_bf + cell;
+                for (int c = 0; c < CG && b0 + c < a.nb; c++) {
+                    float2 v = src[c * PS];
+                    v.x *= sgn;
+                    v.y *= sgn;
+                    if (a.accumulate) { const float2 old = *o; v.x += old.x; v.y += old.y; }
+                    *o = v;
+                    o += ostep;
+                }
+            }
+        };
+
+        uint32_t g = 0;
+        for (;;) {
+            const int st = (int)(g % kWsStages);
+            if (!mbar_wait_ok(smem_u32(&s_full[st]), (g / kWsStages) & 1u, a.err, &s_bail)) break;
+            const WspDesc d = s_desc[st];
+            if (d.flags & kWspDone) break;
+            if (d.flags & kWspFirst) {
+#pragma unroll
+                for (int c = 0; c < RPW; c++)
+#pragma unroll
+                    for (int j = 0; j < RW; j++) acc[c][j][0] = acc[c][j][1] = make_float2(0.f, 0.f);
+            }
+            const int cnt = d.cnt;
+            const float *wt = stage_wt(st);
+            const float4 *sv4 = reinterpret_cast<const float4 *>(stage_v(st));
+#pragma unroll
+            for (int c = 0; c < RPW; c++) {
+                const int ry = qy0[c] + row;
+#pragma unroll
+                for (int half = 0; half < kChunkR / 32; half++) {
+                    const int il = half * 32 + lane;
+                    bool hit = false;
+                    if (il < cnt) {
+                        const uint4 r = *reinterpret_cast<const uint4 *>(wt + il * PRF + PRW);
+                        hit = (int)(r.x & 0xffffu) <= qx0[c] + RW - 1 && (int)(r.x >> 16) >= qx0[c] &&
+                              (int)(r.y & 0xffffu) <= qy0[c] + ROWS - 1 && (int)(r.y >> 16) >= qy0[c];
+                        if (D3) hit = hit && (int)(r.z & 0xffffu) <= qz[c] && (int)(r.z >> 16) >= qz[c];
+                    }
+                    uint32_t bits = __ballot_sync(0xffffffffu, hit);
+                    while (bits) {
+                        const int i = half * 32 + __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        const float4 v = sv4[i * (CG / 2) + cp];
+                        const float2 v0 = make_float2(v.x, v.y), v1 = make_float2(v.z, v.w);
+                        const float *wr = wt + i * PRF;
+                        float wyz = wr[T0 + ry];
+                        if (D3) wyz *= wr[T0 + T1 + qz[c]];
+                        const float2 wyz2 = make_float2(wyz, wyz);
+#pragma unroll
+                        for (int jj = 0; jj < RW / 4; jj++) {
+                            const float4 w4 = *reinterpret_cast<const float4 *>(wr + qx0[c] + 4 * jj);
+                            const float2 w01 = __fmul2_rn(make_float2(w4.x, w4.y), wyz2);
+                            const float2 w23 = __fmul2_rn(make_float2(w4.z, w4.w), wyz2);
+                            const float wj[4] = {w01.x, w01.y, w23.x, w23.y};
+#pragma unroll
+                            for (int m = 0; m < 4; m++) {
+                                const float2 wm = make_float2(wj[m], wj[m]);
+                                float2 *ac = acc[c][4 * jj + m];
+                                ac[0] = __ffma2_rn(wm, v0, ac[0]);
+                                ac[1] = __ffma2_rn(wm, v1, ac[1]);
+                            }
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&s_empty[st]));
+            g++;
+            if (!(d.flags & kWspLast)) continue;
+
+            // The unit's tile is complete in the accumulators.
+            const int f = d.ft / k.ntiles_total;
+            const int tile = d.ft - f * k.ntiles_total;
+            const int tx = tile % k.ntiles[0];
+            const int ty = (tile / k.ntiles[0]) % k.ntiles[1];
+            const int tz = tile / (k.ntiles[0] * k.ntiles[1]);
+            const int org0 = tx * T0, org1 = ty * T1, org2 = tz * T2;
+            const int b0 = d.grp * CG;
+            if (d.split < 0) {
+                if (!((d.flags & kWspEmpty) && a.accumulate)) epilogue(f, org0, org1, org2, b0);
+                continue;
+            }
+            // Split tile: write this chunk's partial tile, the last CTA to
+            // finish one sums the partials in chunk order.
+            const SplitInfo si = a.splits[d.split];
+            auto part = [&](int slot) -> float4 * {
+                return reinterpret_cast<float4 *>(a.partials + ((int64_t)slot * a.ncg + d.grp) * a.part_elems);
+            };
+            {
+                float4 *pp = part(si.first_slot + d.chunk);
+#pragma unroll
+                for (int c = 0; c < RPW; c++)
+#pragma unroll
+                    for (int j = 0; j < RW; j++)
+                        pp[(c * RW + j) * kThreads + threadIdx.x] =
+                            make_float4(acc[c][j][0].x, acc[c][j][0].y, acc[c][j][1].x, acc[c][j][1].y);
+            }
+            __threadfence();
+            consumer_bar();
+            if (threadIdx.x == 0) {
+                unsigned int *ctr = a.counters + (int64_t)d.split * a.ncg + d.grp;
+                const unsigned int old = atomicAdd(ctr, 1u);
+                s_last = (old == (unsigned int)(si.nchunks - 1));
+                if (s_last) *ctr = 0u;   // ready for the next launch
+            }
+            consumer_bar();
+            if (!*reinterpret_cast<volatile int *>(&s_last)) continue;
+            __threadfence();
+#pragma unroll
+            for (int c = 0; c < RPW; c++)
+#pragma unroll
+                for (int j = 0; j < RW; j++) {
+                    float4 sm = make_float4(0.f, 0.f, 0.f, 0.f);
+                    for (int ch = 0; ch < si.nchunks; ch++) {
+                        const float4 v = __ldcg(&part(si.first_slot + ch)[(c * RW + j) * kThreads + threadIdx.x]);
+                        sm.x += v.x;
+                        sm.y += v.y;
+                        sm.z += v.z;
+                        sm.w += v.w;
+                    }
+                    acc[c][j][0] = make_float2(sm.x, sm.y);
+                    acc[c][j][1] = make_float2(sm.z, sm.w);
+                }
+            epilogue(f, org0, org1, org2, b0);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int old = atomicAdd(&a.queue[1], 1u);
+        if (old == gridDim.x - 1) {   // every CTA has taken its last unit
+            a.queue[0] = 0u;
+            a.queue[1] = 0u;
+            __threadfence();
+        }
+    }
+}
+
 // ------------------------------------------ reference fold (3D, opt-in) --
 //
 // GB_FLAG_REFERENCE_FOLD.  The reference grids onto a padded grid and folds
@@ -1771,6 +2131,35 @@ static void grid_rows_ws_shape(const GridCfg &c, const ConvArgs &a, dim3 g, cons
     else fail(GB_ERR_INTERNAL, "unsupported gridding region shape");
 }
 
+template <int CG, int RW, int RPW, bool D3>
+static void grid_rows_wsp_launch(const ConvArgs &a, const float2 *s, float2 *o, cudaStream_t st) {
+    auto kern = k_grid_rows_wsp<CG, RW, RPW, D3>;
+    const int smem = wsp_smem_bytes(a.k, CG);
+    // resident CTAs per SM for this shared-memory size (cached per instantiation)
+    static int cached_smem = -1, cached_ctas = 0;
+    if (smem != cached_smem) {
+        GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        int dev = 0, sms = 0, per_sm = 0;
+        GB_CUDA(cudaGetDevice(&dev));
+        GB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWsThreads, smem));
+        cached_ctas = std::max(1, per_sm) * sms;
+        cached_smem = smem;
+    }
+    const int ctas = std::max(1, std::min(a.n_work, cached_ctas));
+    kern<<<ctas, kWsThreads, smem, st>>>(a, s, o); ::gb::note_launch();
+}
+
+template <int CG, bool D3>
+static void grid_rows_wsp_shape(const GridCfg &c, const ConvArgs &a, const float2 *s, float2 *o, cudaStream_t st) {
+    if (c.rw == 4 && c.rpw == 1) grid_rows_wsp_launch<CG, 4, 1, D3>(a, s, o, st);
+    else if (c.rw == 4 && c.rpw == 2) grid_rows_wsp_launch<CG, 4, 2, D3>(a, s, o, st);
+    else if (c.rw == 4 && c.rpw == 4) grid_rows_wsp_launch<CG, 4, 4, D3>(a, s, o, st);
+    else if (c.rw == 8 && c.rpw == 1) grid_rows_wsp_launch<CG, 8, 1, D3>(a, s, o, st);
+    else if (c.rw == 8 && c.rpw == 2) grid_rows_wsp_launch<CG, 8, 2, D3>(a, s, o, st);
+    else fail(GB_ERR_INTERNAL, "unsupported gridding region shape");
+}
+
 template <int CG, bool D3>
 static void grid_rows_shape(const GridCfg &c, const ConvArgs &a, dim3 g, const float2 *s, float2 *o,
                             cudaStream_t st) {
@@ -1782,11 +2171,49 @@ static void grid_rows_shape(const GridCfg &c, const ConvArgs &a, dim3 g, const f
     else fail(GB_ERR_INTERNAL, "unsupported gridding region shape");
 }
 
+// How E^H E grids its own (tile-ordered) samples.
+//   SCHED_ROWS: k_grid_rows on the SORTED workspace, one CTA per work item;
+//   SCHED_WS:   k_grid_rows_ws on the interleaved workspace, one CTA per item;
+//   SCHED_WSP:  k_grid_rows_wsp on the interleaved workspace, one persistent
+//               launch over a work queue.
+// The per-item warp-specialized kernel wins when the launch is a few waves
+// deep: its 4-stage copy pipeline hides the staging latency that dominates a
+// short launch (CG-SENSE 256^2 x 16 coils: 1082 CTAs, 1.25 -> 1.19 ms per
+// recon).  On launches many waves deep the register-staged kernel's higher
+// occupancy (3 CTAs of 8 warps per SM against 2 of 8 + 1) beats it (64 uneven
+// frames x 12 coils: 42.0 against 45.5 ms per batch); the persistent kernel
+// takes those launches.
+enum GridSched { SCHED_ROWS = 0, SCHED_WS = 1, SCHED_WSP = 2 };
+constexpr int kWsMaxWaves = 8;
+
+static GridSched normal_grid_sched(const NufftPlan &p, const GridCfg &c) {
+    if (!c.rows) return SCHED_ROWS;
+    int sms = 0;
+    GB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device));
+    const int64_t ctas = (int64_t)p.n_grd_items * c.ncg;
+    const bool shallow = ctas <= (int64_t)kWsMaxWaves * kWsMinBlocks * sms;
+    const bool wsp_fits = (int64_t)wsp_smem_bytes(p.kp, c.cg) * kWsMinBlocks <= 220 * 1024;
+    switch (p.tiling.schedule) {
+        case 1: return shallow ? SCHED_WS : SCHED_ROWS;
+        case 2: return wsp_fits ? SCHED_WSP : (shallow ? SCHED_WS : SCHED_ROWS);
+        default: return shallow ? SCHED_WS : (wsp_fits ? SCHED_WSP : SCHED_ROWS);
+    }
+}
+
 // Launches the gridding kernel selected by `c` over all work items.
 static void grid_dispatch_cfg(const GridCfg &c, const NufftPlan &p, const ConvArgs &a, const float2 *samples,
                               float2 *grid, cudaStream_t st) {
     dim3 g(p.n_grd_items, c.ncg);
-    if (c.rows && a.layout == LAYOUT_SORTED_IL) {
+    if (c.rows && a.layout == LAYOUT_SORTED_IL && normal_grid_sched(p, c) == SCHED_WSP) {
+        const bool d3 = p.kp.D == 3;
+        if (c.cg == 16) {
+            if (d3) grid_rows_wsp_shape<16, true>(c, a, samples, grid, st);
+            else grid_rows_wsp_shape<16, false>(c, a, samples, grid, st);
+        } else {
+            if (d3) grid_rows_wsp_shape<8, true>(c, a, samples, grid, st);
+            else grid_rows_wsp_shape<8, false>(c, a, samples, grid, st);
+        }
+    } else if (c.rows && a.layout == LAYOUT_SORTED_IL) {
         const bool d3 = p.kp.D == 3;
         if (c.cg == 16) {
             if (d3) grid_rows_ws_shape<16, true>(c, a, g, samples, grid, st);
@@ -1828,6 +2255,7 @@ static void grid_dispatch_cfg(const GridCfg &c, const NufftPlan &p, const ConvAr
 // (must run outside stream capture).
 void launch_grid_prepare(NufftPlan &p, int nb, cudaStream_t st) {
     const GridCfg c = grid_config(p, nb);
+    if (p.grid_queue.ensure(2)) GB_CUDA(cudaMemsetAsync(p.grid_queue.get(), 0, 2 * sizeof(unsigned int), st));
     if (p.n_splits > 0) {
         const size_t need_ctr = (size_t)p.n_splits * c.ncg;
         if (p.split_counters.n < need_ctr || p.split_counter_groups == 0) {
@@ -1853,32 +2281,22 @@ void launch_grid(NufftPlan &p, const float2 *samples, float2 *grid, int nb, Samp
     a.splits = p.splits.get();
     a.ncg = c.ncg;
     a.part_elems = c.part_elems;
+    launch_grid_prepare(p, nb, st);
     if (p.n_splits > 0) {
-        launch_grid_prepare(p, nb, st);
         a.partials = p.partials.get();
         a.counters = p.split_counters.get();
     }
+    a.queue = p.grid_queue.get();
+    a.n_work = p.n_grd_items * c.ncg;
     if (p.n_grd_items == 0) return;
     grid_dispatch_cfg(c, p, a, samples, grid, st);
     launch_ref_fold_fix(p, a, samples, grid, st);
 }
 
-// The warp-specialized gridding (and so the interleaved workspace) wins when
-// the launch is a few waves deep: its 4-stage copy pipeline hides the
-// staging latency that dominates a short launch (CG-SENSE 256^2 x 16 coils:
-// 1082 CTAs, 1.25 -> 1.19 ms per recon).  On launches many waves deep the
-// register-staged kernel's higher occupancy (3 CTAs of 8 warps per SM against
-// 2 of 8 + 1) wins instead (64 uneven frames x 12 coils: 42.0 against 45.5 ms
-// per batch), so past kWsMaxWaves resident waves E^H E keeps SORTED.
-constexpr int kWsMaxWaves = 8;
-
+// The sample workspace layout of E^H E follows its gridding schedule.
 SampleLayout normal_op_layout(const NufftPlan &p, int nb) {
     const GridCfg c = grid_config(p, nb);
-    if (!c.rows) return LAYOUT_SORTED;
-    int sms = 0;
-    GB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device));
-    const int64_t ctas = (int64_t)p.n_grd_items * c.ncg;
-    return ctas <= (int64_t)kWsMaxWaves * kWsMinBlocks * sms ? LAYOUT_SORTED_IL : LAYOUT_SORTED;
+    return normal_grid_sched(p, c) == SCHED_ROWS ? LAYOUT_SORTED : LAYOUT_SORTED_IL;
 }
 
 // Scratch (split-tile partial tiles and their counters) that launch_grid

@@ -218,6 +218,7 @@ struct Tiling {
     int tile[kMaxD] = {16, 16, 1};
     int cg = 8;                 // coils per CTA (coil group)
     int split_len = 0;          // gridding list length above which a tile is split (0 = auto)
+    int schedule = 0;           // E^H E gridding: 0 auto, 1 one CTA per work item, 2 persistent work queue
 };
 
 struct NufftPlan {
@@ -266,6 +267,7 @@ struct NufftPlan {
     DevBuf<SplitInfo> splits;
     int n_splits = 0, n_slots = 0;
     DevBuf<unsigned int> split_counters;   // [n_splits * max coil groups]
+    DevBuf<unsigned int> grid_queue;       // persistent gridding: next unit, CTAs finished (zero between launches)
     int split_counter_groups = 0;
     DevBuf<float2> partials;               // [n_slots][cg_groups][cells*cg]
     int64_t total_pairs = 0;

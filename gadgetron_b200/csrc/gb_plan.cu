@@ -565,11 +565,11 @@ uint64_t plan_layout_signature(const NufftPlan &p, int nbf) {
         }
     };
     const void *ptrs[] = {p.pos_sorted.get(), p.wtab.get(), p.pair_rows.get(), p.perm.get(), p.grid_list.get(), p.grd_items.get(),
-                          p.deg_items.get(), p.splits.get(), p.partials.get(), p.split_counters.get(),
+                          p.deg_items.get(), p.splits.get(), p.partials.get(), p.split_counters.get(), p.grid_queue.get(),
                           p.img_os.get(), p.kgrid.get(), p.samp_ws.get(), p.deap_img.get(), p.deap_os.get()};
     for (const void *q : ptrs) mix((uint64_t)(uintptr_t)q);
     const int64_t vals[] = {p.n_deg_items, p.n_grd_items, p.n_splits, p.n_slots, p.Mtot, (int64_t)p.F,
-                            p.tiling.tile[0], p.tiling.tile[1], p.tiling.tile[2], p.tiling.cg,
+                            p.tiling.tile[0], p.tiling.tile[1], p.tiling.tile[2], p.tiling.cg, p.tiling.schedule,
                             p.split_counter_groups, (int64_t)p.split_counters.n, (int64_t)p.partials.n, nbf};
     for (int64_t v : vals) mix((uint64_t)v);
     auto it = p.fft_plans.find(nbf);

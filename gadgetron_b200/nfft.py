@@ -161,6 +161,16 @@ class cuNFFT_plan:
         t = (ctypes.c_int * 3)(*(list(tile) + [1] * (3 - len(tile))))
         check(lib.gb_nufft_set_tiling(self._h, t, int(coil_group)))
 
+    def set_grid_schedule(self, schedule: int):
+        """Gridding schedule of the normal operator: 0 by launch depth, 1 one
+        CTA per work item, 2 one persistent work-queue launch (same results)."""
+        check(lib.gb_nufft_set_grid_schedule(self._h, int(schedule)))
+
+    def get_grid_schedule(self) -> int:
+        v = ctypes.c_int()
+        check(lib.gb_nufft_get_grid_schedule(self._h, ctypes.byref(v)))
+        return v.value
+
     # -- NFFT_plan::preprocess (NFFT.h:67-68)
     def preprocess(self, trajectory: torch.Tensor, mode: NFFT_prep_mode = NFFT_prep_mode.ALL,
                    num_frames: int = 1, frame_offsets: Optional[Sequence[int]] = None):

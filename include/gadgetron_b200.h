@@ -238,6 +238,15 @@ GB_API gb_status gb_nufft_time_normal_convolutions(gb_nufft_plan plan, uint32_t 
 GB_API gb_status gb_nufft_get_tiling(gb_nufft_plan plan, int *tile, int *coil_group);
 GB_API gb_status gb_nufft_set_tiling(gb_nufft_plan plan, const int *tile, int coil_group);
 
+/* How the normal operator (mult_MH_M, the CG-SENSE iteration) grids its own
+ * tile-ordered samples: 0 (default) chooses by launch depth; 1 one CTA per
+ * gridding work item; 2 one persistent launch whose CTAs take (frame, tile,
+ * coil group) work units from a device-side queue.  Results are the same
+ * bit for bit; only the speed differs.  Takes effect at the next launch (a
+ * captured CG graph is re-captured).  No reference counterpart (tuning). */
+GB_API gb_status gb_nufft_set_grid_schedule(gb_nufft_plan plan, int schedule);
+GB_API gb_status gb_nufft_get_grid_schedule(gb_nufft_plan plan, int *schedule);
+
 /* ------------------------------------------------------------------ SENSE */
 
 /* Replaces cuNonCartesianSenseOperator<float,D>(ConvolutionType) + setup(

@@ -171,13 +171,14 @@ def test_traj_grad_fd_3d_alpha_1_5_w4():
     assert err <= FD_TOL, err
 
 
-def test_batched_many_frames_register_staged_path():
+def test_batched_many_frames_deep_launch_schedules():
     """48 uneven frames of 64^2 (mos 128, 64 tiles a frame): the gridding
-    launch of E^H E is more than 8 resident waves deep, which selects the
-    register-staged gridding over the plan's sorted sample layout (small
-    launches take the warp-specialized kernel over the interleaved layout,
-    covered by every other CG test).  Frame-independent CG against one
-    oracle solve per frame."""
+    launch of E^H E is more than 8 resident waves deep.  Schedule 1 takes the
+    register-staged gridding over the plan's sorted sample layout, schedule 2
+    (and the default) the persistent work-queue kernel over the interleaved
+    layout (small launches take the per-item warp-specialized kernel,
+    covered by every other CG test).  Both give the same images bit for bit;
+    frame-independent CG against one oracle solve per frame."""
     dev = torch.device("cuda:0")
     N, mos, W, C, F, iters = 64, 128, 5.5, 8, 48, 6
     spokes = [4 + (f * 5) % 9 for f in range(F)]
@@ -208,10 +209,17 @@ def test_batched_many_frames_register_staged_path():
     cg.set_max_iterations(iters)
     cg.set_tc_tolerance(0.0)
     cg.set_frame_independent(True)
-    for use_graph in (False, True):
-        cg.set_use_graph(use_graph)
-        xb = cg.solve(torch.from_numpy(d).to(dev)).cpu().numpy()
-        for f in range(0, F, 7):
-            xr = O.cg_solve(ops[f], d[:, offs[f]:offs[f + 1]][:, None, :], iterations=iters, tc_tolerance=0.0)
-            assert rel_l2(xb[f], xr[0]) <= CG_TOL, (use_graph, f)
+    refs = {f: O.cg_solve(ops[f], d[:, offs[f]:offs[f + 1]][:, None, :], iterations=iters, tc_tolerance=0.0)
+            for f in range(0, F, 7)}
+    sols = {}
+    for sched in (1, 2):
+        E.get_plan().set_grid_schedule(sched)
+        for use_graph in (False, True):
+            cg.set_use_graph(use_graph)
+            xb = cg.solve(torch.from_numpy(d).to(dev)).cpu().numpy()
+            sols[(sched, use_graph)] = xb
+            for f, xr in refs.items():
+                assert rel_l2(xb[f], xr[0]) <= CG_TOL, (sched, use_graph, f)
+    assert np.array_equal(sols[(1, True)], sols[(2, True)])
+    assert np.array_equal(sols[(1, False)], sols[(2, False)])
     assert E.get_plan().device_errors() == 0
