@@ -565,7 +565,7 @@ struct TailArgs {
     CgGlobal *G;
     double2 *part1, *part2;  // [nseg][gridDim.x]
     double *hist;
-    unsigned int *bar;       // grid barrier: arrival count, generation
+    unsigned int *bar;       // per segment: barrier arrival count, generation
     unsigned int *err;
     uint32_t spin_limit;     // polls of a barrier wait before giving up
     float2 *pad;             // next iteration's padded image (outer-major), or null after the last iteration
@@ -573,8 +573,9 @@ struct TailArgs {
     int seg_rows;            // image rows (of N0 pixels) per segment
 };
 
-// Grid-wide barrier for a cooperative launch (all blocks resident).  The
-// wait is bounded: after spin_limit polls (2^26 by default, about 4 s) the
+// Barrier of the nblocks blocks of one segment (a cooperative launch: all
+// blocks resident; segments share nothing, so each has its own counters).
+// The wait is bounded: after spin_limit polls (2^26 by default, about 4 s) the
 // block records the failure in bit 1 of *err and goes on.  Past such a
 // timeout the barrier counters no longer match the launch's phases, so the
 // host clears them before every solve, and the solve's values are void (the
@@ -622,11 +623,18 @@ __device__ double2 tail_segment_sum(const double2 *part, int nparts, double2 *sh
     return tot;
 }
 
-__global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
+// TPP threads share a pixel in the coil sums of phases 1 and 3 (coils b = sub,
+// sub + TPP, ...; the partial sums are combined by a shuffle): each thread's
+// loads are then one round of TPP-times fewer coils, which halves the
+// dependent-latency chain of a short tail (one image row per block).  Blocks
+// are 256 * TPP threads.
+template <int TPP>
+__global__ void __launch_bounds__(256 * TPP, 4 / TPP) k_cg_tail(TailArgs t) {
     __shared__ double2 sh[32];
     const KParams &k = t.k;
     const int seg = blockIdx.y, nbx = gridDim.x;
-    const unsigned int nblocks = gridDim.x * gridDim.y;
+    const unsigned int nblocks = gridDim.x;   // blocks of this segment
+    unsigned int *bar = t.bar + 2 * seg;
     CgSeg &S = t.segs[seg];
     const bool was_done = S.done != 0;
     const double rq = S.rq, rq0 = S.rq0;
@@ -647,11 +655,18 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
     const int my_rows = (int)blockIdx.x < t.seg_rows ? (t.seg_rows - 1 - (int)blockIdx.x) / nbx + 1 : 0;
     const int my_elems = my_rows * n0;
 
+    const int sub = (int)threadIdx.x % TPP;                           // coil phase of this thread
+    const int px0 = (int)threadIdx.x / TPP, pxs = (int)blockDim.x / TPP;   // pixel lane, pixels per pass
+
     // Phase 1: q = weight * crop(kg) * conj(csm) summed + kappa p ; <p, q>.
+    // (The pass loop is uniform across the block so that the TPP threads of a
+    // pixel meet at the shuffle.)
     double2 acc = make_double2(0.0, 0.0);
     if (!was_done) {
-        for (int l = threadIdx.x; l < my_elems; l += blockDim.x) {
-            const int i = l / n0, x = l - i * n0;
+        for (int l0 = 0; l0 < my_elems; l0 += pxs) {
+            const int l = l0 + px0;
+            const bool ok = l < my_elems;
+            const int i = ok ? l / n0 : 0, x = ok ? l - i * n0 : 0;
             const int rr = (int)blockIdx.x + i * nbx;
             int f, z, y, rem;
             row_coords(row0 + rr, f, z, y, rem);
@@ -662,21 +677,27 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
             const int64_t grow = (int64_t)gz * t.kl.s_z + (int64_t)gy * t.kl.s_y + ox;
             const int64_t nrow = (int64_t)rem * n0;
             const int64_t erow = (int64_t)(row0 + rr) * n0;
-            {
-                const int gx = x + ox;
-                float fac = t.deap[x] * fyz;
-                if ((gx + gy + gz) & 1) fac = -fac;
-                fac *= t.scale * t.weight;
-                const int64_t g = grow + x, n = nrow + x, e = erow + x;
-                float2 s = make_float2(0.f, 0.f);
+            const int gx = x + ox;
+            float fac = t.deap[x] * fyz;
+            if ((gx + gy + gz) & 1) fac = -fac;
+            fac *= t.scale * t.weight;
+            const int64_t g = grow + x, n = nrow + x, e = erow + x;
+            float2 s = make_float2(0.f, 0.f);
+            if (ok) {
 #pragma unroll 8
-                for (int b = 0; b < t.nb; b++) {
+                for (int b = sub; b < t.nb; b += TPP) {
                     const float2 v = t.kg[((int64_t)b * t.F + f) * t.kl.s_bf + g];
                     const float2 c = t.csm[(int64_t)b * k.NN + n];
                     const float vr = v.x * fac, vi = v.y * fac;
                     s.x += vr * c.x + vi * c.y;
                     s.y += vi * c.x - vr * c.y;
                 }
+            }
+            if (TPP == 2) {
+                s.x += __shfl_xor_sync(0xffffffffu, s.x, 1);
+                s.y += __shfl_xor_sync(0xffffffffu, s.y, 1);
+            }
+            if (ok && sub == 0) {
                 const float2 pv = t.p[e];
                 const float2 rp = reg_term(pv, t.reg, e);
                 s.x += t.kappa * rp.x;
@@ -689,7 +710,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
     }
     acc = block_reduce_d2(acc, sh);
     if (threadIdx.x == 0) t.part1[(size_t)seg * nbx + blockIdx.x] = acc;
-    tail_grid_barrier(t.bar, nblocks, t.err, t.spin_limit);
+    tail_grid_barrier(bar, nblocks, t.err, t.spin_limit);
 
     // Phase 2: alpha = rq / <p,q> ; x += alpha p ; r -= alpha q ; <r, P^2 r>.
     const double2 pq = tail_segment_sum(t.part1 + (size_t)seg * nbx, nbx, sh);
@@ -721,7 +742,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
     }
     acc = block_reduce_d2(acc, sh);
     if (threadIdx.x == 0) t.part2[(size_t)seg * nbx + blockIdx.x] = acc;
-    tail_grid_barrier(t.bar, nblocks, t.err, t.spin_limit);
+    tail_grid_barrier(bar, nblocks, t.err, t.spin_limit);
 
     // Phase 3: segment scalars, stop rule, history; then the direction update
     // p = beta p + P^2 r and the forward pad of p for the next iteration.
@@ -767,7 +788,9 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
     const int gx0 = t.pad_full ? 0 : ox, gx1 = t.pad_full ? k.mos[0] : ox + n0;
     const int w3 = gx1 - gx0;
     const int my_pad = my_rows * w3;
-    for (int l = threadIdx.x; l < my_pad; l += blockDim.x) {
+    for (int l0 = 0; l0 < my_pad; l0 += pxs) {   // uniform across the block (the __syncwarp below)
+        const bool ok = l0 + px0 < my_pad;
+        const int l = ok ? l0 + px0 : 0;
         const int i = l / w3;
         const int rr = (int)blockIdx.x + i * nbx;
         int f, z, y, rem;
@@ -782,24 +805,25 @@ __global__ void __launch_bounds__(256, 4) k_cg_tail(TailArgs t) {
         {
             const int gx = gx0 + (l - i * w3);
             const int x = gx - ox;
-            const bool in = x >= 0 && x < k.N[0];
+            const bool in = ok && x >= 0 && x < k.N[0];
             float fac = 0.f;
             float2 v = make_float2(0.f, 0.f);
+            const int64_t e = erow + x;
             if (in) {
-                const int64_t e = erow + x;
                 v = t.p[e];
                 if (!done_now) {
                     float2 rv = t.r[e];
                     if (t.P) { const float w = t.P[e]; const float w2 = w * w; rv.x *= w2; rv.y *= w2; }
                     v = make_float2(beta * v.x + rv.x, beta * v.y + rv.y);
-                    t.p[e] = v;
                 }
                 fac = t.deap[x] * fyz;
                 if ((gx + gy + gz) & 1) fac = -fac;
             }
+            __syncwarp();   // the pixel's other threads have read p
+            if (in && !done_now && sub == 0) t.p[e] = v;
             const int64_t g = gline + gx, n = nrow + x;
 #pragma unroll 8
-            for (int b = 0; b < t.nb; b++) {
+            for (int b = sub; b < t.nb && ok; b += TPP) {
                 const float2 c = in ? cmul2(v, t.csm[(int64_t)b * k.NN + n]) : make_float2(0.f, 0.f);
                 t.pad[((int64_t)b * t.F + f) * t.kl.s_bf + g] = make_float2(c.x * fac, c.y * fac);
             }
@@ -988,7 +1012,10 @@ static void cg_iteration_fused(CgSolver &cg, cudaStream_t st, double *hist, bool
     ta.pad_full = fft_custom_ok(p) ? 0 : 1;
     ta.seg_rows = (int)(cg.seg_len / p.kp.N[0]);
     void *args[] = {&ta};
-    GB_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg_tail, cg.tail_grid, dim3(256), args, 0, st));
+    if (cg.tail_tpp == 2)
+        GB_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg_tail<2>, cg.tail_grid, dim3(512), args, 0, st));
+    else
+        GB_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg_tail<1>, cg.tail_grid, dim3(256), args, 0, st));
     ::gb::note_launch();
 }
 
@@ -1042,16 +1069,27 @@ static void cg_prepare(CgSolver &cg, cudaStream_t st) {
     const dim3 sg = seg_grid(cg);
     cg.partials.ensure((size_t)sg.x * sg.y);
     cg.partials2.ensure((size_t)sg.x * sg.y);
-    if (cg.tail_bar.ensure(2)) GB_CUDA(cudaMemsetAsync(cg.tail_bar.get(), 0, 2 * sizeof(unsigned int), st));
-    // The fused iteration tail needs the outer-major pad buffer (D >= 2) and
-    // all of its blocks resident at once (cooperative launch).
+    if (cg.tail_bar.ensure(2 * (size_t)cg.nseg))
+        GB_CUDA(cudaMemsetAsync(cg.tail_bar.get(), 0, cg.tail_bar.n * sizeof(unsigned int), st));
+    // The fused iteration tail needs D >= 2 and all of its blocks resident at
+    // once (cooperative launch).
     cg.use_tail = false;
     if (p.D >= 2 && cg.seg_len % p.kp.N[0] == 0) {
         int dev = 0, coop = 0, nsm = 0, per_sm = 0;
         GB_CUDA(cudaGetDevice(&dev));
         GB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
         GB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_tail, 256, 0));
+        // Two threads per pixel when every block holds at most one image row
+        // (a short tail whose time is its latency chain); one otherwise (long
+        // tails keep the larger number of resident blocks per segment).
+        int per2 = 0;
+        GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_cg_tail<2>, 512, 0));
+        const int64_t rows = (cg.seg_len / p.kp.N[0]) * cg.nseg;
+        cg.tail_tpp = (nb >= 8 && rows <= (int64_t)per2 * nsm) ? 2 : 1;
+        if (cg.tail_tpp == 2)
+            per_sm = per2;
+        else
+            GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_tail<1>, 256, 0));
         // blocks per segment: up to the resident capacity, at most one per image row
         const int64_t cap = (int64_t)per_sm * nsm;
         const int64_t seg_rows = cg.seg_len / p.kp.N[0];
@@ -1085,7 +1123,7 @@ static void cg_record(CgSolver &cg, const float2 *d, float2 *x_out, double *hist
     const int64_t n = (int64_t)p.F * p.kp.NN;
     // A grid barrier that timed out in an earlier solve leaves its counters
     // out of step: start every solve from cleared ones.
-    if (cg.use_tail) GB_CUDA(cudaMemsetAsync(cg.tail_bar.get(), 0, 2 * sizeof(unsigned int), st));
+    if (cg.use_tail) GB_CUDA(cudaMemsetAsync(cg.tail_bar.get(), 0, 2 * (size_t)cg.nseg * sizeof(unsigned int), st));
     // rhs0 = weight * E^H d
     nufft_adjoint(p, d, LAYOUT_ORIGINAL, s.dcw, s.csm, s.ncoils, cg.rhs0.get(), false, false, cg.weight,
                   CUFFT_INVERSE, st);

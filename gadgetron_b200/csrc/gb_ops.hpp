@@ -63,6 +63,7 @@ struct CgSolver {
     DevBuf<float2> x, r, p, q, rhs0, rhs;
     DevBuf<double2> x64, partials, partials2;
     DevBuf<unsigned int> tail_bar;   // grid barrier of the fused iteration tail
+    int tail_tpp = 1;                // threads per pixel of the tail's coil sums
     bool use_tail = false;           // fused tail (cooperative launch) available for this shape
     dim3 tail_grid;                  // its launch grid (blocks per segment, segments)
     DevBuf<CgSeg> segs;
