@@ -1785,118 +1785,59 @@ k_degrid_c2nc(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ 
 // weights beyond the footprint; 3D slices predicated on the sample's z
 // count), so the inner loop is loads and FMAs only.  NT = the largest tap count a
 // footprint can have (2*ceil(W/2), plus one when W is an even integer).
+// Per-sample inputs of one pass of the table degridding (loaded a pass ahead).
+struct DegRaw {
+    float sp[3];
+    float4 t0[3], t1[3];
+    uint32_t j;
+    float dw;
+};
+
 template <int CG, int NT, bool D3>
-__global__ void __launch_bounds__(kThreads, D3 ? 2 : 3)
-k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ out) {
+__device__ __forceinline__ void degrid_table_load_raw(const ConvArgs &a, const WorkItem &it, int bs, DegRaw &r) {
+    using Sh = DegridShape<CG>;
+    constexpr int LPS = Sh::LPS, SPW = Sh::SPW;
+    constexpr int D = D3 ? 3 : 2;
+    const int lane = threadIdx.x & 31;
+    const int sl = lane / LPS;
+    const bool lane_ok = sl < SPW;   // false only for the 2 spare lanes of coil group 12
+    const int i = bs + sl;
+    const bool valid = lane_ok && i < it.end;
+    const int ic = valid ? i : it.begin;   // a valid row for the loads of idle lanes
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+        r.sp[d] = a.pos[(int64_t)d * a.Mtot + ic];
+        const float4 *trow = reinterpret_cast<const float4 *>(a.wtab + ((int64_t)ic * D + d) * kWMax);
+        r.t0[d] = __ldg(trow);
+        r.t1[d] = NT > 4 ? __ldg(trow + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    const bool need_j = a.layout == LAYOUT_ORIGINAL || a.dcw;
+    r.j = need_j ? a.perm[ic] : (uint32_t)ic;
+    r.dw = a.dcw ? a.dcw[r.j] : 1.f;
+}
+
+// The sample passes of one degridding work item over its staged region
+// (tile_s: the tile plus halo, cell stride CS, zero pad after it); `cur` holds
+// the first pass's inputs of this warp.
+template <int CG, int NT, bool D3>
+__device__ __forceinline__ void degrid_table_passes(const ConvArgs &a, const WorkItem &it, int b0, int org0,
+                                                    int org1, int org2, const float2 *tile_s,
+                                                    float2 *__restrict__ out, DegRaw cur) {
     using Sh = DegridShape<CG>;
     constexpr int CPL = Sh::CPL, LPS = Sh::LPS, SPW = Sh::SPW;
     constexpr int D = D3 ? 3 : 2;
-    // Staged cell stride in float2.  2D: padded to an odd number of 16-byte
-    // chunks (conflict-free staging stores; the region copy is a large share
-    // of a 2D item's work).  3D: unpadded (the copy is a few percent of an
-    // item's work there and the region is large).
     constexpr int CS = D3 ? CG : CG + 2;
-    static_assert(CG >= 4, "table degridding stages coil pairs");
-    extern __shared__ float4 smem_raw[];
     const KParams &k = a.k;
-    const WorkItem it = a.items[blockIdx.x];
-    const int grp = blockIdx.y;
-    const int b0 = grp * CG;
-    const int f = it.ft / k.ntiles_total;
-    const int tile = it.ft - f * k.ntiles_total;
-    const int tx = tile % k.ntiles[0];
-    const int ty = (tile / k.ntiles[0]) % k.ntiles[1];
-    const int tz = tile / (k.ntiles[0] * k.ntiles[1]);
-    const int org0 = tx * k.tile[0], org1 = ty * k.tile[1], org2 = tz * k.tile[2];
     const int R0 = region_dim(k, 0), R1 = region_dim(k, 1), R2 = region_dim(k, 2);
-    const int h2 = D3 ? k.hw : 0;
-    float2 *tile_s = reinterpret_cast<float2 *>(smem_raw);
-
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int sl = lane / LPS, ll = lane % LPS;
-
-    // Per-sample inputs of one pass, loaded a pass ahead (the first pass's
-    // loads overlap the region copy).
-    struct Raw {
-        float sp[3];
-        float4 t0[3], t1[3];
-        uint32_t j;
-        float dw;
-    };
-    const bool lane_ok = sl < SPW;   // false only for the 2 spare lanes of coil group 12
-    auto load_raw = [&](int bs, Raw &r) {
-        const int i = bs + sl;
-        const bool valid = lane_ok && i < it.end;
-        const int ic = valid ? i : it.begin;   // a valid row for the loads of idle lanes
-#pragma unroll
-        for (int d = 0; d < D; d++) {
-            r.sp[d] = a.pos[(int64_t)d * a.Mtot + ic];
-            const float4 *trow = reinterpret_cast<const float4 *>(a.wtab + ((int64_t)ic * D + d) * kWMax);
-            r.t0[d] = __ldg(trow);
-            r.t1[d] = NT > 4 ? __ldg(trow + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        const bool need_j = a.layout == LAYOUT_ORIGINAL || a.dcw;
-        r.j = need_j ? a.perm[ic] : (uint32_t)ic;
-        r.dw = a.dcw ? a.dcw[r.j] : 1.f;
-    };
-    Raw cur, nxt;
+    const bool lane_ok = sl < SPW;
+    DegRaw nxt;
     int base = it.begin + warp * SPW;
-    if (base < it.end) load_raw(base, cur);
-    {
-        // Region staging through registers.  Thread e of the CTA takes cells
-        // e, e + kThreads, ... of the region in x-fastest order (every load
-        // instruction is a coalesced run of one coil plane, no idle lanes at
-        // row ends), loads all CG coils of UC cells before storing any (the
-        // loads in flight cover the memory latency), then stores each cell's
-        // coils as 16-byte chunks (with padded cells, the chunks that a warp
-        // stores at once fall into different banks).
-        constexpr int UC = CG <= 4 ? 2 : 1;   // cells in flight per thread
-        const int ncell = R0 * R1 * R2;
-        const int gx0 = org0 - k.hw, gy0 = org1 - k.hw, gz0 = org2 - h2;
-        const int64_t pstride = (int64_t)a.F * a.kl.s_bf;
-        const float2 *fbase = grid + (int64_t)b0 * pstride + (int64_t)f * a.kl.s_bf;
-        for (int e0 = threadIdx.x; e0 < ncell; e0 += UC * kThreads) {
-            float2 v[UC][CG];
-#pragma unroll
-            for (int u = 0; u < UC; u++) {
-                const int e = e0 + u * kThreads;
-                const int row = e / R0, xo = e - row * R0;
-                const int rz = row / R1, ry = row - rz * R1;
-                int gx = gx0 + xo, gy = gy0 + ry, gz = gz0 + rz;
-                gx = gx < 0 ? gx + k.mos[0] : (gx >= k.mos[0] ? gx - k.mos[0] : gx);
-                gy = gy < 0 ? gy + k.mos[1] : (gy >= k.mos[1] ? gy - k.mos[1] : gy);
-                gz = gz < 0 ? gz + k.mos[2] : (gz >= k.mos[2] ? gz - k.mos[2] : gz);
-                const float2 *src = fbase + (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y + gx;
-                const bool in = e < ncell;
-#pragma unroll
-                for (int c = 0; c < CG; c++)
-                    v[u][c] = (in && b0 + c < a.nb) ? __ldg(src + c * pstride) : make_float2(0.f, 0.f);
-            }
-#pragma unroll
-            for (int u = 0; u < UC; u++) {
-                const int e = e0 + u * kThreads;
-                if (e < ncell) {
-                    float4 *cell = reinterpret_cast<float4 *>(tile_s + (size_t)e * CS);
-#pragma unroll
-                    for (int q = 0; q < CG / 2; q++)
-                        cell[q] = make_float4(v[u][2 * q].x, v[u][2 * q].y, v[u][2 * q + 1].x, v[u][2 * q + 1].y);
-                }
-            }
-        }
-        {
-            // zero pad after the region: a tap with zero weight beyond the
-            // footprint may read up to one row and one cell past it
-            const int npad = (R0 + 1) * CS;
-            for (int e = threadIdx.x; e < npad; e += kThreads)
-                tile_s[(size_t)R0 * R1 * R2 * CS + e] = make_float2(0.f, 0.f);
-        }
-    }
-    __syncthreads();
-
     for (; base < it.end; base += 8 * SPW) {
         const int i = base + sl;
         const bool valid = lane_ok && i < it.end;
-        if (base + 8 * SPW < it.end) load_raw(base + 8 * SPW, nxt);
+        if (base + 8 * SPW < it.end) degrid_table_load_raw<CG, NT, D3>(a, it, base + 8 * SPW, nxt);
         int rs[3] = {0, 0, 0}, n[3] = {1, 1, 1};
         float w[3][NT];
 #pragma unroll
@@ -1998,6 +1939,89 @@ k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__
         }
         cur = nxt;
     }
+}
+
+template <int CG, int NT, bool D3>
+__global__ void __launch_bounds__(kThreads, D3 ? 2 : 3)
+k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ out) {
+    constexpr int SPW = DegridShape<CG>::SPW;
+    // Staged cell stride in float2.  2D: padded to an odd number of 16-byte
+    // chunks (conflict-free staging stores; the region copy is a large share
+    // of a 2D item's work).  3D: unpadded (the copy is a few percent of an
+    // item's work there and the region is large).
+    constexpr int CS = D3 ? CG : CG + 2;
+    static_assert(CG >= 4, "table degridding stages coil pairs");
+    extern __shared__ float4 smem_raw[];
+    const KParams &k = a.k;
+    const WorkItem it = a.items[blockIdx.x];
+    const int grp = blockIdx.y;
+    const int b0 = grp * CG;
+    const int f = it.ft / k.ntiles_total;
+    const int tile = it.ft - f * k.ntiles_total;
+    const int tx = tile % k.ntiles[0];
+    const int ty = (tile / k.ntiles[0]) % k.ntiles[1];
+    const int tz = tile / (k.ntiles[0] * k.ntiles[1]);
+    const int org0 = tx * k.tile[0], org1 = ty * k.tile[1], org2 = tz * k.tile[2];
+    const int R0 = region_dim(k, 0), R1 = region_dim(k, 1), R2 = region_dim(k, 2);
+    const int h2 = D3 ? k.hw : 0;
+    float2 *tile_s = reinterpret_cast<float2 *>(smem_raw);
+
+    const int warp = threadIdx.x >> 5;
+
+    DegRaw cur;
+    int base = it.begin + warp * SPW;
+    if (base < it.end) degrid_table_load_raw<CG, NT, D3>(a, it, base, cur);
+    {
+        // Region staging through registers.  Thread e of the CTA takes cells
+        // e, e + kThreads, ... of the region in x-fastest order (every load
+        // instruction is a coalesced run of one coil plane, no idle lanes at
+        // row ends), loads all CG coils of UC cells before storing any (the
+        // loads in flight cover the memory latency), then stores each cell's
+        // coils as 16-byte chunks (with padded cells, the chunks that a warp
+        // stores at once fall into different banks).
+        constexpr int UC = CG <= 4 ? 2 : 1;   // cells in flight per thread
+        const int ncell = R0 * R1 * R2;
+        const int gx0 = org0 - k.hw, gy0 = org1 - k.hw, gz0 = org2 - h2;
+        const int64_t pstride = (int64_t)a.F * a.kl.s_bf;
+        const float2 *fbase = grid + (int64_t)b0 * pstride + (int64_t)f * a.kl.s_bf;
+        for (int e0 = threadIdx.x; e0 < ncell; e0 += UC * kThreads) {
+            float2 v[UC][CG];
+#pragma unroll
+            for (int u = 0; u < UC; u++) {
+                const int e = e0 + u * kThreads;
+                const int row = e / R0, xo = e - row * R0;
+                const int rz = row / R1, ry = row - rz * R1;
+                int gx = gx0 + xo, gy = gy0 + ry, gz = gz0 + rz;
+                gx = gx < 0 ? gx + k.mos[0] : (gx >= k.mos[0] ? gx - k.mos[0] : gx);
+                gy = gy < 0 ? gy + k.mos[1] : (gy >= k.mos[1] ? gy - k.mos[1] : gy);
+                gz = gz < 0 ? gz + k.mos[2] : (gz >= k.mos[2] ? gz - k.mos[2] : gz);
+                const float2 *src = fbase + (int64_t)gz * a.kl.s_z + (int64_t)gy * a.kl.s_y + gx;
+                const bool in = e < ncell;
+#pragma unroll
+                for (int c = 0; c < CG; c++)
+                    v[u][c] = (in && b0 + c < a.nb) ? __ldg(src + c * pstride) : make_float2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < UC; u++) {
+                const int e = e0 + u * kThreads;
+                if (e < ncell) {
+                    float4 *cell = reinterpret_cast<float4 *>(tile_s + (size_t)e * CS);
+#pragma unroll
+                    for (int q = 0; q < CG / 2; q++)
+                        cell[q] = make_float4(v[u][2 * q].x, v[u][2 * q].y, v[u][2 * q + 1].x, v[u][2 * q + 1].y);
+                }
+            }
+        }
+        {
+            // zero pad after the region: a tap with zero weight beyond the
+            // footprint may read up to one row and one cell past it
+            const int npad = (R0 + 1) * CS;
+            for (int e = threadIdx.x; e < npad; e += kThreads)
+                tile_s[(size_t)R0 * R1 * R2 * CS + e] = make_float2(0.f, 0.f);
+        }
+    }
+    __syncthreads();
+    degrid_table_passes<CG, NT, D3>(a, it, b0, org0, org1, org2, tile_s, out, cur);
 }
 
 __global__ void k_sum_groups(const float *__restrict__ part, int ngroups, int64_t n,

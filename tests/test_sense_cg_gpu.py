@@ -180,9 +180,10 @@ def test_batched_uneven_frames_equal_per_frame_solves(cuda):
 def test_grid_schedules_bit_identical(cuda):
     """The normal operator's gridding schedules -- one CTA per work item
     (schedule 1; here the warp-specialized kernel on the interleaved sample
-    layout) and one persistent work-queue launch (schedule 2) -- give E^H E
-    and CG results equal bit for bit, on uneven frames whose dense radial
-    centres are split over several work items, and match the oracle."""
+    layout) and one persistent work-queue launch (schedule 2) -- give
+    forward, E^H E and CG results equal bit for bit, on uneven frames whose
+    dense radial centres are split over several work items, and match the
+    oracle."""
     N, mos, W, C = 32, 64, 5.5, 12
     spokes = [64, 7, 13, 40, 5]
     trajs = [S.radial_golden_angle_2d(s, 64, profile_offset=11 * f) for f, s in enumerate(spokes)]
@@ -202,10 +203,13 @@ def test_grid_schedules_bit_identical(cuda):
     xt = torch.from_numpy(x).to(cuda)
     d = torch.empty((C, offs[-1]), dtype=torch.complex64, device=cuda)
     E.mult_M(xt, d)
-    outs, sols = {}, {}
+    outs, sols, fwd = {}, {}, {}
     for sched in (1, 2, 0):
         plan.set_grid_schedule(sched)
         assert plan.get_grid_schedule() == sched
+        y = torch.empty_like(d)
+        E.mult_M(xt, y)
+        fwd[sched] = y.cpu().numpy()
         o = torch.empty_like(xt)
         E.mult_MH_M(xt, o)
         outs[sched] = o.cpu().numpy()
@@ -216,6 +220,7 @@ def test_grid_schedules_bit_identical(cuda):
         cg.set_frame_independent(True)
         cg.set_use_graph(True)
         sols[sched] = cg.solve(d).cpu().numpy()
+    assert np.array_equal(fwd[1], fwd[2]) and np.array_equal(fwd[0], fwd[1])
     assert np.array_equal(outs[1], outs[2]) and np.array_equal(outs[0], outs[1])
     assert np.array_equal(sols[1], sols[2]) and np.array_equal(sols[0], sols[1])
     for f in (0, 3):
