@@ -114,6 +114,7 @@ def _load():
         "gb_cg_set_use_graph": (i32, [P, i32]),
         "gb_cg_set_frame_independent": (i32, [P, i32]),
         "gb_cg_set_barrier_spin_limit": (i32, [P, u32]),
+        "gb_cg_set_row_fusion": (i32, [P, i32]),
         "gb_cg_solve": (i32, [P, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
@@ -133,7 +134,7 @@ EXPORTED = (
     "gb_sense_set_dcw gb_sense_mult_M gb_sense_mult_MH gb_sense_mult_MH_M gb_sense_get_nufft_plan gb_sense_autotune "
     "gb_cg_create gb_cg_destroy gb_cg_set_encoding_operator gb_cg_set_max_iterations "
     "gb_cg_set_tc_tolerance gb_cg_set_x0 gb_cg_set_preconditioner gb_cg_set_identity_regularization "
-    "gb_cg_set_refinements gb_cg_set_use_graph gb_cg_set_frame_independent gb_cg_set_barrier_spin_limit gb_cg_solve "
+    "gb_cg_set_refinements gb_cg_set_use_graph gb_cg_set_frame_independent gb_cg_set_barrier_spin_limit gb_cg_set_row_fusion gb_cg_solve "
     "gb_cg_set_image_regularization gb_image_operator_compute gb_sense_precond_weights "
     "gb_radial_trajectory_golden_ratio_2d gb_radial_trajectory_fixed_angle_2d gb_radial_trajectory_variable_angle_2d "
     "gb_radial_dcw_golden_ratio_2d gb_radial_dcw_fixed_angle_2d gb_sdc_estimate_dcw "

@@ -674,6 +674,13 @@ GB_API gb_status gb_cg_set_barrier_spin_limit(gb_cg_solver solver, uint32_t spin
     });
 }
 
+GB_API gb_status gb_cg_set_row_fusion(gb_cg_solver solver, int enable) {
+    return guarded([&] {
+        if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");
+        solver->c.row_fusion = enable != 0;
+    });
+}
+
 GB_API gb_status gb_cg_set_frame_independent(gb_cg_solver solver, int independent) {
     return guarded([&] {
         if (!solver) fail(GB_ERR_INVALID_ARGUMENT, "NULL solver");

@@ -318,6 +318,9 @@ int64_t fft_band_offset(const NufftPlan &p, int nbf);
 // (row_off + r % rpp) * n).  Input points outside [in_lo, in_hi) are taken as
 // zero without being read; only points in [out_lo, out_hi) are written.
 bool fft_custom_ok(const NufftPlan &p);
+// W_N^e, e < N, for the project FFT passes of length n (created on first use,
+// outside any stream capture; synchronises then).
+const float2 *fft_twiddles(NufftPlan &p, int n, cudaStream_t st);
 void fft_custom_prepare(NufftPlan &p, cudaStream_t st);
 void fft_cols(NufftPlan &p, int n, const float2 *in, float2 *out, int64_t ncols, int64_t cpp, int64_t pstride,
               int64_t ostride, int in_lo, int in_hi, int out_lo, int out_hi, bool inverse, cudaStream_t st);

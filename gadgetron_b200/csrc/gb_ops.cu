@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "gb_dft.cuh"
 #include "gb_internal.cuh"
 #include "gb_ops.hpp"
 
@@ -848,6 +849,233 @@ __global__ void __launch_bounds__(256 * TPP, 4 / TPP) k_cg_tail(TailArgs t) {
     }
 }
 
+// ----------------------------------- CG with the row passes fused (2D) ---
+//
+// 2D plans under the project FFT passes run the CG iteration as seven plain
+// launches with no grid barrier: the x (row) pass of each FFT direction is
+// fused with what the iteration does next to it.
+//   k_rows_pad       p = beta p + P^2 r (segments still running; beta from the
+//                    previous iteration's k_cg_update), then per coil the
+//                    interior row p x csm x deapodization x checkerboard x
+//                    1/sqrt(G) transformed in place of the row pass's input --
+//                    the padded image never goes through HBM;
+//   (y pass, degridding, gridding, adjoint y pass: as in the other paths)
+//   k_rows_crop_dot  per image row, every coil's band row transformed back,
+//                    cropped in shared memory, deapodized and summed with
+//                    conj(csm) into q (+ kappa R^2 p), the FP64 partial of
+//                    <p, q>, alpha from the last block of the segment -- the
+//                    band rows of the adjoint never go through HBM;
+//   k_cg_update      x, r and <r, P^2 r>, beta, the stop rule and the history.
+// A block is one image row of one frame (all coils: one half-warp per coil
+// and round).  The arithmetic of every element is that of k_pad_forward /
+// k_fft_rows / k_cg_crop_dot (the same expressions and row transform).
+
+struct RowsArgs {
+    KParams k;
+    const float *deap;   // [D][deap_stride] image-domain deapodization
+    int deap_stride;
+    float scale, weight, kappa;
+    const float *reg;
+    const float2 *csm;
+    int nb, F;
+    float2 *ws;          // k_rows_pad: the padded workspace (band rows written); k_rows_crop_dot: k-space (band rows read)
+    const float2 *tw;    // W_N^e of the row length mos[0]
+    float2 *p;
+    const float2 *r;
+    float2 *q;
+    const float *P;
+    CgSeg *segs;
+    double2 *partials;
+    int seg_per_frame;
+    int update;          // k_rows_pad: apply p = beta p + P^2 r first
+};
+
+template <int N2, int IN>
+__global__ void __launch_bounds__(256) k_rows_pad(RowsArgs a) {
+    extern __shared__ float2 rows_sm[];   // [half-warps][17 N2] exchange, then the row of p
+    const KParams &k = a.k;
+    const int N0 = k.N[0], N1 = k.N[1], m0 = k.mos[0];
+    const int R = blockIdx.x, f = R / N1, y = R - f * N1;
+    const int ox = (m0 - N0) >> 1, oy = (k.mos[1] - N1) >> 1;
+    const int gy = y + oy;
+    const int hw = threadIdx.x >> 4, t = threadIdx.x & 15, nhw = blockDim.x >> 4;
+    float2 *rs = rows_sm + hw * (17 * N2);
+    float2 *prow = rows_sm + nhw * (17 * N2);
+    const CgSeg &S = a.segs[a.seg_per_frame ? f : 0];
+    const int64_t erow = ((int64_t)f * N1 + y) * N0;
+    for (int x = threadIdx.x; x < N0; x += blockDim.x) {
+        const int64_t e = erow + x;
+        float2 v = a.p[e];
+        if (a.update && !S.done) {   // p = beta p + P^2 r, in place
+            const float b = (float)S.beta;
+            float2 rv = a.r[e];
+            if (a.P) { const float w = a.P[e]; const float w2 = w * w; rv.x *= w2; rv.y *= w2; }
+            v = make_float2(b * v.x + rv.x, b * v.y + rv.y);
+            a.p[e] = v;
+        }
+        prow[x] = v;
+    }
+    __syncthreads();
+    float fyz = a.scale;
+    fyz *= a.deap[a.deap_stride + y];
+    for (int c0 = 0; c0 < a.nb; c0 += nhw) {   // uniform across the block
+        const int b = c0 + hw;
+        const bool ok = b < a.nb;
+        const float2 *crow = a.csm + (int64_t)(ok ? b : 0) * k.NN + (int64_t)y * N0;
+        float2 *orow = a.ws + ((int64_t)(ok ? b : 0) * a.F + f) * k.G + (int64_t)gy * m0;
+        row_fft_halfwarp<N2, IN, kSpanAll>(
+            t, 1.f, a.tw, rs, ox, ox + N0, 0, m0,
+            [&](int o) {
+                if (!ok) return make_float2(0.f, 0.f);
+                const int x = o - ox;
+                float fac = a.deap[x] * fyz;
+                if ((o + gy) & 1) fac = -fac;
+                const float2 c = cmul(prow[x], crow[x]);
+                return make_float2(c.x * fac, c.y * fac);
+            },
+            [&](int kk, float2 v) {
+                if (ok) orow[kk] = v;
+            });
+        __syncwarp();   // this half-warp's exchange is read before the next round writes it
+    }
+}
+
+template <int N2, int OUT>
+__global__ void __launch_bounds__(256) k_rows_crop_dot(RowsArgs a) {
+    extern __shared__ float2 rows_sm[];   // [half-warps][17 N2] exchange, then [nb][N0] cropped rows
+    const KParams &k = a.k;
+    const int N0 = k.N[0], N1 = k.N[1], m0 = k.mos[0];
+    CgSeg &S = a.segs[blockIdx.y];
+    if (S.done) return;   // the whole segment
+    const int R = blockIdx.y * gridDim.x + blockIdx.x, f = R / N1, y = R - f * N1;
+    const int ox = (m0 - N0) >> 1, oy = (k.mos[1] - N1) >> 1;
+    const int gy = y + oy;
+    const int hw = threadIdx.x >> 4, t = threadIdx.x & 15, nhw = blockDim.x >> 4;
+    float2 *rs = rows_sm + hw * (17 * N2);
+    float2 *crop = rows_sm + nhw * (17 * N2);
+    for (int c0 = 0; c0 < a.nb; c0 += nhw) {   // uniform across the block
+        const int b = c0 + hw;
+        const bool ok = b < a.nb;
+        const float2 *irow = a.ws + ((int64_t)(ok ? b : 0) * a.F + f) * k.G + (int64_t)gy * m0;
+        float2 *crow = crop + (int64_t)(ok ? b : 0) * N0 - ox;
+        row_fft_halfwarp<N2, kSpanAll, OUT>(
+            t, -1.f, a.tw, rs, 0, m0, ox, ox + N0,
+            [&](int o) { return ok ? irow[o] : make_float2(0.f, 0.f); },
+            [&](int kk, float2 v) {
+                if (ok) crow[kk] = v;
+            });
+        __syncwarp();
+    }
+    __syncthreads();
+    // q = weight * crop * conj(csm) summed + kappa R^2 p ; <p, q>  (as k_cg_crop_dot)
+    float fyz = 1.f;
+    fyz = a.deap[a.deap_stride + y];
+    const int64_t nrow = (int64_t)y * N0, erow = ((int64_t)f * N1 + y) * N0;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int x = threadIdx.x; x < N0; x += blockDim.x) {
+        const int gx = x + ox;
+        float fac = a.deap[x] * fyz;
+        if ((gx + gy) & 1) fac = -fac;
+        fac *= a.scale * a.weight;
+        const int64_t n = nrow + x, e = erow + x;
+        float2 s = make_float2(0.f, 0.f);
+#pragma unroll 8
+        for (int b = 0; b < a.nb; b++) {
+            const float2 v = crop[(int64_t)b * N0 + x];
+            const float2 c = a.csm[(int64_t)b * k.NN + n];
+            const float vr = v.x * fac, vi = v.y * fac;
+            s.x += vr * c.x + vi * c.y;
+            s.y += vi * c.x - vr * c.y;
+        }
+        const float2 pv = a.p[e];
+        const float2 rp = reg_term(pv, a.reg, e);
+        s.x += a.kappa * rp.x;
+        s.y += a.kappa * rp.y;
+        a.q[e] = s;
+        acc.x += (double)pv.x * s.x + (double)pv.y * s.y;
+        acc.y += (double)pv.x * s.y - (double)pv.y * s.x;
+    }
+    double2 tot;
+    if (last_block_sum(acc, a.partials, &S.ctr_dot, &tot) && threadIdx.x == 0) {
+        const double den = tot.x * tot.x + tot.y * tot.y;
+        // alpha = rq / pq  (rq real), cgSolver.h:318
+        S.alpha_re = S.rq * tot.x / den;
+        S.alpha_im = -S.rq * tot.y / den;
+    }
+}
+
+// Threads of the fused row kernels: one half-warp per coil and round, whole
+// warps, at most 256 (coils beyond 16 take several rounds).
+static int rows_threads(int nb) { return 32 * std::max(1, std::min(8, (nb + 1) / 2)); }
+
+static size_t rows_smem(const KParams &k, int nb, int threads, bool crop) {
+    const size_t xch = (size_t)(threads / 16) * 17 * (k.mos[0] / 16);
+    return (xch + (crop ? (size_t)nb * k.N[0] : (size_t)k.N[0])) * sizeof(float2);
+}
+
+template <int N2, int SPAN>
+static void launch_rows_pad_t(const RowsArgs &a, unsigned rows, int threads, size_t smem, cudaStream_t st) {
+    auto kern = k_rows_pad<N2, SPAN>;
+    if (smem > 48 * 1024) GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<rows, threads, smem, st>>>(a); ::gb::note_launch();
+}
+
+template <int N2, int SPAN>
+static void launch_rows_crop_t(const RowsArgs &a, dim3 g, int threads, size_t smem, cudaStream_t st) {
+    auto kern = k_rows_crop_dot<N2, SPAN>;
+    if (smem > 48 * 1024) GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<g, threads, smem, st>>>(a); ::gb::note_launch();
+}
+
+#define GB_ROWS_N2_SWITCH(n2, CALL)                 \
+    switch (n2) {                                   \
+        case 2: CALL(2); break;                     \
+        case 4: CALL(4); break;                     \
+        case 6: CALL(6); break;                     \
+        case 8: CALL(8); break;                     \
+        case 10: CALL(10); break;                   \
+        case 12: CALL(12); break;                   \
+        case 16: CALL(16); break;                   \
+        case 20: CALL(20); break;                   \
+        case 24: CALL(24); break;                   \
+        case 32: CALL(32); break;                   \
+        case 40: CALL(40); break;                   \
+        default: fail(GB_ERR_INTERNAL, "unsupported FFT length"); \
+    }
+
+// Whether the CG iteration runs with the fused row passes: 2D plans under the
+// project FFT passes whose fused kernels fit in shared memory.
+static bool rows_fused_ok(const NufftPlan &p, int nb) {
+    if (p.D != 2 || !fft_custom_ok(p)) return false;
+    const int th = rows_threads(nb);
+    return rows_smem(p.kp, nb, th, true) <= 200 * 1024 && rows_smem(p.kp, nb, th, false) <= 200 * 1024;
+}
+
+static void launch_rows_pad(const RowsArgs &a, cudaStream_t st) {
+    const int threads = rows_threads(a.nb);
+    const size_t smem = rows_smem(a.k, a.nb, threads, false);
+    const unsigned rows = (unsigned)(a.F * a.k.N[1]);
+    const bool half = a.k.N[0] * 2 == a.k.mos[0];
+#define GB_ROWS_PAD(K) \
+    (half ? launch_rows_pad_t<K, kSpanHalf>(a, rows, threads, smem, st) : launch_rows_pad_t<K, kSpanRange>(a, rows, threads, smem, st))
+    GB_ROWS_N2_SWITCH(a.k.mos[0] / 16, GB_ROWS_PAD)
+#undef GB_ROWS_PAD
+    GB_CUDA(cudaGetLastError());
+}
+
+static void launch_rows_crop_dot(const RowsArgs &a, int nseg, cudaStream_t st) {
+    const int threads = rows_threads(a.nb);
+    const size_t smem = rows_smem(a.k, a.nb, threads, true);
+    const int rows = a.F * a.k.N[1];
+    const dim3 g((unsigned)(rows / nseg), (unsigned)nseg);
+    const bool half = a.k.N[0] * 2 == a.k.mos[0];
+#define GB_ROWS_CROP(K) \
+    (half ? launch_rows_crop_t<K, kSpanHalf>(a, g, threads, smem, st) : launch_rows_crop_t<K, kSpanRange>(a, g, threads, smem, st))
+    GB_ROWS_N2_SWITCH(a.k.mos[0] / 16, GB_ROWS_CROP)
+#undef GB_ROWS_CROP
+    GB_CUDA(cudaGetLastError());
+}
+
 // Initialisation per segment: r = rhs - q (q optional), p = P^2 r,
 // rq = Re<r, p>; set_rq0 also records rq0 and clears the iteration state
 // (cgSolver.h:219-288).
@@ -1019,6 +1247,58 @@ static void cg_iteration_fused(CgSolver &cg, cudaStream_t st, double *hist, bool
     ::gb::note_launch();
 }
 
+// One iteration with the fused row passes (2D, project FFT passes): see the
+// kernels k_rows_pad / k_rows_crop_dot.  `first`: p is already P^2 r (no
+// direction update before the pad).
+static void cg_iteration_rows(CgSolver &cg, cudaStream_t st, double *hist, bool first) {
+    SenseOp &s = *cg.E;
+    NufftPlan &p = s.plan;
+    const KParams &k = p.kp;
+    const int nb = s.ncoils;
+    const int64_t nbf = (int64_t)nb * p.F;
+    const int64_t n = (int64_t)p.F * k.NN;
+    const KLayout kl = ws_layout(p, nbf);
+    float2 *pad = p.img_os.get();
+    float2 *kg = ensure_kgrid(p, nbf);
+    float2 *samp = ensure_samp(p, nb);
+    const int m0 = k.mos[0], m1 = k.mos[1];
+    const int y0 = (m1 - k.N[1]) / 2;
+    RowsArgs ra{};
+    ra.k = k;
+    ra.deap = p.deap_img.get();
+    ra.deap_stride = p.maxN;
+    ra.scale = (float)(1.0 / std::sqrt((double)k.G));
+    ra.weight = cg.weight;
+    ra.kappa = cg.kappa;
+    ra.reg = cg.kappa != 0.f ? cg.reg : nullptr;
+    ra.csm = s.csm;
+    ra.nb = nb;
+    ra.F = (int)p.F;
+    ra.tw = fft_twiddles(p, m0, st);
+    ra.p = cg.p.get();
+    ra.r = cg.r.get();
+    ra.q = cg.q.get();
+    ra.P = cg.precond;
+    ra.segs = cg.segs.get();
+    ra.partials = cg.partials.get();
+    ra.seg_per_frame = cg.nseg > 1 ? 1 : 0;
+    // p update + pad + x pass (forward) into the band rows of the pad buffer
+    ra.ws = pad;
+    ra.update = first ? 0 : 1;
+    launch_rows_pad(ra, st);
+    fft_cols(p, m1, pad, kg, nbf * m0, m0, k.G, m0, y0, y0 + k.N[1], 0, m1, false, st);
+    const SampleLayout lay = normal_op_layout(p, nb);
+    launch_degrid(p, kg, samp, nb, lay, s.dcw, 2, true, false, st, &kl);
+    launch_grid(p, samp, kg, nb, lay, nullptr, true, false, st, &kl);
+    fft_cols(p, m1, kg, kg, nbf * m0, m0, k.G, m0, 0, m1, y0, y0 + k.N[1], true, st);
+    // x pass (adjoint) + crop + conjugate coil sum + <p, q> -> alpha
+    ra.ws = kg;
+    launch_rows_crop_dot(ra, cg.nseg, st);
+    k_cg_update<<<seg_grid(cg), 256, 0, st>>>(cg.seg_len, cg.x.get(), cg.r.get(), cg.p.get(), cg.q.get(),
+                                              cg.precond, n, cg.segs.get(), cg.G.get(), cg.partials.get(), hist); ::gb::note_launch();
+    GB_CUDA(cudaGetLastError());
+}
+
 // Applies E^H E (with weight and kappa) to `in` into `out` without the dot.
 static void cg_apply_normal(CgSolver &cg, const float2 *in, float2 *out, cudaStream_t st) {
     SenseOp &s = *cg.E;
@@ -1040,6 +1320,10 @@ static void cg_solve_once(CgSolver &cg, const float2 *rhs, const float2 *x0, dou
                                                 cg.p.get(), cg.precond, n, cg.segs.get(), cg.G.get(),
                                                 cg.partials.get(), 0, (double)cg.tol, hist_base); ::gb::note_launch();
         GB_CUDA(cudaGetLastError());
+    }
+    if (cg.use_rows) {
+        for (uint32_t it = 0; it < cg.iterations; it++) cg_iteration_rows(cg, st, hist, it == 0);
+        return;
     }
     if (cg.use_tail && cg.iterations > 0) {
         SenseOp &s = *cg.E;
@@ -1074,7 +1358,12 @@ static void cg_prepare(CgSolver &cg, cudaStream_t st) {
     // The fused iteration tail needs D >= 2 and all of its blocks resident at
     // once (cooperative launch).
     cg.use_tail = false;
-    if (p.D >= 2 && cg.seg_len % p.kp.N[0] == 0) {
+    cg.use_rows = cg.row_fusion && rows_fused_ok(p, nb) && cg.seg_len % p.kp.N[0] == 0;
+    if (cg.use_rows) {
+        // one block per image row in k_rows_crop_dot: a partial slot each
+        cg.partials.ensure(std::max<size_t>((size_t)sg.x * sg.y, (size_t)p.F * p.kp.N[1]));
+    }
+    if (!cg.use_rows && p.D >= 2 && cg.seg_len % p.kp.N[0] == 0) {
         int dev = 0, coop = 0, nsm = 0, per_sm = 0;
         GB_CUDA(cudaGetDevice(&dev));
         GB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
@@ -1169,7 +1458,7 @@ void cg_solve(CgSolver &cg, const void *d, void *x_out, double *hist, uint32_t *
     if (cg.use_graph) {
         GraphKey key{d, x_out, hist, cg.iterations, cg.refinements, cg.x0, cg.precond, cg.reg, cg.kappa, cg.weight,
                      cg.tol, s.csm, s.dcw, s.ncoils, plan_layout_signature(s.plan, s.ncoils * (int)s.plan.F),
-                     cg.independent_frames, cg.barrier_spin_limit};
+                     cg.independent_frames, cg.barrier_spin_limit, cg.row_fusion};
         if (!cg.graph_exec || !(key == cg.graph_key)) {
             cudaStream_t cs;
             GB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));

@@ -29,8 +29,10 @@ struct GraphKey {
     uint64_t generation;
     bool independent;
     uint32_t spin_limit;
+    bool row_fusion;
     bool operator==(const GraphKey &o) const {
-        return generation == o.generation && independent == o.independent && spin_limit == o.spin_limit && d == o.d && x == o.x && hist == o.hist && iterations == o.iterations &&
+        return generation == o.generation && independent == o.independent && spin_limit == o.spin_limit &&
+               row_fusion == o.row_fusion && d == o.d && x == o.x && hist == o.hist && iterations == o.iterations &&
                refinements == o.refinements && x0 == o.x0 && precond == o.precond && reg == o.reg && kappa == o.kappa &&
                weight == o.weight && tol == o.tol && csm == o.csm && dcw == o.dcw && ncoils == o.ncoils;
     }
@@ -64,6 +66,8 @@ struct CgSolver {
     DevBuf<double2> x64, partials, partials2;
     DevBuf<unsigned int> tail_bar;   // grid barrier of the fused iteration tail
     int tail_tpp = 1;                // threads per pixel of the tail's coil sums
+    bool use_rows = false;           // 2D: iteration with the row passes fused (no grid barrier)
+    bool row_fusion = true;          // allow it (tests compare against the cooperative tail)
     bool use_tail = false;           // fused tail (cooperative launch) available for this shape
     dim3 tail_grid;                  // its launch grid (blocks per segment, segments)
     DevBuf<CgSeg> segs;

@@ -122,6 +122,11 @@ class cuCgSolver:
         block gives up and flags bit 1 of the device error word (0: default)."""
         check(lib.gb_cg_set_barrier_spin_limit(self._h, int(polls)))
 
+    def set_row_fusion(self, enable: bool):
+        """2D: x passes of the FFTs fused into the pad and the crop (default)
+        or, when disabled, the barrier-synchronised fused tail."""
+        check(lib.gb_cg_set_row_fusion(self._h, int(bool(enable))))
+
     def set_use_graph(self, use: bool):
         check(lib.gb_cg_set_use_graph(self._h, int(bool(use))))
 

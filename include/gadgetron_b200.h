@@ -425,6 +425,14 @@ GB_API gb_status gb_cg_set_refinements(gb_cg_solver solver, uint32_t refinements
  * counters.  A small limit makes the timeout path run on purpose (tests).
  * No reference counterpart. */
 GB_API gb_status gb_cg_set_barrier_spin_limit(gb_cg_solver solver, uint32_t spin_limit);
+
+/* 2D plans under the project FFT passes run each CG iteration with the x
+ * pass of the forward FFT fused into the direction update and pad, and the x
+ * pass of the adjoint FFT fused into the crop, coil sum and <p,q> (plain
+ * launches, no grid barrier): enable = 1, the default.  enable = 0 selects the
+ * barrier-synchronised fused tail used by 3D plans instead.  Results agree to
+ * rounding.  No reference counterpart (tuning, tests). */
+GB_API gb_status gb_cg_set_row_fusion(gb_cg_solver solver, int enable);
 /* Solve the frames of a multi-frame operator as independent problems: each
  * frame gets its own CG scalars (rq, alpha, beta, stop flag) while every
  * kernel still covers all frames in one launch.  0 (default) = the

@@ -233,6 +233,39 @@ def test_grid_schedules_bit_identical(cuda):
         plan.set_grid_schedule(3)
 
 
+@pytest.mark.parametrize("frames,coils", [(1, 16), (3, 12), (2, 5)])
+def test_row_fused_iteration_matches_cooperative_tail(cuda, frames, coils):
+    """2D CG with the x passes fused into the pad and the crop (the default)
+    against the barrier-synchronised fused tail: same iterates to rounding,
+    same residual history, both at the oracle's FP64 CG; frame-independent
+    solves with a preconditioner too."""
+    case = sense_case(N=64, coils=coils, frames=frames, seed=41 + frames)
+    E, orc = make_ops(case, cuda)
+    d = orc.mult_M(case["phantom"]).astype(np.complex64)
+    dt = torch.from_numpy(d.reshape(coils, -1)).to(cuda)
+    P = torch.from_numpy(np.random.default_rng(7).uniform(0.5, 1.5, (frames, 64, 64)).astype(np.float32)).to(cuda)
+    for precond in (None, P):
+        sols, hists = {}, {}
+        for fused in (True, False):
+            cg = gb.cuCgSolver()
+            cg.set_encoding_operator(E)
+            cg.set_max_iterations(8)
+            cg.set_tc_tolerance(0.0)
+            cg.set_frame_independent(frames > 1)
+            cg.set_use_graph(True)
+            cg.set_row_fusion(fused)
+            if precond is not None:
+                cg.set_preconditioner(precond)
+            sols[fused] = cg.solve(dt).cpu().numpy()
+            hists[fused] = cg.residual_history[:8].cpu().numpy().copy()
+        assert rel_l2(sols[True], sols[False]) <= 2e-6
+        np.testing.assert_allclose(hists[True], hists[False], rtol=1e-5)
+        if precond is None and frames == 1:   # (frame-independent solves: per-frame oracle elsewhere)
+            xr = O.cg_solve(orc, d, iterations=8, tc_tolerance=0.0)
+            assert rel_l2(sols[True], xr) <= 1e-4
+    assert E.get_plan().device_errors() == 0
+
+
 def test_image_operator_matches_oracle(cuda):
     """cuImageOperator::compute (imageOperator.h:27-45, cuImageOperator.h:35-62):
     same float formulas, same histogram offset."""
@@ -312,16 +345,18 @@ def test_cg_image_regularization_and_preconditioner(cuda, frames, use_graph):
 
 
 def test_grid_barrier_timeout_flags_error_and_next_solve_recovers(cuda):
-    """The fused CG iteration's grid barrier is a bounded wait.  With its limit
-    set to one poll, blocks give up instead of waiting: the solve returns, the
-    device error word reports bit 1, and nothing hangs.  Solves after it at
-    the default limit (plain and graph-captured) start from cleared barrier
+    """The fused CG tail's grid barrier is a bounded wait (2D plans take it
+    with the row fusion off; 3D plans always).  With its limit set to one
+    poll, blocks give up instead of waiting: the solve returns, the device
+    error word reports bit 1, and nothing hangs.  Solves after it at the
+    default limit (plain and graph-captured) start from cleared barrier
     counters and match the oracle again."""
     case = sense_case(coils=4, seed=31)
     E, orc = make_ops(case, cuda)
     d = orc.mult_M(case["phantom"]).astype(np.complex64)
     dt = torch.from_numpy(d.reshape(4, -1)).to(cuda)
     cg = gb.cuCgSolver()
+    cg.set_row_fusion(False)
     cg.set_encoding_operator(E)
     cg.set_max_iterations(6)
     cg.set_tc_tolerance(0.0)
