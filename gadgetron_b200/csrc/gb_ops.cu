@@ -409,6 +409,44 @@ __device__ bool last_block_sum(double2 mine, double2 *partials, unsigned int *ct
     return true;
 }
 
+// last_block_sum for NV values per block (slots blockIdx * NV + v of the
+// segment's partials), summed in the same fixed order.
+template <int NV>
+__device__ bool last_block_sum_v(const double2 (&mine)[NV], double2 *partials, unsigned int *ctr,
+                                 double2 (&total)[NV]) {
+    __shared__ double2 sh[32];
+    __shared__ int s_last;
+    double2 *seg_part = partials + (size_t)blockIdx.y * gridDim.x * NV;
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        const double2 r = block_reduce_d2(mine[v], sh);
+        __syncthreads();   // sh is reused by the next reduction
+        if (threadIdx.x == 0) seg_part[(size_t)blockIdx.x * NV + v] = r;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int old = atomicAdd(ctr, 1u);
+        s_last = (old == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+            const double2 q = __ldcg(&seg_part[(size_t)b * NV + v]);
+            acc.x += q.x;
+            acc.y += q.y;
+        }
+        acc = block_reduce_d2(acc, sh);
+        __syncthreads();
+        total[v] = acc;   // meaningful in thread 0
+    }
+    if (threadIdx.x == 0) *ctr = 0u;
+    return true;
+}
+
 // kappa R^H R p for the regulariser R = diag(reg) (reg null: R = I), as
 // imageOperator::mult_MH_M forms it: (p * reg) * reg.
 __device__ __forceinline__ float2 reg_term(float2 pv, const float *reg, int64_t e) {
@@ -851,24 +889,38 @@ __global__ void __launch_bounds__(256 * TPP, 4 / TPP) k_cg_tail(TailArgs t) {
 
 // ----------------------------------- CG with the row passes fused (2D) ---
 //
-// 2D plans under the project FFT passes run the CG iteration as seven plain
+// 2D plans under the project FFT passes run the CG iteration as plain
 // launches with no grid barrier: the x (row) pass of each FFT direction is
-// fused with what the iteration does next to it.
-//   k_rows_pad       p = beta p + P^2 r (segments still running; beta from the
-//                    previous iteration's k_cg_update), then per coil the
-//                    interior row p x csm x deapodization x checkerboard x
-//                    1/sqrt(G) transformed in place of the row pass's input --
-//                    the padded image never goes through HBM;
+// fused with what the iteration does next to it.  Short iterations (every row
+// kernel one wave) fold the update into the next pad, as below: six launches.
+// Long ones (many frames) keep k_cg_update after k_rows_crop_dot (x, r,
+// <r, P^2 r>, beta, stop rule, history: its grid-stride loops move the CG
+// vectors at full bandwidth) and k_rows_pad only updates p: seven launches.
+//   k_rows_pad       the previous iteration's end -- x += alpha p, r -= alpha q,
+//                    p = beta p + P^2 r for segments still running, the FP64
+//                    partial of <r, P^2 r> and, in the segment's last block, the
+//                    residual, stop rule and history (cgSolver.h:318-375) --
+//                    then per coil the interior row p x csm x deapodization x
+//                    checkerboard x 1/sqrt(G) transformed in place of the row
+//                    pass's input: the padded image never goes through HBM;
 //   (y pass, degridding, gridding, adjoint y pass: as in the other paths)
 //   k_rows_crop_dot  per image row, every coil's band row transformed back,
 //                    cropped in shared memory, deapodized and summed with
-//                    conj(csm) into q (+ kappa R^2 p), the FP64 partial of
-//                    <p, q>, alpha from the last block of the segment -- the
-//                    band rows of the adjoint never go through HBM;
-//   k_cg_update      x, r and <r, P^2 r>, beta, the stop rule and the history.
-// A block is one image row of one frame (all coils: one half-warp per coil
-// and round).  The arithmetic of every element is that of k_pad_forward /
-// k_fft_rows / k_cg_crop_dot (the same expressions and row transform).
+//                    conj(csm) into q (+ kappa R^2 p); the FP64 partials of
+//                    <p, q>, <r, P^2 q> and <q, P^2 q>; the segment's last
+//                    block sets alpha = rq / <p, q> and beta from
+//                    rq' = rq - 2 Re(alpha <r, P^2 q>) + |alpha|^2 <q, P^2 q>,
+//                    the norm of r - alpha q (float alpha, as the update uses
+//                    it) expanded, so that k_rows_pad can update p in the same
+//                    pass as r: the band rows of the adjoint never go through
+//                    HBM and no separate update launch is needed.  rq itself
+//                    is always the dot of the stored r (k_rows_pad, k_cg_init),
+//                    so the expansion's rounding does not accumulate.
+// After the last iteration k_cg_update applies the final x and r update.  A
+// block is one image row of one frame (all coils: one half-warp per coil and
+// round).  The arithmetic of every element is that of k_pad_forward /
+// k_fft_rows / k_cg_crop_dot / k_cg_update (the same expressions and row
+// transform); only beta's rounding differs (relative ~1e-7 of rq / rq').
 
 struct RowsArgs {
     KParams k;
@@ -880,14 +932,17 @@ struct RowsArgs {
     int nb, F;
     float2 *ws;          // k_rows_pad: the padded workspace (band rows written); k_rows_crop_dot: k-space (band rows read)
     const float2 *tw;    // W_N^e of the row length mos[0]
+    float2 *x;
     float2 *p;
-    const float2 *r;
+    float2 *r;
     float2 *q;
     const float *P;
     CgSeg *segs;
+    CgGlobal *G;
+    double *hist;
     double2 *partials;
-    int seg_per_frame;
-    int update;          // k_rows_pad: apply p = beta p + P^2 r first
+    int update;          // k_rows_pad: 0 none, 1 p = beta p + P^2 r, 2 the previous iteration's whole end (x, r, p, residual)
+    int expand;          // k_rows_crop_dot: also beta from the expanded |r - alpha q|^2 (with update 2)
 };
 
 template <int N2, int IN>
@@ -895,25 +950,80 @@ __global__ void __launch_bounds__(256) k_rows_pad(RowsArgs a) {
     extern __shared__ float2 rows_sm[];   // [half-warps][17 N2] exchange, then the row of p
     const KParams &k = a.k;
     const int N0 = k.N[0], N1 = k.N[1], m0 = k.mos[0];
-    const int R = blockIdx.x, f = R / N1, y = R - f * N1;
+    const int R = blockIdx.y * gridDim.x + blockIdx.x, f = R / N1, y = R - f * N1;
     const int ox = (m0 - N0) >> 1, oy = (k.mos[1] - N1) >> 1;
     const int gy = y + oy;
     const int hw = threadIdx.x >> 4, t = threadIdx.x & 15, nhw = blockDim.x >> 4;
     float2 *rs = rows_sm + hw * (17 * N2);
     float2 *prow = rows_sm + nhw * (17 * N2);
-    const CgSeg &S = a.segs[a.seg_per_frame ? f : 0];
+    CgSeg &S = a.segs[blockIdx.y];
+    const bool was_done = S.done != 0;
     const int64_t erow = ((int64_t)f * N1 + y) * N0;
+    double2 acc = make_double2(0.0, 0.0);
+    const bool upd = a.update == 2 && !was_done;
+    const bool upd_p = a.update == 1 && !was_done;
+    const float ar = (float)S.alpha_re, ai = (float)S.alpha_im, beta = (float)S.beta;
     for (int x = threadIdx.x; x < N0; x += blockDim.x) {
         const int64_t e = erow + x;
         float2 v = a.p[e];
-        if (a.update && !S.done) {   // p = beta p + P^2 r, in place
-            const float b = (float)S.beta;
+        if (upd_p) {   // p = beta p + P^2 r (beta from k_cg_update), in place
             float2 rv = a.r[e];
             if (a.P) { const float w = a.P[e]; const float w2 = w * w; rv.x *= w2; rv.y *= w2; }
-            v = make_float2(b * v.x + rv.x, b * v.y + rv.y);
+            v = make_float2(beta * v.x + rv.x, beta * v.y + rv.y);
+            a.p[e] = v;
+        }
+        if (upd) {
+            // x += alpha p ; r -= alpha q  (as k_cg_update)
+            const float2 qv = a.q[e];
+            float2 xv = a.x[e], rv = a.r[e];
+            xv.x += ar * v.x - ai * v.y;
+            xv.y += ar * v.y + ai * v.x;
+            rv.x -= ar * qv.x - ai * qv.y;
+            rv.y -= ar * qv.y + ai * qv.x;
+            a.x[e] = xv;
+            a.r[e] = rv;
+            float w2 = 1.f;
+            if (a.P) { const float w = a.P[e]; w2 = w * w; }
+            acc.x += (double)rv.x * (double)(rv.x * w2) + (double)rv.y * (double)(rv.y * w2);
+            // p = beta p + P^2 r  (as the pad's direction update)
+            if (a.P) { rv.x *= w2; rv.y *= w2; }
+            v = make_float2(beta * v.x + rv.x, beta * v.y + rv.y);
             a.p[e] = v;
         }
         prow[x] = v;
+    }
+    // <r, P^2 r> of the updated r: the segment's last block records the
+    // residual, stop rule and history (its reduction's barriers also make
+    // the row of p visible to the transforms).
+    if (a.update == 2) {
+        double2 tot[1];
+        const double2 mine[1] = {acc};
+        if (last_block_sum_v<1>(mine, a.partials, &S.ctr_upd, tot) && threadIdx.x == 0) {
+            if (!was_done) {   // residual, stop rule (cgSolver.h:336-352)
+                const double rq_new = tot[0].x;
+                S.rq = rq_new;
+                S.metric = rq_new / S.rq0;
+                if (S.metric < a.G->tol) S.done = 1;
+            }
+            __threadfence();
+            const unsigned int old = atomicAdd(&a.G->seg_ctr, 1u);
+            if (old == gridDim.y - 1) {   // last segment of this iteration: history
+                __threadfence();
+                a.G->seg_ctr = 0u;
+                if (!a.G->all_done) {
+                    double mx = 0.0;
+                    int all = 1;
+                    for (unsigned s = 0; s < gridDim.y; s++) {
+                        const double m = *((volatile double *)&a.segs[s].metric);
+                        mx = m > mx ? m : mx;
+                        all &= (*((volatile int *)&a.segs[s].done) != 0);
+                    }
+                    if (a.hist) a.hist[a.G->hist_base + a.G->iters] = mx;
+                    a.G->iters += 1;
+                    if (all) a.G->all_done = 1;
+                }
+            }
+        }
     }
     __syncthreads();
     float fyz = a.scale;
@@ -971,7 +1081,7 @@ __global__ void __launch_bounds__(256) k_rows_crop_dot(RowsArgs a) {
     float fyz = 1.f;
     fyz = a.deap[a.deap_stride + y];
     const int64_t nrow = (int64_t)y * N0, erow = ((int64_t)f * N1 + y) * N0;
-    double2 acc = make_double2(0.0, 0.0);
+    double2 acc[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
     for (int x = threadIdx.x; x < N0; x += blockDim.x) {
         const int gx = x + ox;
         float fac = a.deap[x] * fyz;
@@ -992,15 +1102,39 @@ __global__ void __launch_bounds__(256) k_rows_crop_dot(RowsArgs a) {
         s.x += a.kappa * rp.x;
         s.y += a.kappa * rp.y;
         a.q[e] = s;
-        acc.x += (double)pv.x * s.x + (double)pv.y * s.y;
-        acc.y += (double)pv.x * s.y - (double)pv.y * s.x;
+        // conj(p) q ; w conj(r) q ; w |q|^2   (w = P^2)
+        acc[0].x += (double)pv.x * s.x + (double)pv.y * s.y;
+        acc[0].y += (double)pv.x * s.y - (double)pv.y * s.x;
+        if (a.expand) {
+            const float2 rv = a.r[e];
+            double w2 = 1.0;
+            if (a.P) { const double w = a.P[e]; w2 = w * w; }
+            acc[1].x += w2 * ((double)rv.x * s.x + (double)rv.y * s.y);
+            acc[1].y += w2 * ((double)rv.x * s.y - (double)rv.y * s.x);
+            acc[2].x += w2 * ((double)s.x * s.x + (double)s.y * s.y);
+        }
     }
-    double2 tot;
-    if (last_block_sum(acc, a.partials, &S.ctr_dot, &tot) && threadIdx.x == 0) {
-        const double den = tot.x * tot.x + tot.y * tot.y;
+    if (!a.expand) {
+        double2 tot;
+        if (last_block_sum(acc[0], a.partials, &S.ctr_dot, &tot) && threadIdx.x == 0) {
+            const double den = tot.x * tot.x + tot.y * tot.y;
+            // alpha = rq / pq  (rq real), cgSolver.h:318
+            S.alpha_re = S.rq * tot.x / den;
+            S.alpha_im = -S.rq * tot.y / den;
+        }
+        return;
+    }
+    double2 tot[3];
+    if (last_block_sum_v<3>(acc, a.partials, &S.ctr_dot, tot) && threadIdx.x == 0) {
+        const double den = tot[0].x * tot[0].x + tot[0].y * tot[0].y;
         // alpha = rq / pq  (rq real), cgSolver.h:318
-        S.alpha_re = S.rq * tot.x / den;
-        S.alpha_im = -S.rq * tot.y / den;
+        const double rq = S.rq;
+        S.alpha_re = rq * tot[0].x / den;
+        S.alpha_im = -rq * tot[0].y / den;
+        // |r - alpha q|^2_w with alpha as the update rounds it
+        const double fr = (double)(float)S.alpha_re, fi = (double)(float)S.alpha_im;
+        const double rq_new = rq - 2.0 * (fr * tot[1].x - fi * tot[1].y) + (fr * fr + fi * fi) * tot[2].x;
+        S.beta = rq_new / rq;
     }
 }
 
@@ -1010,14 +1144,15 @@ static int rows_threads(int nb) { return 32 * std::max(1, std::min(8, (nb + 1) /
 
 static size_t rows_smem(const KParams &k, int nb, int threads, bool crop) {
     const size_t xch = (size_t)(threads / 16) * 17 * (k.mos[0] / 16);
+    // crop: the cropped rows of every coil; pad: the row of p
     return (xch + (crop ? (size_t)nb * k.N[0] : (size_t)k.N[0])) * sizeof(float2);
 }
 
 template <int N2, int SPAN>
-static void launch_rows_pad_t(const RowsArgs &a, unsigned rows, int threads, size_t smem, cudaStream_t st) {
+static void launch_rows_pad_t(const RowsArgs &a, dim3 g, int threads, size_t smem, cudaStream_t st) {
     auto kern = k_rows_pad<N2, SPAN>;
     if (smem > 48 * 1024) GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<rows, threads, smem, st>>>(a); ::gb::note_launch();
+    kern<<<g, threads, smem, st>>>(a); ::gb::note_launch();
 }
 
 template <int N2, int SPAN>
@@ -1051,13 +1186,14 @@ static bool rows_fused_ok(const NufftPlan &p, int nb) {
     return rows_smem(p.kp, nb, th, true) <= 200 * 1024 && rows_smem(p.kp, nb, th, false) <= 200 * 1024;
 }
 
-static void launch_rows_pad(const RowsArgs &a, cudaStream_t st) {
+static void launch_rows_pad(const RowsArgs &a, int nseg, cudaStream_t st) {
     const int threads = rows_threads(a.nb);
     const size_t smem = rows_smem(a.k, a.nb, threads, false);
-    const unsigned rows = (unsigned)(a.F * a.k.N[1]);
+    const int rows = a.F * a.k.N[1];
+    const dim3 g((unsigned)(rows / nseg), (unsigned)nseg);
     const bool half = a.k.N[0] * 2 == a.k.mos[0];
 #define GB_ROWS_PAD(K) \
-    (half ? launch_rows_pad_t<K, kSpanHalf>(a, rows, threads, smem, st) : launch_rows_pad_t<K, kSpanRange>(a, rows, threads, smem, st))
+    (half ? launch_rows_pad_t<K, kSpanHalf>(a, g, threads, smem, st) : launch_rows_pad_t<K, kSpanRange>(a, g, threads, smem, st))
     GB_ROWS_N2_SWITCH(a.k.mos[0] / 16, GB_ROWS_PAD)
 #undef GB_ROWS_PAD
     GB_CUDA(cudaGetLastError());
@@ -1248,8 +1384,8 @@ static void cg_iteration_fused(CgSolver &cg, cudaStream_t st, double *hist, bool
 }
 
 // One iteration with the fused row passes (2D, project FFT passes): see the
-// kernels k_rows_pad / k_rows_crop_dot.  `first`: p is already P^2 r (no
-// direction update before the pad).
+// kernels k_rows_pad / k_rows_crop_dot.  `first`: p is already P^2 r (nothing
+// of a previous iteration to finish before the pad).
 static void cg_iteration_rows(CgSolver &cg, cudaStream_t st, double *hist, bool first) {
     SenseOp &s = *cg.E;
     NufftPlan &p = s.plan;
@@ -1275,28 +1411,33 @@ static void cg_iteration_rows(CgSolver &cg, cudaStream_t st, double *hist, bool 
     ra.nb = nb;
     ra.F = (int)p.F;
     ra.tw = fft_twiddles(p, m0, st);
+    ra.x = cg.x.get();
     ra.p = cg.p.get();
     ra.r = cg.r.get();
     ra.q = cg.q.get();
     ra.P = cg.precond;
     ra.segs = cg.segs.get();
+    ra.G = cg.G.get();
+    ra.hist = hist;
     ra.partials = cg.partials.get();
-    ra.seg_per_frame = cg.nseg > 1 ? 1 : 0;
-    // p update + pad + x pass (forward) into the band rows of the pad buffer
+    // the previous iteration's updates + pad + x pass (forward) into the band rows of the pad buffer
     ra.ws = pad;
-    ra.update = first ? 0 : 1;
-    launch_rows_pad(ra, st);
+    ra.update = first ? 0 : (cg.rows_fold ? 2 : 1);
+    ra.expand = cg.rows_fold ? 1 : 0;
+    launch_rows_pad(ra, cg.nseg, st);
     fft_cols(p, m1, pad, kg, nbf * m0, m0, k.G, m0, y0, y0 + k.N[1], 0, m1, false, st);
     const SampleLayout lay = normal_op_layout(p, nb);
     launch_degrid(p, kg, samp, nb, lay, s.dcw, 2, true, false, st, &kl);
     launch_grid(p, samp, kg, nb, lay, nullptr, true, false, st, &kl);
     fft_cols(p, m1, kg, kg, nbf * m0, m0, k.G, m0, 0, m1, y0, y0 + k.N[1], true, st);
-    // x pass (adjoint) + crop + conjugate coil sum + <p, q> -> alpha
+    // x pass (adjoint) + crop + conjugate coil sum + <p, q> -> alpha (and beta)
     ra.ws = kg;
     launch_rows_crop_dot(ra, cg.nseg, st);
-    k_cg_update<<<seg_grid(cg), 256, 0, st>>>(cg.seg_len, cg.x.get(), cg.r.get(), cg.p.get(), cg.q.get(),
-                                              cg.precond, n, cg.segs.get(), cg.G.get(), cg.partials.get(), hist); ::gb::note_launch();
-    GB_CUDA(cudaGetLastError());
+    if (!cg.rows_fold) {
+        k_cg_update<<<seg_grid(cg), 256, 0, st>>>(cg.seg_len, cg.x.get(), cg.r.get(), cg.p.get(), cg.q.get(),
+                                                  cg.precond, n, cg.segs.get(), cg.G.get(), cg.partials.get(), hist); ::gb::note_launch();
+        GB_CUDA(cudaGetLastError());
+    }
 }
 
 // Applies E^H E (with weight and kappa) to `in` into `out` without the dot.
@@ -1323,6 +1464,11 @@ static void cg_solve_once(CgSolver &cg, const float2 *rhs, const float2 *x0, dou
     }
     if (cg.use_rows) {
         for (uint32_t it = 0; it < cg.iterations; it++) cg_iteration_rows(cg, st, hist, it == 0);
+        if (cg.rows_fold) {   // the last iteration's x and r update, residual and history
+            k_cg_update<<<seg_grid(cg), 256, 0, st>>>(cg.seg_len, cg.x.get(), cg.r.get(), cg.p.get(), cg.q.get(),
+                                                      cg.precond, n, cg.segs.get(), cg.G.get(), cg.partials.get(), hist); ::gb::note_launch();
+            GB_CUDA(cudaGetLastError());
+        }
         return;
     }
     if (cg.use_tail && cg.iterations > 0) {
@@ -1360,8 +1506,16 @@ static void cg_prepare(CgSolver &cg, cudaStream_t st) {
     cg.use_tail = false;
     cg.use_rows = cg.row_fusion && rows_fused_ok(p, nb) && cg.seg_len % p.kp.N[0] == 0;
     if (cg.use_rows) {
-        // one block per image row in k_rows_crop_dot: a partial slot each
-        cg.partials.ensure(std::max<size_t>((size_t)sg.x * sg.y, (size_t)p.F * p.kp.N[1]));
+        // one block per image row in the row kernels: three partial slots each
+        cg.partials.ensure(std::max<size_t>((size_t)sg.x * sg.y, 3 * (size_t)p.F * p.kp.N[1]));
+        // A short iteration (every row kernel one wave: at most two rows per
+        // SM) is bound by its chain of launches: the update then rides in the
+        // next pad (six launches).  Long ones keep the separate update kernel,
+        // whose grid-stride loops move x, r, p at full bandwidth.
+        int dev = 0, nsm = 0;
+        GB_CUDA(cudaGetDevice(&dev));
+        GB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        cg.rows_fold = (int64_t)p.F * p.kp.N[1] <= 2 * (int64_t)nsm;
     }
     if (!cg.use_rows && p.D >= 2 && cg.seg_len % p.kp.N[0] == 0) {
         int dev = 0, coop = 0, nsm = 0, per_sm = 0;

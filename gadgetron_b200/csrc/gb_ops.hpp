@@ -68,6 +68,7 @@ struct CgSolver {
     int tail_tpp = 1;                // threads per pixel of the tail's coil sums
     bool use_rows = false;           // 2D: iteration with the row passes fused (no grid barrier)
     bool row_fusion = true;          // allow it (tests compare against the cooperative tail)
+    bool rows_fold = false;          // with it: the x, r, p update folded into the next pad
     bool use_tail = false;           // fused tail (cooperative launch) available for this shape
     dim3 tail_grid;                  // its launch grid (blocks per segment, segments)
     DevBuf<CgSeg> segs;

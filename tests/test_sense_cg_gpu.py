@@ -235,10 +235,12 @@ def test_grid_schedules_bit_identical(cuda):
 
 @pytest.mark.parametrize("frames,coils", [(1, 16), (3, 12), (2, 5)])
 def test_row_fused_iteration_matches_cooperative_tail(cuda, frames, coils):
-    """2D CG with the x passes fused into the pad and the crop (the default)
-    against the barrier-synchronised fused tail: same iterates to rounding,
-    same residual history, both at the oracle's FP64 CG; frame-independent
-    solves with a preconditioner too."""
+    """2D CG with the x passes fused into the pad and the crop (the default;
+    beta from the expanded norm of r - alpha q, the update folded into the
+    next pad) against the barrier-synchronised fused tail (beta from the dot
+    of the updated r): same iterates and residual history to rounding, both
+    at the oracle's FP64 CG; frame-independent solves with a preconditioner
+    too."""
     case = sense_case(N=64, coils=coils, frames=frames, seed=41 + frames)
     E, orc = make_ops(case, cuda)
     d = orc.mult_M(case["phantom"]).astype(np.complex64)
@@ -258,8 +260,8 @@ def test_row_fused_iteration_matches_cooperative_tail(cuda, frames, coils):
                 cg.set_preconditioner(precond)
             sols[fused] = cg.solve(dt).cpu().numpy()
             hists[fused] = cg.residual_history[:8].cpu().numpy().copy()
-        assert rel_l2(sols[True], sols[False]) <= 2e-6
-        np.testing.assert_allclose(hists[True], hists[False], rtol=1e-5)
+        assert rel_l2(sols[True], sols[False]) <= 1e-5
+        np.testing.assert_allclose(hists[True], hists[False], rtol=1e-4)
         if precond is None and frames == 1:   # (frame-independent solves: per-frame oracle elsewhere)
             xr = O.cg_solve(orc, d, iterations=8, tc_tolerance=0.0)
             assert rel_l2(sols[True], xr) <= 1e-4
