@@ -29,6 +29,100 @@ namespace gb {
 NufftPlan::~NufftPlan() {
     for (auto &kv : fft_plans) cufftDestroy(kv.second);
     for (auto &kv : fft_plans_om) cufftDestroy(kv.second);
+    for (auto &g : prep_graph)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (h_stage) cudaFreeHost(h_stage);
+    if (upload_done) {
+        cudaEventSynchronize(upload_done);
+        cudaEventDestroy(upload_done);
+    }
+    if (h_upload) cudaFreeHost(h_upload);
+}
+
+// Pinned staging for host -> device uploads of preprocess: waits until the
+// previous uploads from it have been read, then returns room for `bytes`.
+static unsigned char *upload_room(NufftPlan &p, size_t bytes) {
+    if (p.upload_done) GB_CUDA(cudaEventSynchronize(p.upload_done));
+    if (bytes > p.h_upload_n) {
+        if (p.h_upload) GB_CUDA(cudaFreeHost(p.h_upload));
+        p.h_upload = nullptr;
+        p.h_upload_n = 0;
+        GB_CUDA(cudaMallocHost((void **)&p.h_upload, bytes));
+        p.h_upload_n = bytes;
+    }
+    return p.h_upload;
+}
+
+static void upload_issued(NufftPlan &p, cudaStream_t st) {
+    if (!p.upload_done) GB_CUDA(cudaEventCreateWithFlags(&p.upload_done, cudaEventDisableTiming));
+    GB_CUDA(cudaEventRecord(p.upload_done, st));
+}
+
+// Pinned host words of the plan (grown, never shrunk).
+static uint32_t *stage_words(NufftPlan &p, size_t n) {
+    if (n > p.h_stage_n) {
+        if (p.h_stage) GB_CUDA(cudaFreeHost(p.h_stage));
+        p.h_stage = nullptr;
+        p.h_stage_n = 0;
+        GB_CUDA(cudaMallocHost((void **)&p.h_stage, n * sizeof(uint32_t)));
+        p.h_stage_n = n;
+    }
+    return p.h_stage;
+}
+
+static uint64_t mix_key(uint64_t h, uint64_t v) {
+    for (int b = 0; b < 8; b++) {
+        h ^= (v >> (8 * b)) & 0xffu;
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+// Runs a segment of device work on `st`: eagerly the first time a key is
+// seen, recorded into a graph (on a private stream) and launched the second
+// time, replayed from the recorded graph afterwards.  `work` must not
+// allocate when its key repeats (the key covers every buffer it uses).
+template <class Work>
+static void run_prep_segment(NufftPlan::PrepGraph &g, uint64_t key, cudaStream_t st, Work &&work) {
+    if (g.exec && g.key == key) {
+        GB_CUDA(cudaGraphLaunch(g.exec, st));
+        note_launch(g.kernels);
+        return;
+    }
+    if (g.seen != key) {
+        work(st);
+        g.seen = key;
+        return;
+    }
+    cudaStream_t cs;
+    GB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    const uint64_t before = launch_count();
+    GB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    try {
+        work(cs);
+    } catch (...) {
+        cudaStreamEndCapture(cs, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        throw;
+    }
+    const cudaError_t ec = cudaStreamEndCapture(cs, &graph);
+    const uint64_t kernels = launch_count() - before;
+    note_launch(0 - kernels);   // recorded, not launched
+    if (g.exec) {
+        cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    }
+    cudaError_t ei = ec;
+    if (ec == cudaSuccess) ei = cudaGraphInstantiate(&g.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cs);
+    GB_CUDA(ei);
+    g.key = key;
+    g.kernels = kernels;
+    GB_CUDA(cudaGraphLaunch(g.exec, st));
+    note_launch(kernels);
 }
 
 static double host_kb1(float delta, const NufftPlan &p, int d) {
@@ -372,7 +466,12 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     }
     DevBuf<int64_t> &d_off = p.pp_off;
     d_off.ensure(F + 1);
-    GB_CUDA(cudaMemcpyAsync(d_off.get(), off.data(), (F + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    {
+        unsigned char *up = upload_room(p, (F + 1) * sizeof(int64_t));
+        std::memcpy(up, off.data(), (F + 1) * sizeof(int64_t));
+        GB_CUDA(cudaMemcpyAsync(d_off.get(), up, (F + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+        upload_issued(p, st);
+    }
     DevBuf<float> &pos = p.pp_pos;
     pos.ensure((size_t)D * M);
     DevBuf<uint32_t> &key = p.pp_key, &idx = p.pp_idx, &key_sorted = p.pp_key_sorted;
@@ -381,72 +480,100 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     key_sorted.ensure(M);
     DevBuf<int> &err = p.pp_err;
     err.ensure(1);
-    GB_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), st));
-    const int TB = 256;
-    k_scale_bin<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, traj, M, d_off.get(), F, pos.get(),
-                                                               key.get(), idx.get(), err.get()); ::gb::note_launch();
-    GB_CUDA(cudaGetLastError());
-    // The range flag is read together with the pair count below (one host
-    // synchronisation); until then out-of-range samples sit in tile 0 and
-    // every kernel in between stays in bounds for any position value.
-
-    // Stable sort of samples by home key (frame, tile).
     p.perm.ensure(M);
-    sort_pairs(key.get(), key_sorted.get(), idx.get(), p.perm.get(), M, bits_for(nkeys), p.pp_sort, st);
     p.pos_sorted.ensure((size_t)D * M);
-    k_gather_pos<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(D, M, pos.get(), p.perm.get(),
-                                                                p.pos_sorted.get()); ::gb::note_launch();
-    GB_CUDA(cudaGetLastError());
     p.wtab.ensure((size_t)M * D * kWMax);
-    k_weight_table<<<(unsigned)((M * D + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(),
-                                                                     reinterpret_cast<float4 *>(p.wtab.get())); ::gb::note_launch();
-    GB_CUDA(cudaGetLastError());
-
-    // Home ranges.
     p.home_off.ensure(nkeys + 1);
-    k_sorted_offsets<<<(unsigned)((M + TB) / TB), TB, 0, st>>>(key_sorted.get(), M, (uint32_t)nkeys,
-                                                              p.home_off.get()); ::gb::note_launch();
-    GB_CUDA(cudaGetLastError());
-
-    // Gridding pair lists.
     DevBuf<uint32_t> &pcnt = p.pp_pcnt, &poff = p.pp_poff;
     pcnt.ensure(M + 1);
     poff.ensure(M + 1);
-    GB_CUDA(cudaMemsetAsync(pcnt.get() + M, 0, sizeof(uint32_t), st));
-    k_count_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(), pcnt.get()); ::gb::note_launch();
-    GB_CUDA(cudaGetLastError());
-    exclusive_scan(pcnt.get(), poff.get(), M + 1, p.pp_sort, st);
-    uint32_t npairs = 0;
-    int h_err = 0;
-    GB_CUDA(cudaMemcpyAsync(&npairs, poff.get() + M, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    GB_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    const int TB = 256;
+    uint64_t kp_hash = 1469598103934665603ull;
+    {
+        uint64_t w[(sizeof(KParams) + 7) / 8] = {};
+        std::memcpy(w, &k, sizeof(KParams));
+        for (uint64_t v : w) kp_hash = mix_key(kp_hash, v);
+    }
+
+    // Segment A: scaling and range check, home keys, stable sort of the
+    // samples by (frame, home tile), sorted positions, weight table, home
+    // ranges, pair counts and their scan.  Until the range flag is read
+    // back with the pair count, out-of-range samples sit in tile 0 and every
+    // kernel in between stays in bounds for any position value.
+    uint64_t key_a = kp_hash;
+    for (uint64_t v : {(uint64_t)(uintptr_t)traj, (uint64_t)M, (uint64_t)F, (uint64_t)nkeys,
+                       (uint64_t)(uintptr_t)d_off.get(), (uint64_t)(uintptr_t)pos.get(), (uint64_t)(uintptr_t)key.get(),
+                       (uint64_t)(uintptr_t)idx.get(), (uint64_t)(uintptr_t)key_sorted.get(),
+                       (uint64_t)(uintptr_t)err.get(), (uint64_t)(uintptr_t)p.perm.get(),
+                       (uint64_t)(uintptr_t)p.pos_sorted.get(), (uint64_t)(uintptr_t)p.wtab.get(),
+                       (uint64_t)(uintptr_t)p.home_off.get(), (uint64_t)(uintptr_t)pcnt.get(),
+                       (uint64_t)(uintptr_t)poff.get(), (uint64_t)(uintptr_t)p.pp_sort.get(), (uint64_t)p.pp_sort.n})
+        key_a = mix_key(key_a, v);
+    run_prep_segment(p.prep_graph[0], key_a, st, [&](cudaStream_t s) {
+        GB_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
+        k_scale_bin<<<(unsigned)((M + TB - 1) / TB), TB, 0, s>>>(k, traj, M, d_off.get(), F, pos.get(),
+                                                                  key.get(), idx.get(), err.get()); ::gb::note_launch();
+        GB_CUDA(cudaGetLastError());
+        sort_pairs(key.get(), key_sorted.get(), idx.get(), p.perm.get(), M, bits_for(nkeys), p.pp_sort, s);
+        k_gather_pos<<<(unsigned)((M + TB - 1) / TB), TB, 0, s>>>(D, M, pos.get(), p.perm.get(),
+                                                                   p.pos_sorted.get()); ::gb::note_launch();
+        GB_CUDA(cudaGetLastError());
+        k_weight_table<<<(unsigned)((M * D + TB - 1) / TB), TB, 0, s>>>(k, M, p.pos_sorted.get(),
+                                                                        reinterpret_cast<float4 *>(p.wtab.get())); ::gb::note_launch();
+        GB_CUDA(cudaGetLastError());
+        k_sorted_offsets<<<(unsigned)((M + TB) / TB), TB, 0, s>>>(key_sorted.get(), M, (uint32_t)nkeys,
+                                                                 p.home_off.get()); ::gb::note_launch();
+        GB_CUDA(cudaGetLastError());
+        GB_CUDA(cudaMemsetAsync(pcnt.get() + M, 0, sizeof(uint32_t), s));
+        k_count_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, s>>>(k, M, p.pos_sorted.get(), pcnt.get()); ::gb::note_launch();
+        GB_CUDA(cudaGetLastError());
+        exclusive_scan(pcnt.get(), poff.get(), M + 1, p.pp_sort, s);
+    });
+    uint32_t *hs = stage_words(p, 2);
+    GB_CUDA(cudaMemcpyAsync(hs, poff.get() + M, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaMemcpyAsync(hs + 1, err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
     GB_CUDA(cudaStreamSynchronize(st));
-    if (h_err) fail(GB_ERR_TRAJECTORY_RANGE, "trajectory out of range [-1/2, 1/2]");
+    const uint32_t npairs = hs[0];
+    if (hs[1]) fail(GB_ERR_TRAJECTORY_RANGE, "trajectory out of range [-1/2, 1/2]");
     p.total_pairs = npairs;
+
+    // Segment B: the gridding pair lists -- (tile, sample) pairs written,
+    // stably sorted by (frame, tile), their ranges, and the pair rows of the
+    // row-variant gridding (2D/3D tiles up to 96 cells of extent sum).
     DevBuf<uint32_t> &pkey = p.pp_pkey, &pval = p.pp_pval, &pkey_sorted = p.pp_pkey_sorted;
     pkey.ensure(npairs);
     pval.ensure(npairs);
     pkey_sorted.ensure(npairs);
     p.grid_list.ensure(npairs);
-    k_write_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, st>>>(k, M, p.pos_sorted.get(), key_sorted.get(),
-                                                                 poff.get(), pkey.get(), pval.get()); ::gb::note_launch();
-    GB_CUDA(cudaGetLastError());
-    sort_pairs(pkey.get(), pkey_sorted.get(), pval.get(), p.grid_list.get(), npairs, bits_for(nkeys), p.pp_sort, st);
     p.grid_off.ensure(nkeys + 1);
-    k_sorted_offsets<<<(unsigned)(((int64_t)npairs + TB) / TB), TB, 0, st>>>(pkey_sorted.get(), npairs,
-                                                                            (uint32_t)nkeys, p.grid_off.get()); ::gb::note_launch();
-    GB_CUDA(cudaGetLastError());
-    // Pair rows for the row-variant gridding kernel (2D/3D tiles up to 96 cells of extent sum).
-    p.pair_row_stride = 0;
-    if (D >= 2 && pair_row_weights(k) <= 96 && npairs > 0) {
-        const int rf = pair_row_floats(k);
-        p.pair_rows.ensure((size_t)npairs * rf);
-        k_pair_rows<<<(unsigned)(((int64_t)npairs * D + TB - 1) / TB), TB, 0, st>>>(
-            k, M, npairs, p.pos_sorted.get(), p.wtab.get(), pkey_sorted.get(), p.grid_list.get(), p.pair_rows.get(),
-            rf, pair_row_weights(k)); ::gb::note_launch();
+    const bool rows = D >= 2 && pair_row_weights(k) <= 96 && npairs > 0;
+    const int rf = rows ? pair_row_floats(k) : 0;
+    if (rows) p.pair_rows.ensure((size_t)npairs * rf);
+    uint64_t key_b = kp_hash;
+    for (uint64_t v : {(uint64_t)npairs, (uint64_t)M, (uint64_t)nkeys, (uint64_t)rf,
+                       (uint64_t)(uintptr_t)p.pos_sorted.get(), (uint64_t)(uintptr_t)key_sorted.get(),
+                       (uint64_t)(uintptr_t)poff.get(), (uint64_t)(uintptr_t)pkey.get(), (uint64_t)(uintptr_t)pval.get(),
+                       (uint64_t)(uintptr_t)pkey_sorted.get(), (uint64_t)(uintptr_t)p.grid_list.get(),
+                       (uint64_t)(uintptr_t)p.grid_off.get(), (uint64_t)(uintptr_t)p.wtab.get(),
+                       (uint64_t)(uintptr_t)p.pair_rows.get(), (uint64_t)(uintptr_t)p.pp_sort.get(),
+                       (uint64_t)p.pp_sort.n})
+        key_b = mix_key(key_b, v);
+    run_prep_segment(p.prep_graph[1], key_b, st, [&](cudaStream_t s) {
+        k_write_pairs<<<(unsigned)((M + TB - 1) / TB), TB, 0, s>>>(k, M, p.pos_sorted.get(), key_sorted.get(),
+                                                                    poff.get(), pkey.get(), pval.get()); ::gb::note_launch();
         GB_CUDA(cudaGetLastError());
-        p.pair_row_stride = rf;
-    }
+        sort_pairs(pkey.get(), pkey_sorted.get(), pval.get(), p.grid_list.get(), npairs, bits_for(nkeys), p.pp_sort, s);
+        k_sorted_offsets<<<(unsigned)(((int64_t)npairs + TB) / TB), TB, 0, s>>>(pkey_sorted.get(), npairs,
+                                                                               (uint32_t)nkeys, p.grid_off.get()); ::gb::note_launch();
+        GB_CUDA(cudaGetLastError());
+        if (rows) {
+            k_pair_rows<<<(unsigned)(((int64_t)npairs * D + TB - 1) / TB), TB, 0, s>>>(
+                k, M, npairs, p.pos_sorted.get(), p.wtab.get(), pkey_sorted.get(), p.grid_list.get(), p.pair_rows.get(),
+                rf, pair_row_weights(k)); ::gb::note_launch();
+            GB_CUDA(cudaGetLastError());
+        }
+    });
+    p.pair_row_stride = rf;
     if (p.err_flag.ensure(1)) GB_CUDA(cudaMemsetAsync(p.err_flag.get(), 0, sizeof(unsigned int), st));
 
     p.F = F;
@@ -468,9 +595,10 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
 void plan_build_work(NufftPlan &p, cudaStream_t st) {
     const KParams &k = p.kp;
     const uint32_t nkeys = p.F * (uint32_t)k.ntiles_total;
-    std::vector<uint32_t> hoff(nkeys + 1), goff(nkeys + 1);
-    GB_CUDA(cudaMemcpyAsync(hoff.data(), p.home_off.get(), (nkeys + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    GB_CUDA(cudaMemcpyAsync(goff.data(), p.grid_off.get(), (nkeys + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    uint32_t *hoff = stage_words(p, 2 * ((size_t)nkeys + 1));   // pinned: both readbacks, one synchronisation
+    uint32_t *goff = hoff + nkeys + 1;
+    GB_CUDA(cudaMemcpyAsync(hoff, p.home_off.get(), (nkeys + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaMemcpyAsync(goff, p.grid_off.get(), (nkeys + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     GB_CUDA(cudaStreamSynchronize(st));
     p.h_home_counts.resize(nkeys);
     for (uint32_t i = 0; i < nkeys; i++) p.h_home_counts[i] = hoff[i + 1] - hoff[i];
@@ -542,18 +670,24 @@ void plan_build_work(NufftPlan &p, cudaStream_t st) {
 
     p.n_deg_items = (int)deg.size();
     p.deg_items.ensure(std::max<size_t>(1, deg.size()));
-    if (!deg.empty())
-        GB_CUDA(cudaMemcpyAsync(p.deg_items.get(), deg.data(), deg.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
     p.n_grd_items = (int)grd.size();
     p.grd_items.ensure(std::max<size_t>(1, grd.size()));
-    GB_CUDA(cudaMemcpyAsync(p.grd_items.get(), grd.data(), grd.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
     p.n_splits = (int)splits.size();
     p.n_slots = slots;
     p.splits.ensure(std::max<size_t>(1, splits.size()));
-    if (!splits.empty())
-        GB_CUDA(cudaMemcpyAsync(p.splits.get(), splits.data(), splits.size() * sizeof(SplitInfo), cudaMemcpyHostToDevice, st));
+    // The three lists go up from pinned staging (asynchronous; the staging
+    // is not rewritten before these copies have been read).
+    const size_t bd = deg.size() * sizeof(WorkItem), bg = grd.size() * sizeof(WorkItem);
+    const size_t bs = splits.size() * sizeof(SplitInfo);
+    unsigned char *up = upload_room(p, bd + bg + bs);
+    if (bd) std::memcpy(up, deg.data(), bd);
+    if (bg) std::memcpy(up + bd, grd.data(), bg);
+    if (bs) std::memcpy(up + bd + bg, splits.data(), bs);
+    if (bd) GB_CUDA(cudaMemcpyAsync(p.deg_items.get(), up, bd, cudaMemcpyHostToDevice, st));
+    if (bg) GB_CUDA(cudaMemcpyAsync(p.grd_items.get(), up + bd, bg, cudaMemcpyHostToDevice, st));
+    if (bs) GB_CUDA(cudaMemcpyAsync(p.splits.get(), up + bd + bg, bs, cudaMemcpyHostToDevice, st));
+    upload_issued(p, st);
     p.split_counter_groups = 0;   // (re)allocated by the gridding launcher
-    GB_CUDA(cudaStreamSynchronize(st));   // host vectors above go out of scope
 }
 
 uint64_t plan_layout_signature(const NufftPlan &p, int nbf) {

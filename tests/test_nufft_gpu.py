@@ -254,6 +254,49 @@ def test_determinism(cuda):
     assert torch.equal(a, b)
 
 
+def test_repeated_preprocess_replays_recorded_segments(cuda):
+    """Preprocess records its two device segments as graphs the second time
+    the same shapes arrive on the same buffers and replays them after that.
+    A trajectory changed in place between calls (same buffer, new values, so
+    every later call replays) must give the results of a fresh plan; an
+    out-of-range trajectory is still reported on a replay; a trajectory of
+    another length re-runs eagerly."""
+    case = radial_case(N=64, spokes=24, samples=128, batches=2, seed=51)
+    dev = torch.device("cuda:0")
+    other = S.radial_golden_angle_2d(24, 128, profile_offset=977).astype(np.float32)
+    traj_t = torch.from_numpy(case["traj"]).to(dev)
+    plan = gb.NFFT.make_plan(case["N"], case["mos"], case["W"])
+    x = torch.from_numpy(case["img"]).to(dev)
+    for rep in range(4):   # eager, recorded, replayed, replayed
+        src = case["traj"] if rep % 2 == 0 else other
+        traj_t.copy_(torch.from_numpy(src))
+        plan.preprocess(traj_t)
+        y = torch.empty((case["batches"], case["M"]), dtype=torch.complex64, device=dev)
+        plan.compute(x, y, None, gb.NFFT_comp_mode.FORWARDS_C2NC)
+        fresh = gb.NFFT.make_plan(case["N"], case["mos"], case["W"])
+        fresh.preprocess(torch.from_numpy(src).to(dev))
+        y2 = torch.empty_like(y)
+        fresh.compute(x, y2, None, gb.NFFT_comp_mode.FORWARDS_C2NC)
+        assert torch.equal(y, y2), rep
+        back = torch.empty_like(x)
+        plan.compute(y, back, None, gb.NFFT_comp_mode.BACKWARDS_NC2C)
+        back2 = torch.empty_like(x)
+        fresh.compute(y2, back2, None, gb.NFFT_comp_mode.BACKWARDS_NC2C)
+        assert torch.equal(back, back2), rep
+    bad = case["traj"].copy()
+    bad[5, 0] = 0.75
+    traj_t.copy_(torch.from_numpy(bad))
+    with pytest.raises(RuntimeError):
+        plan.preprocess(traj_t)
+    short = torch.from_numpy(case["traj"][: case["M"] // 2].copy()).to(dev)
+    plan.preprocess(short)
+    orc = O.OraclePlan(case["N"], case["mos"], case["W"])
+    orc.preprocess(case["traj"][: case["M"] // 2].reshape(1, -1, 2))
+    y = torch.empty((case["batches"], case["M"] // 2), dtype=torch.complex64, device=dev)
+    plan.compute(x, y, None, gb.NFFT_comp_mode.FORWARDS_C2NC)
+    assert rel_l2(y.cpu().numpy(), orc.forward_c2nc(case["img"])) <= PARITY_TOL
+
+
 def test_error_paths(cuda):
     plan = gb.NFFT.make_plan((32, 32), (64, 64), 5.5)
     x = torch.zeros((1, 1, 32, 32), dtype=torch.complex64, device=cuda)
