@@ -57,7 +57,7 @@ constexpr int kColsPerCta = 8;
 constexpr int kColsRow = 16 * kColsPerCta + 8;
 
 template <int N2, int IN, int OUT>
-__global__ void __launch_bounds__(16 * kColsPerCta, 4) k_fft_cols(FftColArgs a) {
+__global__ void __launch_bounds__(16 * kColsPerCta, (N2 <= 24) ? 6 : 4) k_fft_cols(FftColArgs a) {
     constexpr int N = 16 * N2;
     extern __shared__ float2 fft_sm[];
     const int c = threadIdx.x % kColsPerCta, t = threadIdx.x / kColsPerCta;

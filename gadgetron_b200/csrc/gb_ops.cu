@@ -1051,7 +1051,7 @@ __global__ void __launch_bounds__(256) k_rows_pad(RowsArgs a) {
 }
 
 template <int N2, int OUT>
-__global__ void __launch_bounds__(256) k_rows_crop_dot(RowsArgs a) {
+__global__ void __launch_bounds__(256, (N2 <= 24) ? 3 : 2) k_rows_crop_dot(RowsArgs a) {
     extern __shared__ float2 rows_sm[];   // [half-warps][17 N2] exchange, then [nb][N0] cropped rows
     const KParams &k = a.k;
     const int N0 = k.N[0], N1 = k.N[1], m0 = k.mos[0];
