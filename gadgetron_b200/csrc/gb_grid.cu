@@ -1826,7 +1826,7 @@ __device__ __forceinline__ void degrid_table_passes(const ConvArgs &a, const Wor
     using Sh = DegridShape<CG>;
     constexpr int CPL = Sh::CPL, LPS = Sh::LPS, SPW = Sh::SPW;
     constexpr int D = D3 ? 3 : 2;
-    constexpr int CS = D3 ? CG : CG + 2;
+    constexpr int CS = (D3 || CG == 12) ? CG : CG + 2;
     const KParams &k = a.k;
     const int R0 = region_dim(k, 0), R1 = region_dim(k, 1), R2 = region_dim(k, 2);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1942,14 +1942,14 @@ __device__ __forceinline__ void degrid_table_passes(const ConvArgs &a, const Wor
 }
 
 template <int CG, int NT, bool D3>
-__global__ void __launch_bounds__(kThreads, D3 ? 2 : 3)
+__global__ void __launch_bounds__(kThreads, D3 ? 2 : (CG == 12 ? 4 : 3))
 k_degrid_table(ConvArgs a, const float2 *__restrict__ grid, float2 *__restrict__ out) {
     constexpr int SPW = DegridShape<CG>::SPW;
     // Staged cell stride in float2.  2D: padded to an odd number of 16-byte
     // chunks (conflict-free staging stores; the region copy is a large share
     // of a 2D item's work).  3D: unpadded (the copy is a few percent of an
     // item's work there and the region is large).
-    constexpr int CS = D3 ? CG : CG + 2;
+    constexpr int CS = (D3 || CG == 12) ? CG : CG + 2;
     static_assert(CG >= 4, "table degridding stages coil pairs");
     extern __shared__ float4 smem_raw[];
     const KParams &k = a.k;
@@ -2391,7 +2391,7 @@ static void degrid_dispatch(int cg, const ConvArgs &a, dim3 g, size_t smem, cons
 }
 
 static size_t degrid_table_smem(const KParams &k, int cg) {
-    const int cs = k.D == 3 ? cg : cg + 2;   // cell stride of k_degrid_table
+    const int cs = (k.D == 3 || cg == 12) ? cg : cg + 2;   // cell stride of k_degrid_table
     const size_t pad = (size_t)(region_dim(k, 0) + 1) * cs;
     return ((size_t)region_dim(k, 0) * region_dim(k, 1) * region_dim(k, 2) * cs + pad) * sizeof(float2);
 }
