@@ -590,6 +590,27 @@ void plan_preprocess(NufftPlan &p, const float *traj, uint64_t Mtot, uint32_t F,
     p.prepped = true;
 }
 
+// Stable sort of work items by length, longest first (the same order as a
+// std::stable_sort on that key): a counting sort when the lengths are small,
+// as they are for tile lists -- this runs in every preprocess.
+static void sort_items_by_length(std::vector<WorkItem> &v) {
+    if (v.size() < 2) return;
+    int maxlen = 0;
+    for (const WorkItem &w : v) maxlen = std::max(maxlen, w.end - w.begin);
+    if (maxlen > (1 << 16)) {
+        std::stable_sort(v.begin(), v.end(), [](const WorkItem &a, const WorkItem &b) {
+            return (a.end - a.begin) > (b.end - b.begin);
+        });
+        return;
+    }
+    std::vector<uint32_t> start((size_t)maxlen + 2, 0u);
+    for (const WorkItem &w : v) start[(size_t)(maxlen - (w.end - w.begin)) + 1]++;
+    for (size_t i = 1; i < start.size(); i++) start[i] += start[i - 1];
+    std::vector<WorkItem> out(v.size());
+    for (const WorkItem &w : v) out[start[(size_t)(maxlen - (w.end - w.begin))]++] = w;
+    v.swap(out);
+}
+
 // Host-side work lists: degridding chunks of home samples, gridding tiles
 // (heavy tiles split into chunks reduced by the last CTA).
 void plan_build_work(NufftPlan &p, cudaStream_t st) {
@@ -620,9 +641,7 @@ void plan_build_work(NufftPlan &p, cudaStream_t st) {
             deg.push_back(w);
         }
     }
-    std::stable_sort(deg.begin(), deg.end(), [](const WorkItem &a, const WorkItem &b) {
-        return (a.end - a.begin) > (b.end - b.begin);
-    });
+    sort_items_by_length(deg);
 
     // Gridding items.
     int64_t total = goff[nkeys];
@@ -662,9 +681,7 @@ void plan_build_work(NufftPlan &p, cudaStream_t st) {
             slots += nch;
         }
     }
-    std::stable_sort(light.begin(), light.end(), [](const WorkItem &a, const WorkItem &b) {
-        return (a.end - a.begin) > (b.end - b.begin);
-    });
+    sort_items_by_length(light);
     std::vector<WorkItem> grd(heavy);
     grd.insert(grd.end(), light.begin(), light.end());
 
