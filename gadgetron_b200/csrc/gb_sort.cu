@@ -186,6 +186,35 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t *__r
     }
 }
 
+// One block: exclusive scan of a short array, tile after tile with a running
+// carry (a few tiles: one launch instead of three).  In place allowed.
+__global__ void __launch_bounds__(kScanThreads) k_scan_small(const uint32_t *__restrict__ in, int64_t n,
+                                                             uint32_t *__restrict__ out) {
+    __shared__ uint32_t sh[33];
+    uint32_t carry = 0u;
+    for (int64_t tb = 0; tb < n; tb += kScanTile) {
+        const int64_t base = tb + (int64_t)threadIdx.x * kScanPerThread;
+        uint32_t v[kScanPerThread];
+        uint32_t s = 0u;
+#pragma unroll
+        for (int i = 0; i < kScanPerThread; i++) {
+            v[i] = base + i < n ? in[base + i] : 0u;
+            s += v[i];
+        }
+        uint32_t pre = block_exclusive_scan(s, sh);
+        __syncthreads();
+        const uint32_t total = sh[32];
+        pre += carry;
+#pragma unroll
+        for (int i = 0; i < kScanPerThread; i++) {
+            if (base + i < n) out[base + i] = pre;
+            pre += v[i];
+        }
+        carry += total;
+        __syncthreads();
+    }
+}
+
 // One block: exclusive scan of the tile sums, chunk by chunk.
 __global__ void __launch_bounds__(kScanThreads) k_scan_sums(uint32_t *__restrict__ sums, int64_t n) {
     __shared__ uint32_t sh[33];
@@ -212,8 +241,8 @@ void scan_scratch_need(int64_t n, size_t *bytes) {
 void exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *tile_scratch, cudaStream_t st) {
     if (n <= 0) return;
     const int64_t tiles = (n + kScanTile - 1) / kScanTile;
-    if (tiles == 1) {
-        k_scan_tiles<<<1, kScanThreads, 0, st>>>(in, n, out, nullptr, nullptr); note_launch();
+    if (tiles <= 4) {   // short: one block, one launch
+        k_scan_small<<<1, kScanThreads, 0, st>>>(in, n, out); note_launch();
         GB_CUDA(cudaGetLastError());
         return;
     }
