@@ -185,7 +185,10 @@ __device__ __forceinline__ bool out_span(int q, int kk, int lo, int hi) {
 // then the 16-point DFTs give X[k2 + N2 q].  load(o) supplies input point o
 // (called only inside the IN span), store(kk, v) takes output kk (only inside
 // the OUT span).  Inverse (sg = -1) runs as conj(DFT(conj x)).  Both halves
-// of the warp must call it (it has a __syncwarp).
+// of the warp must call it (it has __syncwarp()s).  The first 16 columns'
+// exchange cells (rs[0, 272)) are all read before the first store, and later
+// groups read only above them: store may write there (a caller's output row
+// of at most 272 points can share the exchange buffer).
 template <int N2, int IN, int OUT, class Load, class Store>
 __device__ __forceinline__ void row_fft_halfwarp(int t, float sg, const float2 *__restrict__ tw, float2 *rs,
                                                  int in_lo, int in_hi, int out_lo, int out_hi, Load load,
@@ -212,10 +215,13 @@ __device__ __forceinline__ void row_fft_halfwarp(int t, float sg, const float2 *
 #pragma unroll
     for (int g = 0; g < G; g++) {
         const int k2 = t + 16 * g;
+        float2 z[16];
         if (k2 < N2) {
-            float2 z[16];
 #pragma unroll
             for (int u = 0; u < 16; u++) z[u] = rs[u + 17 * k2];
+        }
+        if (g == 0) __syncwarp();   // columns 0..15 read before any store
+        if (k2 < N2) {
             dft<16>(z);
 #pragma unroll
             for (int q = 0; q < 16; q++) {

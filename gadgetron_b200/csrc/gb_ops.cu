@@ -943,6 +943,7 @@ struct RowsArgs {
     double2 *partials;
     int update;          // k_rows_pad: 0 none, 1 p = beta p + P^2 r, 2 the previous iteration's whole end (x, r, p, residual)
     int expand;          // k_rows_crop_dot: also beta from the expanded |r - alpha q|^2 (with update 2)
+    int crop_alias;      // k_rows_crop_dot: coil b's cropped row in half-warp b's exchange cells (one round)
 };
 
 template <int N2, int IN>
@@ -1052,7 +1053,11 @@ __global__ void __launch_bounds__(256) k_rows_pad(RowsArgs a) {
 
 template <int N2, int OUT>
 __global__ void __launch_bounds__(256, (N2 <= 24) ? 3 : 2) k_rows_crop_dot(RowsArgs a) {
-    extern __shared__ float2 rows_sm[];   // [half-warps][17 N2] exchange, then [nb][N0] cropped rows
+    // [half-warps][17 N2] exchange, then [nb][N0] cropped rows; with
+    // crop_alias (every coil in the first round, N0 <= 272) coil b's cropped
+    // row takes the first N0 exchange cells of half-warp b, which the row
+    // transform has read before it stores.
+    extern __shared__ float2 rows_sm[];
     const KParams &k = a.k;
     const int N0 = k.N[0], N1 = k.N[1], m0 = k.mos[0];
     CgSeg &S = a.segs[blockIdx.y];
@@ -1062,12 +1067,13 @@ __global__ void __launch_bounds__(256, (N2 <= 24) ? 3 : 2) k_rows_crop_dot(RowsA
     const int gy = y + oy;
     const int hw = threadIdx.x >> 4, t = threadIdx.x & 15, nhw = blockDim.x >> 4;
     float2 *rs = rows_sm + hw * (17 * N2);
-    float2 *crop = rows_sm + nhw * (17 * N2);
+    float2 *crop = a.crop_alias ? rows_sm : rows_sm + nhw * (17 * N2);
+    const int cst = a.crop_alias ? 17 * N2 : N0;   // crop row stride
     for (int c0 = 0; c0 < a.nb; c0 += nhw) {   // uniform across the block
         const int b = c0 + hw;
         const bool ok = b < a.nb;
         const float2 *irow = a.ws + ((int64_t)(ok ? b : 0) * a.F + f) * k.G + (int64_t)gy * m0;
-        float2 *crow = crop + (int64_t)(ok ? b : 0) * N0 - ox;
+        float2 *crow = crop + (int64_t)(ok ? b : 0) * cst - ox;
         row_fft_halfwarp<N2, kSpanAll, OUT>(
             t, -1.f, a.tw, rs, 0, m0, ox, ox + N0,
             [&](int o) { return ok ? irow[o] : make_float2(0.f, 0.f); },
@@ -1091,7 +1097,7 @@ __global__ void __launch_bounds__(256, (N2 <= 24) ? 3 : 2) k_rows_crop_dot(RowsA
         float2 s = make_float2(0.f, 0.f);
 #pragma unroll 8
         for (int b = 0; b < a.nb; b++) {
-            const float2 v = crop[(int64_t)b * N0 + x];
+            const float2 v = crop[(int64_t)b * cst + x];
             const float2 c = a.csm[(int64_t)b * k.NN + n];
             const float vr = v.x * fac, vi = v.y * fac;
             s.x += vr * c.x + vi * c.y;
@@ -1142,9 +1148,18 @@ __global__ void __launch_bounds__(256, (N2 <= 24) ? 3 : 2) k_rows_crop_dot(RowsA
 // warps, at most 256 (coils beyond 16 take several rounds).
 static int rows_threads(int nb) { return 32 * std::max(1, std::min(8, (nb + 1) / 2)); }
 
+// Whether k_rows_crop_dot keeps coil b's cropped row in half-warp b's
+// exchange cells: every coil in one round, and the row within the cells that
+// the transform's first column group reads (272) when it has several groups.
+static bool rows_crop_alias(const KParams &k, int nb, int threads) {
+    return nb <= threads / 16 && (k.mos[0] / 16 <= 16 || k.N[0] <= 272);
+}
+
 static size_t rows_smem(const KParams &k, int nb, int threads, bool crop) {
     const size_t xch = (size_t)(threads / 16) * 17 * (k.mos[0] / 16);
-    // crop: the cropped rows of every coil; pad: the row of p
+    // crop: the cropped rows of every coil (unless they share the exchange
+    // cells); pad: the row of p
+    if (crop && rows_crop_alias(k, nb, threads)) return xch * sizeof(float2);
     return (xch + (crop ? (size_t)nb * k.N[0] : (size_t)k.N[0])) * sizeof(float2);
 }
 
@@ -1199,8 +1214,10 @@ static void launch_rows_pad(const RowsArgs &a, int nseg, cudaStream_t st) {
     GB_CUDA(cudaGetLastError());
 }
 
-static void launch_rows_crop_dot(const RowsArgs &a, int nseg, cudaStream_t st) {
+static void launch_rows_crop_dot(const RowsArgs &args, int nseg, cudaStream_t st) {
+    RowsArgs a = args;
     const int threads = rows_threads(a.nb);
+    a.crop_alias = rows_crop_alias(a.k, a.nb, threads) ? 1 : 0;
     const size_t smem = rows_smem(a.k, a.nb, threads, true);
     const int rows = a.F * a.k.N[1];
     const dim3 g((unsigned)(rows / nseg), (unsigned)nseg);
